@@ -1,0 +1,977 @@
+// C-ABI of the Krylov engine: contexts, sector Hamiltonians and the host-side
+// drivers that sequence the device kernels (Lanczos passes 1 and 2, Green
+// chains, c/c+ maps, continued fractions).
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "edk_internal.h"
+#include "edk_tables.h"
+#include "edk_tridiag.h"
+
+using namespace edk;
+
+// ---------------------------------------------------------------------------
+// device buffer helper
+// ---------------------------------------------------------------------------
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t ensure(size_t n) {
+        if (n <= bytes && p) return cudaSuccess;
+        release();
+        cudaError_t e = cudaMalloc(&p, n > 0 ? n : 16);
+        if (e == cudaSuccess) bytes = n;
+        return e;
+    }
+    template <typename T> T *as() const { return static_cast<T *>(p); }
+};
+
+template <typename T>
+cudaError_t upload(DevBuf &b, const std::vector<T> &v, cudaStream_t st)
+{
+    cudaError_t e = b.ensure(sizeof(T) * (v.empty() ? 1 : v.size()));
+    if (e != cudaSuccess || v.empty()) return e;
+    e = cudaMemcpyAsync(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(st);   // host vectors may go out of scope
+}
+
+std::vector<double> default_ran_tab()
+{
+    // splitmix64 seeded with 1234567, mapped to [0,1) and rounded to 3
+    // decimals half away from zero (the reference's ANINT, random.f90:80-91).
+    std::vector<double> t(10001);
+    uint64_t x = 1234567ull;
+    for (int i = 0; i < 10001; ++i) {
+        x += 0x9E3779B97F4A7C15ull;
+        uint64_t z = x;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z = z ^ (z >> 31);
+        const double u = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+        t[i] = std::floor(u * 1000.0 + 0.5) / 1000.0;
+    }
+    return t;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+struct edk_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int num_sms = 148;
+    std::string last_error;
+    int64_t launches = 0;
+    // reduction scratch (partials, counter, sums, flags) and Lanczos coefficients
+    DevBuf partials, counter, sums, flags, tri_diag, tri_sub, coef, ran_tab, ran_tab_user;
+    DevBuf cf_n, cf_diag, cf_sub, cf_e, cf_ph, cf_scale, cf_wn, cf_G, cf_flag;
+    size_t tri_cap = 0;
+    int reduce_grid = 0;
+    // optional event timing of row-kernel launches: (class, start, stop)
+    bool timing = false;
+    struct Timed { int cls; cudaEvent_t a, b; };
+    std::vector<Timed> timed;
+    std::vector<cudaEvent_t> event_pool;
+    int64_t t_count[8] = {0};
+    double t_ms[8] = {0};
+    cudaEvent_t get_event() {
+        if (!event_pool.empty()) { cudaEvent_t e = event_pool.back(); event_pool.pop_back(); return e; }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void drain_timing() {
+        for (auto &t : timed) {
+            float ms = 0.f;
+            if (cudaEventSynchronize(t.b) == cudaSuccess && cudaEventElapsedTime(&ms, t.a, t.b) == cudaSuccess) {
+                t_ms[t.cls] += ms;
+                t_count[t.cls] += 1;
+            }
+            event_pool.push_back(t.a);
+            event_pool.push_back(t.b);
+        }
+        timed.clear();
+    }
+    ~edk_ctx() {
+        drain_timing();
+        for (auto e : event_pool) cudaEventDestroy(e);
+    }
+
+    int fail(int code, const char *fmt, ...) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        last_error = buf;
+        return code;
+    }
+    int cuda(cudaError_t e, const char *where) {
+        if (e == cudaSuccess) return EDK_OK;
+        return fail(e == cudaErrorMemoryAllocation ? EDK_ERR_NOMEM : EDK_ERR_CUDA, "%s: %s", where,
+                    cudaGetErrorString(e));
+    }
+    int ensure_tri(size_t n) {
+        if (n <= tri_cap) return EDK_OK;
+        size_t cap = std::max<size_t>(n, 1024);
+        int rc = cuda(tri_diag.ensure(sizeof(double) * cap), "alloc tri");
+        if (rc) return rc;
+        rc = cuda(tri_sub.ensure(sizeof(double) * cap), "alloc tri");
+        if (rc) return rc;
+        rc = cuda(coef.ensure(sizeof(double) * cap), "alloc coef");
+        if (rc) return rc;
+        tri_cap = cap;
+        return EDK_OK;
+    }
+};
+
+namespace {
+
+int ctx_init(edk_ctx *c)
+{
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return c->cuda(e, "cudaSetDevice");
+    cudaDeviceProp prop;
+    e = cudaGetDeviceProperties(&prop, c->device);
+    if (e != cudaSuccess) return c->cuda(e, "cudaGetDeviceProperties");
+    c->num_sms = prop.multiProcessorCount;
+    c->reduce_grid = c->num_sms * 8;
+    int rc;
+    // the row kernel can use up to 2 blocks per SM of the reduction grid size
+    if ((rc = c->cuda(c->partials.ensure(sizeof(double) * 4 * (size_t)c->num_sms * 16), "alloc"))) return rc;
+    if ((rc = c->cuda(c->counter.ensure(64), "alloc"))) return rc;
+    if ((rc = c->cuda(c->sums.ensure(sizeof(double) * 16), "alloc"))) return rc;
+    if ((rc = c->cuda(c->flags.ensure(sizeof(int) * 16), "alloc"))) return rc;
+    if ((rc = c->cuda(cudaMemsetAsync(c->counter.p, 0, 64, c->stream), "memset"))) return rc;
+    if ((rc = c->cuda(cudaMemsetAsync(c->flags.p, 0, sizeof(int) * 16, c->stream), "memset"))) return rc;
+    if ((rc = c->cuda(upload(c->ran_tab, default_ran_tab(), c->stream), "upload ran_tab"))) return rc;
+    if ((rc = c->ensure_tri(1024))) return rc;
+    return EDK_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// sector Hamiltonian
+// ---------------------------------------------------------------------------
+struct edk_h {
+    edk_ctx *ctx = nullptr;
+    ModelHost model;
+    int nup = 0, ndn = 0;
+    int64_t dup = 0, ddn = 0, dim = 0;
+    SpinTableHost tab[2];
+    std::vector<int32_t> rank;
+    std::vector<int32_t> int_off;
+    std::vector<double> int_coef;
+    int hund = 0;
+    // device copies
+    struct SpinDev {
+        DevBuf ptr, tgt, val, valf, diag, diagf, imp, move, ell, ell_val, ell_valf, pal, palf;
+    } sd[2];
+    DevBuf int_off_d, int_coef_d, int_coeff_d, jj_d, jjf_d, umask_d, row_order_d;
+    HamDev H;
+    // Krylov workspace: v_{k-1}, v_k, s, s', psi (per element type)
+    DevBuf work[2][5];
+    // apply_c maps keyed by (spin, dagger, site)
+    struct CMap {
+        int spin, dagger, site;
+        int64_t dim_sigma_tgt;
+        DevBuf src, sg;
+    };
+    std::vector<std::unique_ptr<CMap>> cmaps;
+};
+
+namespace {
+
+int upload_spin(edk_h *h, int s)
+{
+    edk_ctx *c = h->ctx;
+    const SpinTableHost &t = h->tab[s];
+    auto &d = h->sd[s];
+    cudaStream_t st = c->stream;
+    std::vector<float> valf(t.val.begin(), t.val.end()), diagf(t.diag.begin(), t.diag.end());
+    std::vector<float> ellvf(t.ell_val.begin(), t.ell_val.end()), palf(t.palette.begin(), t.palette.end());
+    int rc;
+    if ((rc = c->cuda(upload(d.ptr, t.ptr, st), "upload ptr"))) return rc;
+    if ((rc = c->cuda(upload(d.tgt, t.tgt, st), "upload tgt"))) return rc;
+    if ((rc = c->cuda(upload(d.val, t.val, st), "upload val"))) return rc;
+    if ((rc = c->cuda(upload(d.valf, valf, st), "upload valf"))) return rc;
+    if ((rc = c->cuda(upload(d.diag, t.diag, st), "upload diag"))) return rc;
+    if ((rc = c->cuda(upload(d.diagf, diagf, st), "upload diagf"))) return rc;
+    if ((rc = c->cuda(upload(d.imp, t.imp, st), "upload imp"))) return rc;
+    if ((rc = c->cuda(upload(d.move, t.move, st), "upload move"))) return rc;
+    if ((rc = c->cuda(upload(d.ell, t.ell, st), "upload ell"))) return rc;
+    if ((rc = c->cuda(upload(d.ell_val, t.ell_val, st), "upload ell_val"))) return rc;
+    if ((rc = c->cuda(upload(d.ell_valf, ellvf, st), "upload ell_valf"))) return rc;
+    if ((rc = c->cuda(upload(d.pal, t.palette, st), "upload pal"))) return rc;
+    if ((rc = c->cuda(upload(d.palf, palf, st), "upload palf"))) return rc;
+    SpinTabDev &o = (s == 0) ? h->H.up : h->H.dn;
+    o.ptr = d.ptr.as<int32_t>();
+    o.tgt = d.tgt.as<int32_t>();
+    o.val = d.val.as<double>();
+    o.valf = d.valf.as<float>();
+    o.diag = d.diag.as<double>();
+    o.diagf = d.diagf.as<float>();
+    o.imp = d.imp.as<uint8_t>();
+    o.move = d.move.as<int32_t>();
+    o.ell_k = t.ell_k;
+    o.packed = t.packed ? 1 : 0;
+    o.npal = (int)t.palette.size();
+    o.ell = d.ell.as<uint32_t>();
+    o.ell_val = d.ell_val.as<double>();
+    o.ell_valf = d.ell_valf.as<float>();
+    o.pal = d.pal.as<double>();
+    o.palf = d.palf.as<float>();
+    return EDK_OK;
+}
+
+int check_model(edk_ctx *c, const edk_model *m)
+{
+    if (!m) return c->fail(EDK_ERR_INVALID, "null model");
+    if (m->nc < 1 || m->nc > kMaxNc) return c->fail(EDK_ERR_INVALID, "nc=%d outside [1,%d]", m->nc, kMaxNc);
+    if (m->nb < 0 || m->nc + m->nb > kMaxNs)
+        return c->fail(EDK_ERR_INVALID, "nc+nb=%d outside [1,%d]", m->nc + m->nb, kMaxNs);
+    if (!m->ec || !m->u || !m->jj || (m->nb > 0 && (!m->eb || !m->vbc)))
+        return c->fail(EDK_ERR_INVALID, "null model matrix");
+    // hermiticity of U (impurity_class.f90:839-840) and of the one-body blocks
+    for (int a = 0; a < m->nc; ++a)
+        for (int b = 0; b < m->nc; ++b) {
+            if (m->u[a * m->nc + b] != m->u[b * m->nc + a])
+                return c->fail(EDK_ERR_INVALID, "U is not symmetric");
+            for (int s = 0; s < 2; ++s)
+                if (m->ec[s * m->nc * m->nc + a * m->nc + b] != m->ec[s * m->nc * m->nc + b * m->nc + a])
+                    return c->fail(EDK_ERR_INVALID, "Ec is not symmetric");
+        }
+    for (int s = 0; s < 2; ++s)
+        for (int a = 0; a < m->nb; ++a)
+            for (int b = 0; b < m->nb; ++b)
+                if (m->eb[s * m->nb * m->nb + a * m->nb + b] != m->eb[s * m->nb * m->nb + b * m->nb + a])
+                    return c->fail(EDK_ERR_INVALID, "Eb is not symmetric");
+    const bool hund_possible = std::fabs(m->jhund) > 1e-5;
+    if (hund_possible && m->jhund < 0) return c->fail(EDK_ERR_INVALID, "negative Hund coupling");
+    return EDK_OK;
+}
+
+int work_ptrs(edk_h *h, int dtype, void *(&w)[5])
+{
+    const size_t es = dtype == EDK_F64 ? 8 : 4;
+    for (int i = 0; i < 5; ++i) {
+        int rc = h->ctx->cuda(h->work[dtype][i].ensure(es * (size_t)h->dim), "alloc Krylov workspace");
+        if (rc) return rc;
+        w[i] = h->work[dtype][i].p;
+    }
+    return EDK_OK;
+}
+
+RowArgs base_args(edk_h *h)
+{
+    RowArgs a;
+    edk_ctx *c = h->ctx;
+    a.partials = c->partials.as<double>();
+    a.counter = c->counter.as<unsigned>();
+    a.sums_out = c->sums.as<double>();
+    a.flags = c->flags.as<int>();
+    a.tri_diag = c->tri_diag.as<double>();
+    a.tri_sub = c->tri_sub.as<double>();
+    return a;
+}
+
+int rows(edk_h *h, int dtype, const RowArgs &a)
+{
+    edk_ctx *c = h->ctx;
+    LaunchCfg cfg = plan_rows(h->H, dtype == EDK_F64 ? 8 : 4, c->num_sms);
+    cudaEvent_t ea = nullptr, eb = nullptr;
+    if (c->timing) {
+        ea = c->get_event();
+        eb = c->get_event();
+        cudaEventRecord(ea, c->stream);
+    }
+    cudaError_t e = launch_rows(h->H, dtype, a, cfg, c->stream);
+    if (c->timing) {
+        cudaEventRecord(eb, c->stream);
+        c->timed.push_back({a.mode + (dtype == EDK_F32 ? 4 : 0), ea, eb});
+        if (c->timed.size() > 4096) c->drain_timing();
+    }
+    c->launches++;
+    return c->cuda(e, "row kernel");
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Krylov sequences on the device
+// ---------------------------------------------------------------------------
+namespace {
+
+// Buffers rotate through the steps: vbuf[0..1] hold v_{k-1}, v_k; sbuf[0..1]
+// alternate as gather source s_{k+1} and output s_{k+2}.
+struct Krylov {
+    edk_h *h;
+    int dtype;
+    void *w[5];
+    int ivk = 1, ivkm1 = 0, is = 2, is_out = 3;
+    int k = 0;     // iterations completed (T_k known)
+    const double *psi_coef = nullptr;
+    void *psi = nullptr;
+    double cutoff = 1e-25;
+};
+
+// v1 = start/|start| into w[1]; tri_sub[0] = |start|; psi = coef[0]*v1 when psi set
+int krylov_start(Krylov &K, const void *start_dev, const double *ran_tab_dev, double *norm_out)
+{
+    edk_h *h = K.h;
+    edk_ctx *c = h->ctx;
+    int rc;
+    rc = c->cuda(cudaMemsetAsync(c->flags.p, 0, sizeof(int) * 16, c->stream), "memset flags");
+    if (rc) return rc;
+    const int grid = c->reduce_grid;
+    rc = c->cuda(launch_start_vector(K.dtype, h->dim, ran_tab_dev, start_dev, K.w[K.ivk],
+                                     c->partials.as<double>(), c->counter.as<unsigned>(),
+                                     c->sums.as<double>(), grid, c->stream), "start vector");
+    c->launches++;
+    if (rc) return rc;
+    double nrm2 = 0.0;
+    rc = c->cuda(cudaMemcpyAsync(&nrm2, c->sums.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "d2h");
+    if (rc) return rc;
+    rc = c->cuda(cudaStreamSynchronize(c->stream), "sync");
+    if (rc) return rc;
+    if (norm_out) *norm_out = std::sqrt(nrm2);
+    if (!(std::sqrt(nrm2) >= K.cutoff)) return c->fail(EDK_ERR_ZERO_START, "start vector has zero norm");
+    rc = c->cuda(launch_scale(K.dtype, h->dim, K.w[K.ivk], c->sums.as<double>(), 0, K.psi, K.psi_coef,
+                              c->tri_sub.as<double>(), grid, c->stream), "scale");
+    c->launches++;
+    K.k = 0;
+    return rc;
+}
+
+// iteration k+1 of lanc_opt: k=0 -> H v1, else the fused step
+int krylov_step(Krylov &K)
+{
+    edk_h *h = K.h;
+    RowArgs a = base_args(h);
+    a.cutoff = K.cutoff;
+    if (K.k == 0) {
+        a.mode = kModeFirst;
+        a.x = K.w[K.ivk];
+        a.y = K.w[K.is];
+        int rc = rows(h, K.dtype, a);
+        if (rc) return rc;
+        K.k = 1;
+        return EDK_OK;
+    }
+    a.mode = kModeStep;
+    a.k = K.k;
+    a.x = K.w[K.is];
+    a.y = K.w[K.is_out];
+    a.vk = K.w[K.ivk];
+    a.vkm1 = (K.k >= 2) ? K.w[K.ivkm1] : nullptr;
+    a.vout = K.w[K.ivkm1];
+    a.psi = K.psi;
+    a.psi_coef = K.psi_coef;
+    int rc = rows(h, K.dtype, a);
+    if (rc) return rc;
+    std::swap(K.ivk, K.ivkm1);      // v_{k+1} now in the old v_{k-1} slot
+    std::swap(K.is, K.is_out);
+    K.k += 1;
+    return EDK_OK;
+}
+
+struct TriHost {
+    std::vector<double> diag, sub;
+    int flags[2] = {0, 0};
+};
+
+int fetch_tri(edk_ctx *c, int n, TriHost &t)
+{
+    t.diag.resize(n + 1);
+    t.sub.resize(n + 2);
+    int rc = c->cuda(cudaMemcpyAsync(t.diag.data(), c->tri_diag.p, sizeof(double) * (n + 1),
+                                     cudaMemcpyDeviceToHost, c->stream), "d2h tri");
+    if (rc) return rc;
+    rc = c->cuda(cudaMemcpyAsync(t.sub.data(), c->tri_sub.p, sizeof(double) * (n + 2),
+                                 cudaMemcpyDeviceToHost, c->stream), "d2h tri");
+    if (rc) return rc;
+    rc = c->cuda(cudaMemcpyAsync(t.flags, c->flags.p, sizeof(int) * 2, cudaMemcpyDeviceToHost,
+                                 c->stream), "d2h flags");
+    if (rc) return rc;
+    return c->cuda(cudaStreamSynchronize(c->stream), "sync");
+}
+
+const double *ran_tab_for(edk_ctx *c, const double *user_tab, int *rc)
+{
+    *rc = EDK_OK;
+    if (!user_tab) return c->ran_tab.as<double>();
+    std::vector<double> t(user_tab, user_tab + 10001);
+    *rc = c->cuda(upload(c->ran_tab_user, t, c->stream), "upload ran_tab");
+    return c->ran_tab_user.as<double>();
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C-ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int64_t edk_binom(int n, int k) { return binom(n, k); }
+
+int edk_basis(int ns, int npart, uint64_t *states_host)
+{
+    if (ns < 0 || ns > kMaxNs || npart < 0 || npart > ns || !states_host) return EDK_ERR_INVALID;
+    auto s = enumerate_states(ns, npart);
+    std::memcpy(states_host, s.data(), sizeof(uint64_t) * s.size());
+    return EDK_OK;
+}
+
+int edk_rank_table(int ns, int32_t *rank_host)
+{
+    if (ns < 0 || ns > kMaxNs || !rank_host) return EDK_ERR_INVALID;
+    auto r = rank_table(ns);
+    std::memcpy(rank_host, r.data(), sizeof(int32_t) * r.size());
+    return EDK_OK;
+}
+
+int edk_default_ran_tab(double *tab_host)
+{
+    if (!tab_host) return EDK_ERR_INVALID;
+    const auto t = default_ran_tab();
+    std::memcpy(tab_host, t.data(), sizeof(double) * t.size());
+    return EDK_OK;
+}
+
+int edk_build_table(const edk_model *m, int spin, int npart, int64_t *dim, int64_t *nnz,
+                    int64_t *ptr_host, int32_t *tgt_host, double *val_host, double *diag_host)
+{
+    edk_ctx tmp;
+    if (check_model(&tmp, m) || spin < 0 || spin > 1) return EDK_ERR_INVALID;
+    const int ns = m->nc + m->nb;
+    if (npart < 0 || npart > ns) return EDK_ERR_INVALID;
+    ModelHost mh;
+    mh.nc = m->nc;
+    mh.nb = m->nb;
+    mh.ec.assign(m->ec, m->ec + 2 * m->nc * m->nc);
+    if (m->nb > 0) {
+        mh.eb.assign(m->eb, m->eb + 2 * m->nb * m->nb);
+        mh.vbc.assign(m->vbc, m->vbc + 2 * m->nb * m->nc);
+    }
+    mh.u.assign(m->u, m->u + m->nc * m->nc);
+    mh.jj.assign(m->jj, m->jj + m->nc * m->nc);
+    mh.jhund = m->jhund;
+    mh.cutoff = m->cutoff_hamilt_param;
+    const auto rank = rank_table(ns);
+    const SpinTableHost t = build_spin_table(mh, spin, npart, rank);
+    if (dim) *dim = (int64_t)t.states.size();
+    if (nnz) *nnz = (int64_t)t.tgt.size();
+    if (ptr_host)
+        for (size_t i = 0; i < t.ptr.size(); ++i) ptr_host[i] = t.ptr[i];
+    if (tgt_host) std::memcpy(tgt_host, t.tgt.data(), sizeof(int32_t) * t.tgt.size());
+    if (val_host) std::memcpy(val_host, t.val.data(), sizeof(double) * t.val.size());
+    if (diag_host) std::memcpy(diag_host, t.diag.data(), sizeof(double) * t.diag.size());
+    return EDK_OK;
+}
+
+int edk_ctx_create(int device, void *stream, edk_ctx **out)
+{
+    if (!out) return EDK_ERR_INVALID;
+    auto *c = new (std::nothrow) edk_ctx;
+    if (!c) return EDK_ERR_NOMEM;
+    c->device = device;
+    c->stream = static_cast<cudaStream_t>(stream);
+    int rc = ctx_init(c);
+    if (rc) {
+        delete c;
+        *out = nullptr;
+        return rc;
+    }
+    *out = c;
+    return EDK_OK;
+}
+
+int edk_ctx_destroy(edk_ctx *ctx)
+{
+    if (!ctx) return EDK_OK;
+    cudaStreamSynchronize(ctx->stream);
+    delete ctx;
+    return EDK_OK;
+}
+
+int edk_ctx_set_stream(edk_ctx *ctx, void *stream)
+{
+    if (!ctx) return EDK_ERR_INVALID;
+    ctx->stream = static_cast<cudaStream_t>(stream);
+    return EDK_OK;
+}
+
+const char *edk_ctx_last_error(const edk_ctx *ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+int64_t edk_ctx_launch_count(const edk_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+int edk_ctx_timing(edk_ctx *ctx, int enable)
+{
+    if (!ctx) return EDK_ERR_INVALID;
+    if (enable && !ctx->timing) {
+        ctx->drain_timing();
+        for (int i = 0; i < 8; ++i) { ctx->t_count[i] = 0; ctx->t_ms[i] = 0.0; }
+    }
+    ctx->timing = enable != 0;
+    return EDK_OK;
+}
+
+int edk_ctx_timing_report(edk_ctx *ctx, int which, int64_t *launches, double *total_ms)
+{
+    if (!ctx || which < 0 || which > 7) return EDK_ERR_INVALID;
+    ctx->drain_timing();
+    if (launches) *launches = ctx->t_count[which];
+    if (total_ms) *total_ms = ctx->t_ms[which];
+    return EDK_OK;
+}
+
+int edk_h_create(edk_ctx *ctx, const edk_model *m, int nup, int ndn, edk_h **out)
+{
+    if (!ctx || !out) return EDK_ERR_INVALID;
+    *out = nullptr;
+    int rc = check_model(ctx, m);
+    if (rc) return rc;
+    const int ns = m->nc + m->nb;
+    if (nup < 0 || nup > ns || ndn < 0 || ndn > ns)
+        return ctx->fail(EDK_ERR_INVALID, "sector (%d,%d) outside [0,%d]", nup, ndn, ns);
+    std::unique_ptr<edk_h> h(new (std::nothrow) edk_h);
+    if (!h) return EDK_ERR_NOMEM;
+    h->ctx = ctx;
+    ModelHost &mh = h->model;
+    mh.nc = m->nc;
+    mh.nb = m->nb;
+    mh.ec.assign(m->ec, m->ec + 2 * m->nc * m->nc);
+    mh.eb.assign(m->eb ? m->eb : m->ec, (m->eb ? m->eb : m->ec) + 2 * m->nb * m->nb);
+    mh.vbc.assign(m->vbc ? m->vbc : m->ec, (m->vbc ? m->vbc : m->ec) + 2 * m->nb * m->nc);
+    mh.u.assign(m->u, m->u + m->nc * m->nc);
+    mh.jj.assign(m->jj, m->jj + m->nc * m->nc);
+    mh.jhund = m->jhund;
+    mh.cutoff = m->cutoff_hamilt_param;
+    h->nup = nup;
+    h->ndn = ndn;
+    h->rank = rank_table(ns);
+    h->tab[0] = build_spin_table(mh, 0, nup, h->rank);
+    h->tab[1] = build_spin_table(mh, 1, ndn, h->rank);
+    h->dup = (int64_t)h->tab[0].states.size();
+    h->ddn = (int64_t)h->tab[1].states.size();
+    h->dim = h->dup * h->ddn;
+    if (h->dup >= (1ll << 31) || h->ddn >= (1ll << 31))
+        return ctx->fail(EDK_ERR_UNSUPPORTED, "spin sector dimension beyond 2^31");
+    density_terms(mh, h->int_off, h->int_coef);
+    bool offc = false;
+    for (int a = 0; a < mh.nc; ++a)
+        for (int b = 0; b < mh.nc; ++b)
+            if (a != b && mh.u[a * mh.nc + b] != 0.0) offc = true;
+    h->hund = (std::fabs(mh.jhund) > 1e-5 && offc) ? 1 : 0;
+    // device copies
+    if ((rc = upload_spin(h.get(), 0))) return rc;
+    if ((rc = upload_spin(h.get(), 1))) return rc;
+    cudaStream_t st = ctx->stream;
+    std::vector<float> icf(h->int_coef.begin(), h->int_coef.end()), jjf(mh.jj.begin(), mh.jj.end());
+    std::vector<uint8_t> umask(mh.nc * mh.nc);
+    for (int i = 0; i < mh.nc * mh.nc; ++i) umask[i] = mh.u[i] != 0.0;
+    auto order = row_schedule(h->tab[1].states, mh.nc, mh.nb);
+    if ((rc = ctx->cuda(upload(h->int_off_d, h->int_off, st), "upload"))) return rc;
+    if ((rc = ctx->cuda(upload(h->int_coef_d, h->int_coef, st), "upload"))) return rc;
+    if ((rc = ctx->cuda(upload(h->int_coeff_d, icf, st), "upload"))) return rc;
+    if ((rc = ctx->cuda(upload(h->jj_d, mh.jj, st), "upload"))) return rc;
+    if ((rc = ctx->cuda(upload(h->jjf_d, jjf, st), "upload"))) return rc;
+    if ((rc = ctx->cuda(upload(h->umask_d, umask, st), "upload"))) return rc;
+    if ((rc = ctx->cuda(upload(h->row_order_d, order, st), "upload"))) return rc;
+    HamDev &H = h->H;
+    H.dup = h->dup;
+    H.ddn = h->ddn;
+    H.nc = mh.nc;
+    H.nmove = mh.nc * (mh.nc - 1);
+    H.hund = h->hund;
+    H.ncfg = 1 << mh.nc;
+    H.int_off = h->int_off_d.as<int32_t>();
+    H.int_coef = h->int_coef_d.as<double>();
+    H.int_coeff = h->int_coeff_d.as<float>();
+    H.jj = h->jj_d.as<double>();
+    H.jjf = h->jjf_d.as<float>();
+    H.umask = h->umask_d.as<uint8_t>();
+    H.row_order = h->row_order_d.as<int32_t>();
+    *out = h.release();
+    return EDK_OK;
+}
+
+int edk_h_destroy(edk_h *h)
+{
+    if (!h) return EDK_OK;
+    cudaStreamSynchronize(h->ctx->stream);
+    delete h;
+    return EDK_OK;
+}
+
+int edk_h_dims(const edk_h *h, int64_t *dim, int64_t *dim_up, int64_t *dim_dn)
+{
+    if (!h) return EDK_ERR_INVALID;
+    if (dim) *dim = h->dim;
+    if (dim_up) *dim_up = h->dup;
+    if (dim_dn) *dim_dn = h->ddn;
+    return EDK_OK;
+}
+
+int edk_h_table(const edk_h *h, int spin, int64_t *nnz, int64_t *ptr_host, int32_t *tgt_host,
+                double *val_host, double *diag_host)
+{
+    if (!h || spin < 0 || spin > 1) return EDK_ERR_INVALID;
+    const SpinTableHost &t = h->tab[spin];
+    if (nnz) *nnz = (int64_t)t.tgt.size();
+    if (ptr_host)
+        for (size_t i = 0; i < t.ptr.size(); ++i) ptr_host[i] = t.ptr[i];
+    if (tgt_host) std::memcpy(tgt_host, t.tgt.data(), sizeof(int32_t) * t.tgt.size());
+    if (val_host) std::memcpy(val_host, t.val.data(), sizeof(double) * t.val.size());
+    if (diag_host) std::memcpy(diag_host, t.diag.data(), sizeof(double) * t.diag.size());
+    return EDK_OK;
+}
+
+int edk_hmult(edk_h *h, int dtype, int64_t n, const void *x_dev, void *y_dev)
+{
+    if (!h || !x_dev || !y_dev || (dtype != EDK_F64 && dtype != EDK_F32)) return EDK_ERR_INVALID;
+    if (n != h->dim) return h->ctx->fail(EDK_ERR_INVALID, "n=%lld differs from the sector dimension %lld",
+                                         (long long)n, (long long)h->dim);
+    if (x_dev == y_dev) return h->ctx->fail(EDK_ERR_INVALID, "x and y must not alias");
+    RowArgs a = base_args(h);
+    a.mode = kModeHv;
+    a.x = x_dev;
+    a.y = y_dev;
+    return rows(h, dtype, a);
+}
+
+int edk_hmult_host(edk_h *h, int dtype, int64_t n, const void *x_host, void *y_host)
+{
+    if (!h || !x_host || !y_host) return EDK_ERR_INVALID;
+    if (n != h->dim) return h->ctx->fail(EDK_ERR_INVALID, "n differs from the sector dimension");
+    void *w[5];
+    int rc = work_ptrs(h, dtype, w);
+    if (rc) return rc;
+    edk_ctx *c = h->ctx;
+    const size_t bytes = (size_t)n * (dtype == EDK_F64 ? 8 : 4);
+    if ((rc = c->cuda(cudaMemcpyAsync(w[0], x_host, bytes, cudaMemcpyHostToDevice, c->stream), "h2d"))) return rc;
+    if ((rc = edk_hmult(h, dtype, n, w[0], w[1]))) return rc;
+    if ((rc = c->cuda(cudaMemcpyAsync(y_host, w[1], bytes, cudaMemcpyDeviceToHost, c->stream), "d2h"))) return rc;
+    return c->cuda(cudaStreamSynchronize(c->stream), "sync");
+}
+
+int edk_lanczos_e0(edk_h *h, const edk_lanczos_opts *o, edk_lanczos_result *r)
+{
+    if (!h || !o || !r || !r->diag || !r->subdiag || !r->vecp) return EDK_ERR_INVALID;
+    edk_ctx *c = h->ctx;
+    if (o->dtype != EDK_F64 && o->dtype != EDK_F32) return c->fail(EDK_ERR_INVALID, "dtype");
+    if (o->neigen < 1 || o->neigen > 64) return c->fail(EDK_ERR_INVALID, "neigen outside [1,64]");
+    if (h->dim < 2) return c->fail(EDK_ERR_INVALID, "Lanczos needs dim >= 2 (dense ED below FULL_ED_SWITCH)");
+    const int niter_max = (int)std::min<int64_t>(h->dim - 1, o->nitermax);
+    if (niter_max < 1) return c->fail(EDK_ERR_INVALID, "nitermax < 1");
+    int ne = (int)std::min<int64_t>(std::min<int64_t>(o->neigen, h->dim), niter_max);
+    int rc = c->ensure_tri((size_t)niter_max + 4);
+    if (rc) return rc;
+    Krylov K{h, o->dtype};
+    if ((rc = work_ptrs(h, o->dtype, K.w))) return rc;
+    K.cutoff = o->cutoff_min_lanczos_vec > 0 ? o->cutoff_min_lanczos_vec : 1e-25;
+    const double *tab = ran_tab_for(c, o->ran_tab, &rc);
+    if (rc) return rc;
+    if ((rc = krylov_start(K, o->start_dev, tab, nullptr))) return rc;
+    const int every = std::max(1, o->check_every);
+    std::vector<double> last(ne, 1e300), valp(ne), rdist(ne);
+    std::vector<int> conv(ne, 0);
+    TriHost T;
+    int checked = 0, stop_at = 0, status = EDK_OK;
+    while (!stop_at) {
+        const int target = std::min(niter_max, K.k + every);
+        while (K.k < target)
+            if ((rc = krylov_step(K))) return rc;
+        if ((rc = fetch_tri(c, K.k, T))) return rc;
+        if (T.flags[1]) return c->fail(EDK_ERR_NOT_FINITE, "non-finite Lanczos coefficient");
+        for (int it = checked + 1; it <= K.k; ++it) {
+            const int m = std::min(ne, it);
+            tridiag_lowest(it, T.diag.data(), T.sub.data() + 1, m, valp.data());
+            bool all = true;
+            for (int j = 0; j < ne; ++j) {
+                if (j < m) {
+                    rdist[j] = valp[j] - last[j];
+                    conv[j] = (std::fabs(rdist[j]) < o->tolerance) && it > 2;
+                }
+                if (!(j < m && conv[j])) all = false;
+            }
+            const bool broke = !(T.sub[it] >= K.cutoff);
+            if (all || it == niter_max || broke) {
+                stop_at = it;
+                if (broke && !all && it < niter_max) status = EDK_KRYLOV_EXHAUSTED;
+                break;
+            }
+            for (int j = 0; j < m; ++j) last[j] = valp[j];
+        }
+        checked = K.k;
+        if (!stop_at && K.k >= niter_max) stop_at = niter_max;
+    }
+    // eigenpairs of T_{stop_at}
+    const int n = stop_at;
+    const int m = std::min(ne, n);
+    std::vector<double> w(m), vecs((size_t)m * n);
+    tridiag_lowest(n, T.diag.data(), T.sub.data() + 1, m, w.data());
+    int kept = 0;
+    for (int j = 0; j < m; ++j) {
+        const bool inwin = w[j] >= w[0] && w[j] <= w[0] + o->demax;
+        if (!(j == 0 || (conv[j] && inwin))) continue;
+        std::vector<double> v(n);
+        // orthogonalise against kept vectors of nearby eigenvalues only
+        std::vector<double> prev;
+        int np = 0;
+        for (int q = 0; q < kept; ++q)
+            if (std::fabs(r->E[q] - w[j]) < 1e-8 * std::max(1.0, std::fabs(w[j]))) {
+                prev.insert(prev.end(), r->vecp + (size_t)q * n, r->vecp + (size_t)(q + 1) * n);
+                ++np;
+            }
+        tridiag_vector(n, T.diag.data(), T.sub.data() + 1, w[j], prev.data(), np, v.data());
+        r->E[kept] = w[j];
+        r->converged[kept] = conv[j];
+        std::memcpy(r->vecp + (size_t)kept * n, v.data(), sizeof(double) * n);
+        ++kept;
+    }
+    r->nkept = kept;
+    r->niter = n;
+    r->status = status;
+    std::memcpy(r->diag, T.diag.data(), sizeof(double) * n);
+    std::memcpy(r->subdiag, T.sub.data(), sizeof(double) * (n + 1));
+    return EDK_OK;
+}
+
+int edk_lanczos_gs(edk_h *h, const edk_lanczos_opts *o, int32_t niter, const double *coef_host, void *psi_dev)
+{
+    if (!h || !o || !coef_host || !psi_dev || niter < 1) return EDK_ERR_INVALID;
+    edk_ctx *c = h->ctx;
+    int rc = c->ensure_tri((size_t)niter + 4);
+    if (rc) return rc;
+    Krylov K{h, o->dtype};
+    if ((rc = work_ptrs(h, o->dtype, K.w))) return rc;
+    K.cutoff = o->cutoff_min_lanczos_vec > 0 ? o->cutoff_min_lanczos_vec : 1e-25;
+    std::vector<double> cf(coef_host, coef_host + niter);
+    cf.push_back(0.0);
+    if ((rc = c->cuda(cudaMemcpyAsync(c->coef.p, cf.data(), sizeof(double) * cf.size(),
+                                      cudaMemcpyHostToDevice, c->stream), "h2d coef"))) return rc;
+    K.psi = psi_dev;
+    K.psi_coef = c->coef.as<double>();
+    const double *tab = ran_tab_for(c, o->ran_tab, &rc);
+    if (rc) return rc;
+    if ((rc = krylov_start(K, o->start_dev, tab, nullptr))) return rc;
+    // iterations 1..niter-1 produce v_2..v_niter (the last H*v is not needed
+    // by the eigenvector but keeps one kernel for every step)
+    while (K.k < niter)
+        if ((rc = krylov_step(K))) return rc;
+    if (niter == 1) {
+        // nothing beyond psi = coef[0] v1
+    }
+    // normalise psi
+    if ((rc = c->cuda(launch_norm2(o->dtype, h->dim, psi_dev, c->partials.as<double>(),
+                                   c->counter.as<unsigned>(), c->sums.as<double>() + 8, c->reduce_grid,
+                                   c->stream), "norm2"))) return rc;
+    c->launches++;
+    rc = c->cuda(launch_scale(o->dtype, h->dim, psi_dev, c->sums.as<double>() + 8, 0, nullptr, nullptr,
+                              nullptr, c->reduce_grid, c->stream), "scale");
+    c->launches++;
+    if (rc) return rc;
+    return c->cuda(cudaStreamSynchronize(c->stream), "sync");
+}
+
+int edk_apply_c(edk_h *src, int dtype, int site, int spin, int dagger, int site2, int sign2,
+                const void *in_dev, void *out_dev, int64_t *out_dim)
+{
+    if (!src || !in_dev || !out_dev || spin < 0 || spin > 1) return EDK_ERR_INVALID;
+    edk_ctx *c = src->ctx;
+    const ModelHost &m = src->model;
+    if (site < 0 || site >= m.nc || site2 >= m.nc) return c->fail(EDK_ERR_INVALID, "site outside impurity");
+    const int ns = m.nc + m.nb;
+    const int np = spin == 0 ? src->nup : src->ndn;
+    const int npt = np + (dagger ? 1 : -1);
+    if (npt < 0 || npt > ns) return c->fail(EDK_ERR_INVALID, "target sector outside [0,ns]");
+    const int64_t dsig_t = binom(ns, npt);
+    const int64_t dother = spin == 0 ? src->ddn : src->dup;
+    if (out_dim) *out_dim = dsig_t * dother;
+    // inverse maps: for each target state the source state and sign
+    auto get_map = [&](int st_site, edk_h::CMap **mp) -> int {
+        for (auto &cm : src->cmaps)
+            if (cm->spin == spin && cm->dagger == dagger && cm->site == st_site) { *mp = cm.get(); return EDK_OK; }
+        std::unique_ptr<edk_h::CMap> cm(new edk_h::CMap);
+        cm->spin = spin;
+        cm->dagger = dagger;
+        cm->site = st_site;
+        cm->dim_sigma_tgt = dsig_t;
+        std::vector<int32_t> srcmap((size_t)dsig_t, -1);
+        std::vector<int8_t> sg((size_t)dsig_t, 0);
+        const auto &states = src->tab[spin].states;
+        const int bit = m.nb + st_site;
+        for (size_t i = 0; i < states.size(); ++i) {
+            const uint64_t s = states[i];
+            const bool occ = (s >> bit) & 1ull;
+            if (dagger == occ) continue;                     // nil ket
+            const uint64_t o = s ^ (1ull << bit);
+            // create/destroy sign: occupied orbitals above the bit (apply_C.f90:566-581)
+            const int sign = (__builtin_popcountll(o >> (bit + 1)) & 1) ? -1 : 1;
+            const int32_t j = src->rank[o];
+            srcmap[j] = (int32_t)i;
+            sg[j] = (int8_t)sign;
+        }
+        int rc2 = c->cuda(upload(cm->src, srcmap, c->stream), "upload cmap");
+        if (rc2) return rc2;
+        rc2 = c->cuda(upload(cm->sg, sg, c->stream), "upload cmap");
+        if (rc2) return rc2;
+        *mp = cm.get();
+        src->cmaps.push_back(std::move(cm));
+        return EDK_OK;
+    };
+    edk_h::CMap *m1 = nullptr, *m2 = nullptr;
+    int rc = get_map(site, &m1);
+    if (rc) return rc;
+    if (site2 >= 0) {
+        if ((rc = get_map(site2, &m2))) return rc;
+    }
+    const int64_t dup_src = src->dup;
+    const int64_t dup_tgt = spin == 0 ? dsig_t : src->dup;
+    rc = c->cuda(launch_apply_c(dtype, spin, dother, dup_src, dup_tgt, dsig_t, m1->src.as<int32_t>(),
+                                m1->sg.as<int8_t>(), m2 ? m2->src.as<int32_t>() : nullptr,
+                                m2 ? m2->sg.as<int8_t>() : nullptr, sign2 < 0 ? -1 : 1, in_dev, out_dev,
+                                c->stream),
+                 "apply_c");
+    c->launches++;
+    return rc;
+}
+
+int edk_green_chain(edk_h *t, int dtype, const void *start_dev, int32_t nitergreen, double e0, int iph,
+                    int32_t nw, const double *wn_host, double cutoff_dynamic, double *G_host,
+                    double *diag_host, double *subdiag_host, int32_t *niter_done)
+{
+    if (!t || !start_dev || !wn_host || !G_host || nw < 1 || (iph != 1 && iph != 2)) return EDK_ERR_INVALID;
+    edk_ctx *c = t->ctx;
+    const int niter = (int)std::min<int64_t>(nitergreen, t->dim);
+    if (niter < 1) return c->fail(EDK_ERR_INVALID, "nitergreen < 1");
+    int rc = c->ensure_tri((size_t)niter + 4);
+    if (rc) return rc;
+    Krylov K{t, dtype};
+    if ((rc = work_ptrs(t, dtype, K.w))) return rc;
+    double nrm = 0.0;
+    // the start vector is copied into the workspace and normalised there
+    rc = krylov_start(K, start_dev, nullptr, &nrm);
+    std::memset(G_host, 0, sizeof(double) * 2 * nw);
+    if (niter_done) *niter_done = 0;
+    if (rc == EDK_ERR_ZERO_START || nrm * nrm < cutoff_dynamic) {
+        c->last_error.clear();
+        return EDK_OK;
+    }
+    if (rc) return rc;
+    while (K.k < niter)
+        if ((rc = krylov_step(K))) return rc;
+    TriHost T;
+    if ((rc = fetch_tri(c, K.k, T))) return rc;
+    if (T.flags[1]) return c->fail(EDK_ERR_NOT_FINITE, "non-finite Lanczos coefficient");
+    int n = niter;
+    for (int it = 1; it < niter; ++it)
+        if (!(T.sub[it] >= K.cutoff)) { n = it; break; }
+    if (niter_done) *niter_done = n;
+    if (diag_host) std::memcpy(diag_host, T.diag.data(), sizeof(double) * n);
+    if (subdiag_host) std::memcpy(subdiag_host, T.sub.data(), sizeof(double) * n);
+    const double ph = iph == 1 ? 1.0 : -1.0;
+    const double scale = nrm * nrm;
+    int32_t nn = n;
+    return edk_cf_eval(c, 1, n, &nn, T.diag.data(), T.sub.data(), &e0, &ph, &scale, nw, wn_host, G_host);
+}
+
+int edk_cf_eval(edk_ctx *c, int32_t nchain, int32_t ld, const int32_t *n_host, const double *diag_host,
+                const double *subdiag_host, const double *e_host, const double *ph_host,
+                const double *scale_host, int32_t nw, const double *wn_host, double *G_host)
+{
+    if (!c || nchain < 1 || ld < 1 || nw < 1 || !n_host || !diag_host || !subdiag_host || !G_host)
+        return EDK_ERR_INVALID;
+    for (int i = 0; i < nchain; ++i)
+        if (n_host[i] < 0 || n_host[i] > ld) return c->fail(EDK_ERR_INVALID, "chain length outside [0,ld]");
+    cudaStream_t st = c->stream;
+    int rc;
+    auto up = [&](DevBuf &b, const void *src, size_t bytes) {
+        int r2 = c->cuda(b.ensure(bytes), "alloc cf");
+        if (r2) return r2;
+        return c->cuda(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, st), "h2d cf");
+    };
+    if ((rc = up(c->cf_n, n_host, sizeof(int32_t) * nchain))) return rc;
+    if ((rc = up(c->cf_diag, diag_host, sizeof(double) * (size_t)nchain * ld))) return rc;
+    if ((rc = up(c->cf_sub, subdiag_host, sizeof(double) * (size_t)nchain * ld))) return rc;
+    if ((rc = up(c->cf_e, e_host, sizeof(double) * nchain))) return rc;
+    if ((rc = up(c->cf_ph, ph_host, sizeof(double) * nchain))) return rc;
+    if ((rc = up(c->cf_scale, scale_host, sizeof(double) * nchain))) return rc;
+    if ((rc = up(c->cf_wn, wn_host, sizeof(double) * nw))) return rc;
+    if ((rc = c->cuda(c->cf_G.ensure(sizeof(double) * 2 * (size_t)nchain * nw), "alloc"))) return rc;
+    if ((rc = c->cuda(c->cf_flag.ensure(sizeof(int)), "alloc"))) return rc;
+    if ((rc = c->cuda(cudaMemsetAsync(c->cf_flag.p, 0, sizeof(int), st), "memset"))) return rc;
+    rc = c->cuda(launch_cf(nchain, ld, c->cf_n.as<int32_t>(), c->cf_diag.as<double>(), c->cf_sub.as<double>(),
+                           c->cf_e.as<double>(), c->cf_ph.as<double>(), c->cf_scale.as<double>(), nw,
+                           c->cf_wn.as<double>(), c->cf_G.as<double>(), c->cf_flag.as<int>(), st), "cf");
+    c->launches++;
+    if (rc) return rc;
+    int flag = 0;
+    if ((rc = c->cuda(cudaMemcpyAsync(G_host, c->cf_G.p, sizeof(double) * 2 * (size_t)nchain * nw,
+                                      cudaMemcpyDeviceToHost, st), "d2h"))) return rc;
+    if ((rc = c->cuda(cudaMemcpyAsync(&flag, c->cf_flag.p, sizeof(int), cudaMemcpyDeviceToHost, st), "d2h"))) return rc;
+    if ((rc = c->cuda(cudaStreamSynchronize(st), "sync"))) return rc;
+    if (flag) return c->fail(EDK_ERR_CF_ZERO_DEN, "zero denominator in the continued fraction");
+    return EDK_OK;
+}
+
+int edk_double_occ(edk_h *h, int dtype, const void *psi_dev, int site, double *docc, double *norm2)
+{
+    if (!h || !psi_dev || site < 0 || site >= h->model.nc) return EDK_ERR_INVALID;
+    edk_ctx *c = h->ctx;
+    int rc = c->cuda(launch_double_occ(dtype, h->H, 1 << site, 1 << site, psi_dev, c->partials.as<double>(),
+                                       c->counter.as<unsigned>(), c->sums.as<double>() + 4, c->reduce_grid,
+                                       c->stream), "double occ");
+    c->launches++;
+    if (rc) return rc;
+    double s[2];
+    if ((rc = c->cuda(cudaMemcpyAsync(s, c->sums.as<double>() + 4, sizeof s, cudaMemcpyDeviceToHost,
+                                      c->stream), "d2h"))) return rc;
+    if ((rc = c->cuda(cudaStreamSynchronize(c->stream), "sync"))) return rc;
+    if (docc) *docc = s[0];
+    if (norm2) *norm2 = s[1];
+    return EDK_OK;
+}
+
+int edk_residual(edk_h *h, const void *psi_dev, double e, double *res_norm, double *psi_norm)
+{
+    if (!h || !psi_dev) return EDK_ERR_INVALID;
+    edk_ctx *c = h->ctx;
+    RowArgs a = base_args(h);
+    a.mode = kModeResid;
+    a.x = psi_dev;
+    a.eshift = e;
+    int rc = rows(h, EDK_F64, a);
+    if (rc) return rc;
+    double s[4];
+    if ((rc = c->cuda(cudaMemcpyAsync(s, c->sums.p, sizeof s, cudaMemcpyDeviceToHost, c->stream), "d2h"))) return rc;
+    if ((rc = c->cuda(cudaStreamSynchronize(c->stream), "sync"))) return rc;
+    if (res_norm) *res_norm = std::sqrt(s[0]);
+    if (psi_norm) *psi_norm = std::sqrt(s[2]);
+    return EDK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,121 @@
+// Internal structures shared by the host orchestration (edk_host.cpp) and the
+// device kernels (edk_kernels.cu).  Not part of the public C-ABI.
+#pragma once
+
+#include <cstdint>
+#include <cstddef>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "../../include/edk.h"
+
+namespace edk {
+
+constexpr int kMaxNc = 6;        // impurity sites per spin species
+constexpr int kMaxNs = 30;       // orbitals per spin species
+constexpr int kMaxSmemBytes = 220 * 1024;
+
+// One spin species' table on the device (tab_HAIM2 output, HAIM_offdiag_arrays.f90:210-606).
+struct SpinTabDev {
+    const int32_t *ptr = nullptr;    // dim+1 CSR offsets
+    const int32_t *tgt = nullptr;    // nnz, 0-based target rank
+    const double *val = nullptr;     // nnz
+    const float *valf = nullptr;
+    const double *diag = nullptr;    // dim
+    const float *diagf = nullptr;
+    const uint8_t *imp = nullptr;    // dim: occupation bits of the impurity sites
+    const int32_t *move = nullptr;   // dim * nmove: (rank+1)*sign of moving one
+                                     // electron between impurity sites, 0 if none
+    // Column-major padded copy of the same table (entry k of state c at
+    // k*dim + c), used for the up-spin gathers: packed = 24-bit target rank |
+    // 8-bit palette index, or plain int32 target + value when the table has
+    // more than 256 distinct values.  Padding entries point at the state
+    // itself with value 0 (palette slot 0 holds +0.0).
+    int ell_k = 0;
+    int packed = 0;
+    int npal = 0;
+    const uint32_t *ell = nullptr;
+    const double *ell_val = nullptr;
+    const float *ell_valf = nullptr;
+    const double *pal = nullptr;      // npal <= 256
+    const float *palf = nullptr;
+};
+
+// Everything a row kernel needs to evaluate (H x) for an element.
+struct HamDev {
+    int64_t dup = 0, ddn = 0;
+    int nc = 0, nmove = 0;
+    int hund = 0;                      // spin flip / pair hopping active
+    int ncfg = 0;                      // 1 << nc
+    SpinTabDev up, dn;
+    const int32_t *int_off = nullptr;  // ncfg*ncfg+1 offsets into the coefficient lists
+    const double *int_coef = nullptr;  // per (cfg_up, cfg_dn): the ordered density terms
+    const float *int_coeff = nullptr;
+    const double *jj = nullptr;        // nc*nc (device)
+    const float *jjf = nullptr;
+    const uint8_t *umask = nullptr;    // nc*nc
+    const int32_t *row_order = nullptr;  // ddn: schedule of rows for L2 reuse
+};
+
+enum RowMode : int {
+    kModeHv = 0,       // y = H x
+    kModeFirst = 1,    // Lanczos step 1: w = H v1, sums for alpha_1, beta_2
+    kModeStep = 2,     // Lanczos step k+1 from s_{k+1} = w_k (see edk_kernels.cu)
+    kModeResid = 3,    // sums |Hx - e x|^2, |x|^2
+};
+
+// Arguments of the fused row kernel (raw pointers, element type erased).
+struct RowArgs {
+    int mode = kModeHv;
+    const void *x = nullptr;       // gather source (x / v1 / s_{k+1})
+    void *y = nullptr;             // H x, w, or s_{k+2}
+    const void *vk = nullptr;      // v_k (step)
+    const void *vkm1 = nullptr;    // v_{k-1} (step; may be null)
+    void *vout = nullptr;          // v_{k+1} (step; may alias vkm1)
+    void *psi = nullptr;           // pass-2 accumulator (may be null)
+    const double *psi_coef = nullptr;  // device, coefficient of v_{k+1} at psi_coef[k]
+    double *tri_diag = nullptr;    // device alpha array (Dagotto layout, 0-based alpha_{k+1} at [k])
+    double *tri_sub = nullptr;     // device beta array (tri_sub[k] = beta_{k+1})
+    int k = 0;                     // 1-based step index of v_k
+    double eshift = 0.0;           // residual mode: e
+    double cutoff = 1e-25;
+    double *partials = nullptr;    // gridDim*4 doubles
+    unsigned *counter = nullptr;   // last-block counter
+    double *sums_out = nullptr;    // 4 doubles: final sums (deterministic order)
+    int *flags = nullptr;          // [0] breakdown step (0 = none), [1] non-finite
+};
+
+struct LaunchCfg {
+    int grid = 0, block = 0, rows = 1;
+    size_t smem = 0;
+    bool stage = true;
+};
+
+// ---- kernel launchers (edk_kernels.cu) ------------------------------------
+LaunchCfg plan_rows(const HamDev &H, int elem_bytes, int num_sms);
+cudaError_t launch_rows(const HamDev &H, int dtype, const RowArgs &a, const LaunchCfg &cfg,
+                        cudaStream_t st);
+cudaError_t launch_start_vector(int dtype, int64_t n, const double *ran_tab_dev,
+                                const void *user_start, void *v, double *partials,
+                                unsigned *counter, double *sums_out, int grid, cudaStream_t st);
+cudaError_t launch_scale(int dtype, int64_t n, void *v, const double *sums, int which,
+                         void *psi, const double *psi_coef, double *tri_sub0, int grid,
+                         cudaStream_t st);
+cudaError_t launch_norm2(int dtype, int64_t n, const void *v, double *partials, unsigned *counter,
+                         double *sums_out, int grid, cudaStream_t st);
+cudaError_t launch_convert(int from_dtype, int to_dtype, int64_t n, const void *in, void *out,
+                           cudaStream_t st);
+cudaError_t launch_apply_c(int dtype, int spin, int64_t dother, int64_t dup_src, int64_t dup_tgt,
+                           int64_t dim_sigma_tgt, const int32_t *src1, const int8_t *sg1,
+                           const int32_t *src2, const int8_t *sg2, int sign2, const void *in, void *out,
+                           cudaStream_t st);
+cudaError_t launch_cf(int nchain, int ld, const int32_t *n, const double *diag,
+                      const double *sub, const double *e, const double *ph,
+                      const double *scale, int nw, const double *wn, double *G, int *flag,
+                      cudaStream_t st);
+cudaError_t launch_double_occ(int dtype, const HamDev &H, int site_bit_mask_up, int site_bit_mask_dn,
+                              const void *psi, double *partials, unsigned *counter,
+                              double *sums_out, int grid, cudaStream_t st);
+
+}  // namespace edk

@@ -1,0 +1,677 @@
+// Device kernels of the Krylov engine (sm_100a).
+//
+// The sector vector is a dim_up x dim_dn array, up index contiguous
+// ("row" = one down state = dim_up contiguous elements).  The fused row kernel
+// evaluates (H x) for a group of R rows per thread block:
+//   * the R rows of x are staged in shared memory with 16-byte loads, so the
+//     up-spin hops (targets inside the same row, HAIMupdo.f90:865-881) gather
+//     from shared memory;
+//   * each thread owns columns (up states) and keeps R accumulators, so one
+//     read of an up-table entry serves R rows;
+//   * the down-spin hops (HAIMupdo.f90:883-900) read whole neighbour rows from
+//     global memory, coalesced along the up index; rows are visited in a
+//     host-chosen order that keeps neighbour rows resident in L2;
+//   * diagonal and density-density terms come from the impurity occupation
+//     bits of the two spin states (HAIMupdo.f90:784-848), Hund spin flip and
+//     pair hopping from per-state move tables (HAIMupdo.f90:1017-1129).
+// Per element the additions happen in the reference's order with separate
+// multiply and add (no FMA contraction), so the FP64 result equals a
+// sequential FP64 evaluation of HAIMupdo_multr bit for bit.
+//
+// Lanczos step (kModeStep).  With s_{k+1} = w_k = H v_k - beta_k v_{k-1} (not
+// yet orthogonalised against v_k) and alpha_k, beta_{k+1} known from the
+// previous launch's reductions, one pass computes
+//   v_{k+1}   = (s_{k+1} - alpha_k v_k) / beta_{k+1}
+//   H v_{k+1} = (H s_{k+1} - alpha_k s_{k+1} - alpha_k beta_k v_{k-1}) / beta_{k+1}
+//   w_{k+1}   = H v_{k+1} - beta_{k+1} v_k
+// using H v_k = s_{k+1} + beta_k v_{k-1}, and the sums |w|^2, <w,v_{k+1}>,
+// |v_{k+1}|^2 that give alpha_{k+1} = <w,v_{k+1}> and
+// beta_{k+2}^2 = |w|^2 - 2 alpha <w,v> + alpha^2 |v|^2 (lanc_opt,
+// Lanczos_plain.h:66-173, without its separate orthogonalise/normalise passes).
+// Reductions are deterministic: per-block partials, summed in block order by
+// the last block to finish.
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstring>
+#include "edk_internal.h"
+
+namespace edk {
+
+// ---------------------------------------------------------------------------
+// arithmetic without contraction
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double fmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double fadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double fsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+
+template <typename T> __device__ __forceinline__ const T *tab_val(const SpinTabDev &t);
+template <> __device__ __forceinline__ const double *tab_val<double>(const SpinTabDev &t) { return t.val; }
+template <> __device__ __forceinline__ const float *tab_val<float>(const SpinTabDev &t) { return t.valf; }
+template <typename T> __device__ __forceinline__ const T *tab_diag(const SpinTabDev &t);
+template <> __device__ __forceinline__ const double *tab_diag<double>(const SpinTabDev &t) { return t.diag; }
+template <> __device__ __forceinline__ const float *tab_diag<float>(const SpinTabDev &t) { return t.diagf; }
+template <typename T> __device__ __forceinline__ const T *int_coef(const HamDev &h);
+template <> __device__ __forceinline__ const double *int_coef<double>(const HamDev &h) { return h.int_coef; }
+template <> __device__ __forceinline__ const float *int_coef<float>(const HamDev &h) { return h.int_coeff; }
+template <typename T> __device__ __forceinline__ const T *jj_of(const HamDev &h);
+template <> __device__ __forceinline__ const double *jj_of<double>(const HamDev &h) { return h.jj; }
+template <> __device__ __forceinline__ const float *jj_of<float>(const HamDev &h) { return h.jjf; }
+
+// ---------------------------------------------------------------------------
+// deterministic block / grid reductions of NQ doubles
+// ---------------------------------------------------------------------------
+template <int NQ>
+__device__ __forceinline__ void block_sum(double (&v)[NQ], double (*red)[32])
+{
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) red[q][warp] = v[q];
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            double t = lane < nw ? red[q][lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+            v[q] = t;
+        }
+    }
+}
+
+// Writes this block's NQ partial sums; the last block to arrive sums all
+// partials in block order into `out` and returns true (in thread 0 only).
+template <int NQ>
+__device__ bool grid_sum(double (&v)[NQ], double *partials, unsigned *counter, double *out)
+{
+    __shared__ double red[NQ][32];
+    __shared__ bool last;
+    block_sum<NQ>(v, red);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) partials[(size_t)blockIdx.x * NQ + q] = v[q];
+        __threadfence();
+        unsigned t = atomicAdd(counter, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            double t = 0.0;
+            for (unsigned b = lane; b < gridDim.x; b += 32)
+                t += __ldcg(&partials[(size_t)b * NQ + q]);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+            if (lane == 0) out[q] = t;
+        }
+    }
+    if (threadIdx.x == 0) *counter = 0u;
+    return threadIdx.x == 0;
+}
+
+// ---------------------------------------------------------------------------
+// row staging: 16-byte global loads, scalar shared stores (any alignment)
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void stage_row(T *dst, const T *src, int64_t n)
+{
+    constexpr int V = 16 / sizeof(T);
+    const uintptr_t addr = reinterpret_cast<uintptr_t>(src);
+    int64_t head = (int64_t)(((16u - (addr & 15u)) & 15u) / sizeof(T));
+    if (head > n) head = n;
+    for (int64_t i = threadIdx.x; i < head; i += blockDim.x) dst[i] = __ldg(src + i);
+    const int64_t nv = (n - head) / V;
+    const int4 *sv = reinterpret_cast<const int4 *>(src + head);
+    for (int64_t i = threadIdx.x; i < nv; i += blockDim.x) {
+        int4 q = __ldg(sv + i);
+        T tmp[V];
+        memcpy(tmp, &q, 16);
+#pragma unroll
+        for (int v = 0; v < V; ++v) dst[head + i * V + v] = tmp[v];
+    }
+    for (int64_t i = head + nv * V + threadIdx.x; i < n; i += blockDim.x) dst[i] = __ldg(src + i);
+}
+
+// one electron of one spin moved between impurity sites a -> b
+__device__ __forceinline__ int move_index(int a, int b, int nc)
+{
+    return a * (nc - 1) + (b < a ? b : b - 1);
+}
+
+// Hund spin flip and pair hopping for element (iup, ido) (HAIMupdo.f90:1017-1129).
+template <typename T>
+__device__ __forceinline__ T hund_terms(const HamDev &H, const T *x, int64_t iup, int64_t ido,
+                                        int cu, int cd, T acc)
+{
+    const int nc = H.nc;
+    const T *jj = jj_of<T>(H);
+    // spin flip, sites s1 < s2 singly occupied with opposite spins
+    for (int s1 = 0; s1 < nc; ++s1) {
+        const int b1u = (cu >> s1) & 1, b1d = (cd >> s1) & 1;
+        if (b1u + b1d != 1) continue;
+        for (int s2 = s1 + 1; s2 < nc; ++s2) {
+            if (!H.umask[s1 * nc + s2]) continue;
+            const int b2u = (cu >> s2) & 1, b2d = (cd >> s2) & 1;
+            if (b2u + b2d != 1) continue;
+            int mu = -1, md = -1;
+            if (b1u && b2d) { mu = move_index(s1, s2, nc); md = move_index(s2, s1, nc); }
+            else if (b1d && b2u) { mu = move_index(s2, s1, nc); md = move_index(s1, s2, nc); }
+            if (mu < 0) continue;
+            const int32_t pu = H.up.move[iup * H.nmove + mu];
+            const int32_t pd = H.dn.move[ido * H.nmove + md];
+            if (pu == 0 || pd == 0) continue;
+            const int64_t ju = (pu > 0 ? pu : -pu) - 1, jd = (pd > 0 ? pd : -pd) - 1;
+            const T t = fmul(__ldg(x + ju + jd * H.dup), jj[s1 * nc + s2]);
+            acc = ((pu > 0) == (pd > 0)) ? fadd(acc, t) : fsub(acc, t);
+        }
+    }
+    // pair hopping: s1 doubly occupied, s2 empty
+    for (int s1 = 0; s1 < nc; ++s1) {
+        if (!(((cu >> s1) & 1) && ((cd >> s1) & 1))) continue;
+        for (int s2 = 0; s2 < nc; ++s2) {
+            if (s2 == s1 || !H.umask[s1 * nc + s2]) continue;
+            if (((cu >> s2) & 1) || ((cd >> s2) & 1)) continue;
+            const int m = move_index(s1, s2, nc);
+            const int32_t pu = H.up.move[iup * H.nmove + m];
+            const int32_t pd = H.dn.move[ido * H.nmove + m];
+            if (pu == 0 || pd == 0) continue;
+            const int64_t ju = (pu > 0 ? pu : -pu) - 1, jd = (pd > 0 ? pd : -pd) - 1;
+            const T t = fmul(__ldg(x + ju + jd * H.dup), jj[s1 * nc + s2]);
+            acc = ((pu > 0) == (pd > 0)) ? fadd(acc, t) : fsub(acc, t);
+        }
+    }
+    return acc;
+}
+
+// ---------------------------------------------------------------------------
+// fused row kernel
+// ---------------------------------------------------------------------------
+template <typename T> __device__ __forceinline__ const T *ell_val(const SpinTabDev &t);
+template <> __device__ __forceinline__ const double *ell_val<double>(const SpinTabDev &t) { return t.ell_val; }
+template <> __device__ __forceinline__ const float *ell_val<float>(const SpinTabDev &t) { return t.ell_valf; }
+template <typename T> __device__ __forceinline__ const T *pal_of(const SpinTabDev &t);
+template <> __device__ __forceinline__ const double *pal_of<double>(const SpinTabDev &t) { return t.pal; }
+template <> __device__ __forceinline__ const float *pal_of<float>(const SpinTabDev &t) { return t.palf; }
+
+template <int R> struct RowBounds { static constexpr int kThreads = R >= 8 ? 512 : 1024; };
+
+template <typename T, int R, bool STAGE, bool PACKED>
+__global__ void __launch_bounds__(RowBounds<R>::kThreads, 1) row_kernel(const HamDev H, const RowArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ T pal_s[256];
+    T *xs = reinterpret_cast<T *>(smem_raw);
+    const int64_t dup = H.dup, ddn = H.ddn;
+    const T *__restrict__ x = static_cast<const T *>(a.x);
+
+    double alpha = 0.0, beta_k = 0.0, beta_k1 = 0.0, inv_b = 0.0, cpsi = 0.0;
+    if (a.mode == kModeStep) {
+        beta_k1 = a.tri_sub[a.k];
+        if (!(beta_k1 >= a.cutoff)) return;            // breakdown recorded by the previous launch
+        alpha = a.tri_diag[a.k - 1];
+        beta_k = a.k >= 2 ? a.tri_sub[a.k - 1] : 0.0;
+        inv_b = 1.0 / beta_k1;
+        if (a.psi_coef) cpsi = a.psi_coef[a.k];
+    }
+    if (PACKED) {
+        const T *p = pal_of<T>(H.up);
+        for (int i = threadIdx.x; i < H.up.npal; i += blockDim.x) pal_s[i] = p[i];
+        if (!STAGE) __syncthreads();
+    }
+
+    const uint32_t *__restrict__ ell = H.up.ell;
+    const T *__restrict__ ellv = ell_val<T>(H.up);
+    const int K = H.up.ell_k;
+    const T *__restrict__ dnv = tab_val<T>(H.dn);
+    const T *__restrict__ upd = tab_diag<T>(H.up);
+    const T *__restrict__ dnd = tab_diag<T>(H.dn);
+    const T *__restrict__ icoef = int_coef<T>(H);
+
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    const int64_t ngroups = (ddn + R - 1) / R;
+    for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
+        int row[R];
+        T dd[R];
+        int cd[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int64_t q = g * R + r;
+            row[r] = q < ddn ? H.row_order[q] : -1;
+            dd[r] = row[r] >= 0 ? dnd[row[r]] : T(0);
+            cd[r] = row[r] >= 0 ? (int)H.dn.imp[row[r]] : 0;
+        }
+        if (STAGE) {
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (row[r] >= 0) stage_row<T>(xs + (size_t)r * dup, x + (int64_t)row[r] * dup, dup);
+            __syncthreads();
+        }
+        for (int64_t c = threadIdx.x; c < dup; c += blockDim.x) {
+            const int cu = H.up.imp[c];
+            const T du = upd[c];
+            T acc[R], xo[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (row[r] < 0) { acc[r] = T(0); xo[r] = T(0); continue; }
+                xo[r] = STAGE ? xs[(size_t)r * dup + c] : __ldg(x + (int64_t)row[r] * dup + c);
+                // ordered density terms (U, U', -J) for this pair of impurity configurations
+                const int cfg = cu * H.ncfg + cd[r];
+                const int o0 = H.int_off[cfg], o1 = H.int_off[cfg + 1];
+                T ac = T(0);
+                for (int o = o0; o < o1; ++o) ac = fadd(ac, fmul(icoef[o], xo[r]));
+                acc[r] = fadd(ac, fmul(fadd(du, dd[r]), xo[r]));
+            }
+            // up-spin hops: targets inside the same row (column-major padded table)
+            for (int k = 0; k < K; ++k) {
+                const uint32_t ent = __ldg(ell + (int64_t)k * dup + c);
+                int64_t j;
+                T h;
+                if (PACKED) { j = (int64_t)(ent & 0xFFFFFFu); h = pal_s[ent >> 24]; }
+                else { j = (int64_t)(int32_t)ent; h = __ldg(ellv + (int64_t)k * dup + c); }
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    if (row[r] < 0) continue;
+                    const T xj = STAGE ? xs[(size_t)r * dup + j] : __ldg(x + (int64_t)row[r] * dup + j);
+                    acc[r] = fadd(acc[r], fmul(h, xj));
+                }
+            }
+            // down-spin hops: whole neighbour rows, coalesced along c
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (row[r] < 0) continue;
+                const int f0 = H.dn.ptr[row[r]], f1 = H.dn.ptr[row[r] + 1];
+                for (int f = f0; f < f1; ++f) {
+                    const int64_t jd = H.dn.tgt[f];
+                    acc[r] = fadd(acc[r], fmul(dnv[f], __ldg(x + jd * dup + c)));
+                }
+                if (H.hund) acc[r] = hund_terms<T>(H, x, c, row[r], cu, cd[r], acc[r]);
+            }
+            // epilogue
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (row[r] < 0) continue;
+                const int64_t i = (int64_t)row[r] * dup + c;
+                if (a.mode == kModeHv) {
+                    static_cast<T *>(a.y)[i] = acc[r];
+                } else if (a.mode == kModeFirst) {
+                    const double w = (double)acc[r], v = (double)xo[r];
+                    static_cast<T *>(a.y)[i] = acc[r];
+                    s0 += w * w; s1 += w * v; s2 += v * v;
+                } else if (a.mode == kModeStep) {
+                    const double sv = (double)xo[r];
+                    const double vk = (double)static_cast<const T *>(a.vk)[i];
+                    const double vm = a.vkm1 ? (double)static_cast<const T *>(a.vkm1)[i] : 0.0;
+                    const double v1 = (sv - alpha * vk) * inv_b;
+                    const double hv1 = ((double)acc[r] - alpha * sv - (alpha * beta_k) * vm) * inv_b;
+                    const double w = hv1 - beta_k1 * vk;
+                    const T wt = (T)w, vt = (T)v1;
+                    static_cast<T *>(a.y)[i] = wt;
+                    static_cast<T *>(a.vout)[i] = vt;
+                    if (a.psi) {
+                        T *p = static_cast<T *>(a.psi) + i;
+                        *p = (T)((double)*p + cpsi * (double)vt);
+                    }
+                    const double wd = (double)wt, vd = (double)vt;
+                    s0 += wd * wd; s1 += wd * vd; s2 += vd * vd;
+                } else {   // kModeResid
+                    const double rr = (double)acc[r] - a.eshift * (double)xo[r];
+                    s0 += rr * rr; s2 += (double)xo[r] * (double)xo[r];
+                }
+            }
+        }
+    }
+    if (a.mode == kModeHv) return;
+
+    double v[4] = {s0, s1, s2, s3};
+    if (grid_sum<4>(v, a.partials, a.counter, a.sums_out)) {
+        // thread 0 of the last block: Lanczos coefficients for the next launch
+        if (a.mode == kModeFirst || a.mode == kModeStep) {
+            const double sww = a.sums_out[0], swv = a.sums_out[1], svv = a.sums_out[2];
+            const double al = swv;
+            const double b2 = sww - 2.0 * al * swv + al * al * svv;
+            const int slot = (a.mode == kModeFirst) ? 0 : a.k;       // alpha_{slot+1}
+            double b = b2 > 0.0 ? sqrt(b2) : 0.0;
+            const bool finite = isfinite(al) && isfinite(b2);
+            if (!finite) { a.flags[1] = 1; b = 0.0; }
+            // relative breakdown: the subtraction is at rounding level
+            if (b2 <= 1e-28 * sww) b = 0.0;
+            a.tri_diag[slot] = finite ? al : 0.0;
+            a.tri_sub[slot + 1] = b;
+            if (!(b >= a.cutoff) && a.flags[0] == 0) a.flags[0] = slot + 1;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// start vector, norms, scaling, conversion
+// ---------------------------------------------------------------------------
+// v(i) = ran_tab(modi(i,10000)) (rcvector_class.f90:43-60) or a copy of a user
+// vector; also |v|^2 (deterministic).
+template <typename T>
+__global__ void start_kernel(int64_t n, const double *tab, const T *user, T *v, double *partials,
+                             unsigned *counter, double *sums)
+{
+    double s[1] = {0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        T val = user ? user[i] : (T)tab[(i % 10000) + 1];
+        v[i] = val;
+        s[0] += (double)val * (double)val;
+    }
+    grid_sum<1>(s, partials, counter, sums);
+}
+
+template <typename T>
+__global__ void norm2_kernel(int64_t n, const T *v, double *partials, unsigned *counter, double *sums)
+{
+    double s[1] = {0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double t = (double)v[i];
+        s[0] += t * t;
+    }
+    grid_sum<1>(s, partials, counter, sums);
+}
+
+// v *= 1/sqrt(sums[which]); optionally psi = psi_coef[0] * v and tri_sub[0] = |v|
+template <typename T>
+__global__ void scale_kernel(int64_t n, T *v, const double *sums, int which, T *psi,
+                             const double *psi_coef, double *tri_sub0)
+{
+    const double nrm = sqrt(sums[which]);
+    const double inv = 1.0 / nrm;
+    const double c0 = psi_coef ? psi_coef[0] : 0.0;
+    if (tri_sub0 && blockIdx.x == 0 && threadIdx.x == 0) *tri_sub0 = nrm;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const T t = (T)((double)v[i] * inv);
+        v[i] = t;
+        if (psi) psi[i] = (T)(c0 * (double)t);
+    }
+}
+
+template <typename A, typename B>
+__global__ void convert_kernel(int64_t n, const A *in, B *out)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (B)in[i];
+}
+
+// ---------------------------------------------------------------------------
+// c / c+ maps (apply_Cupdo, apply_C.f90:497-653), output driven
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void apply_c_kernel(int spin, int64_t dother, int64_t dup_src, int64_t dup_tgt,
+                               int64_t dim_sigma_tgt, const int32_t *src1, const int8_t *sg1,
+                               const int32_t *src2, const int8_t *sg2, int sign2, const T *in, T *out)
+{
+    const int64_t n = dim_sigma_tgt * dother;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        int64_t jt, other, o_idx;
+        if (spin == 0) { jt = e % dup_tgt; other = e / dup_tgt; o_idx = jt + other * dup_tgt; }
+        else { other = e % dup_tgt; jt = e / dup_tgt; o_idx = other + jt * dup_tgt; }
+        T acc = T(0);
+        const int32_t i1 = src1[jt];
+        if (i1 >= 0) {
+            const int64_t si = spin == 0 ? (i1 + other * dup_src) : (other + (int64_t)i1 * dup_src);
+            acc = sg1[jt] > 0 ? in[si] : -in[si];
+        }
+        if (src2) {
+            const int32_t i2 = src2[jt];
+            if (i2 >= 0) {
+                const int64_t si = spin == 0 ? (i2 + other * dup_src) : (other + (int64_t)i2 * dup_src);
+                acc = (sg2[jt] * sign2) > 0 ? fadd(acc, in[si]) : fsub(acc, in[si]);
+            }
+        }
+        out[o_idx] = acc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// continued fraction (invert_zmtridiag, matrices_tridiag.f90:163-198)
+// ---------------------------------------------------------------------------
+__global__ void cf_kernel(int nchain, int ld, const int32_t *nlev, const double *diag,
+                          const double *sub, const double *e, const double *ph,
+                          const double *scale, int nw, const double *wn, double *G, int *flag)
+{
+    const int64_t total = (int64_t)nchain * nw;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int c = (int)(t / nw), w = (int)(t % nw);
+        const int n = nlev[c];
+        double gr = 0.0, gi = 0.0;
+        if (n > 0) {
+            const double *d = diag + (size_t)c * ld;
+            const double *s = sub + (size_t)c * ld;
+            const double zi = wn[w];
+            const double p = ph[c], ee = e[c];
+            // r = 1 / (z - ph*(d[n-1]-e))
+            double ar = -p * (d[n - 1] - ee), ai = zi;
+            double den = ar * ar + ai * ai;
+            if (sqrt(den) < 2.220446049250313e-16) { atomicExch(flag, 1); den = 1e-300; }
+            double rr = ar / den, ri = -ai / den;
+            for (int it = n - 2; it >= 0; --it) {
+                const double b2 = s[it + 1] * s[it + 1];
+                ar = -p * (d[it] - ee) - rr * b2;
+                ai = zi - ri * b2;
+                den = ar * ar + ai * ai;
+                if (sqrt(den) < 2.220446049250313e-16) { atomicExch(flag, 1); den = 1e-300; }
+                rr = ar / den;
+                ri = -ai / den;
+            }
+            gr = scale[c] * rr;
+            gi = scale[c] * ri;
+        }
+        G[2 * t] = gr;
+        G[2 * t + 1] = gi;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// double occupancy: sum over elements with both impurity bits set
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void docc_kernel(int64_t dup, int64_t ddn, const uint8_t *imp_up, const uint8_t *imp_dn,
+                            int mask, const T *psi, double *partials, unsigned *counter, double *sums)
+{
+    double s[2] = {0.0, 0.0};
+    const int64_t n = dup * ddn;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = i % dup, r = i / dup;
+        const double v = (double)psi[i];
+        const double v2 = v * v;
+        s[1] += v2;
+        if ((imp_up[c] & mask) && (imp_dn[r] & mask)) s[0] += v2;
+    }
+    grid_sum<2>(s, partials, counter, sums);
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+LaunchCfg plan_rows(const HamDev &H, int elem_bytes, int num_sms)
+{
+    LaunchCfg c;
+    const int64_t rowbytes = H.dup * (int64_t)elem_bytes;
+    int R;
+    if (rowbytes <= kMaxSmemBytes) {
+        int64_t cap = kMaxSmemBytes / (rowbytes > 0 ? rowbytes : 1);
+        R = cap >= 8 ? 8 : cap >= 4 ? 4 : cap >= 2 ? 2 : 1;
+        c.stage = true;
+    } else {
+        R = 4;
+        c.stage = false;
+    }
+    while (R > 1 && (H.ddn + R - 1) / R < num_sms) R >>= 1;   // keep every SM busy
+    c.rows = R;
+    const int maxb = R >= 8 ? 512 : 1024;
+    int block = maxb;
+    if (H.dup < maxb) block = (int)(((H.dup + 31) / 32) * 32);
+    if (block < 64) block = 64;
+    c.block = block;
+    c.smem = c.stage ? (size_t)R * (size_t)rowbytes : 0;
+    const int64_t groups = (H.ddn + R - 1) / R;
+    int per_sm = 2048 / block;
+    if (per_sm > 16) per_sm = 16;
+    if (c.smem > 0) {
+        int by_smem = (int)((228 * 1024) / (c.smem + 1024));
+        if (by_smem < per_sm) per_sm = by_smem;
+    }
+    if (per_sm < 1) per_sm = 1;
+    int64_t grid = (int64_t)num_sms * per_sm;
+    if (grid > groups) grid = groups;
+    if (grid < 1) grid = 1;
+    c.grid = (int)grid;
+    return c;
+}
+
+template <typename T, int R, bool S>
+static cudaError_t launch_rows_t(const HamDev &H, const RowArgs &a, const LaunchCfg &cfg,
+                                 cudaStream_t st)
+{
+    auto k = H.up.packed ? row_kernel<T, R, S, true> : row_kernel<T, R, S, false>;
+    if (cfg.smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)cfg.smem);
+        if (e != cudaSuccess) return e;
+    }
+    k<<<cfg.grid, cfg.block, cfg.smem, st>>>(H, a);
+    return cudaGetLastError();
+}
+
+template <typename T>
+static cudaError_t launch_rows_r(const HamDev &H, const RowArgs &a, const LaunchCfg &cfg,
+                                 cudaStream_t st)
+{
+    if (cfg.stage) {
+        switch (cfg.rows) {
+            case 8: return launch_rows_t<T, 8, true>(H, a, cfg, st);
+            case 4: return launch_rows_t<T, 4, true>(H, a, cfg, st);
+            case 2: return launch_rows_t<T, 2, true>(H, a, cfg, st);
+            default: return launch_rows_t<T, 1, true>(H, a, cfg, st);
+        }
+    }
+    switch (cfg.rows) {
+        case 4: return launch_rows_t<T, 4, false>(H, a, cfg, st);
+        case 2: return launch_rows_t<T, 2, false>(H, a, cfg, st);
+        default: return launch_rows_t<T, 1, false>(H, a, cfg, st);
+    }
+}
+
+cudaError_t launch_rows(const HamDev &H, int dtype, const RowArgs &a, const LaunchCfg &cfg,
+                        cudaStream_t st)
+{
+    return dtype == EDK_F64 ? launch_rows_r<double>(H, a, cfg, st)
+                            : launch_rows_r<float>(H, a, cfg, st);
+}
+
+cudaError_t launch_start_vector(int dtype, int64_t n, const double *tab, const void *user, void *v,
+                                double *partials, unsigned *counter, double *sums, int grid,
+                                cudaStream_t st)
+{
+    if (dtype == EDK_F64)
+        start_kernel<double><<<grid, 256, 0, st>>>(n, tab, (const double *)user, (double *)v,
+                                                   partials, counter, sums);
+    else
+        start_kernel<float><<<grid, 256, 0, st>>>(n, tab, (const float *)user, (float *)v,
+                                                  partials, counter, sums);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_norm2(int dtype, int64_t n, const void *v, double *partials, unsigned *counter,
+                         double *sums, int grid, cudaStream_t st)
+{
+    if (dtype == EDK_F64)
+        norm2_kernel<double><<<grid, 256, 0, st>>>(n, (const double *)v, partials, counter, sums);
+    else
+        norm2_kernel<float><<<grid, 256, 0, st>>>(n, (const float *)v, partials, counter, sums);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scale(int dtype, int64_t n, void *v, const double *sums, int which, void *psi,
+                         const double *psi_coef, double *tri_sub0, int grid, cudaStream_t st)
+{
+    if (dtype == EDK_F64)
+        scale_kernel<double><<<grid, 256, 0, st>>>(n, (double *)v, sums, which, (double *)psi,
+                                                   psi_coef, tri_sub0);
+    else
+        scale_kernel<float><<<grid, 256, 0, st>>>(n, (float *)v, sums, which, (float *)psi,
+                                                  psi_coef, tri_sub0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_convert(int from, int to, int64_t n, const void *in, void *out, cudaStream_t st)
+{
+    const int grid = (int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
+    if (from == EDK_F32 && to == EDK_F64)
+        convert_kernel<float, double><<<grid > 0 ? grid : 1, 256, 0, st>>>(n, (const float *)in, (double *)out);
+    else if (from == EDK_F64 && to == EDK_F32)
+        convert_kernel<double, float><<<grid > 0 ? grid : 1, 256, 0, st>>>(n, (const double *)in, (float *)out);
+    else
+        return cudaMemcpyAsync(out, in, (size_t)n * (from == EDK_F64 ? 8 : 4), cudaMemcpyDeviceToDevice, st);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_apply_c(int dtype, int spin, int64_t dother, int64_t dup_src, int64_t dup_tgt,
+                           int64_t dim_sigma_tgt, const int32_t *src1, const int8_t *sg1,
+                           const int32_t *src2, const int8_t *sg2, int sign2, const void *in, void *out,
+                           cudaStream_t st)
+{
+    const int64_t n = dim_sigma_tgt * dother;
+    int grid = (int)((n + 255) / 256);
+    if (grid > 8192) grid = 8192;
+    if (grid < 1) grid = 1;
+    if (dtype == EDK_F64)
+        apply_c_kernel<double><<<grid, 256, 0, st>>>(spin, dother, dup_src, dup_tgt, dim_sigma_tgt,
+                                                     src1, sg1, src2, sg2, sign2, (const double *)in,
+                                                     (double *)out);
+    else
+        apply_c_kernel<float><<<grid, 256, 0, st>>>(spin, dother, dup_src, dup_tgt, dim_sigma_tgt,
+                                                    src1, sg1, src2, sg2, sign2, (const float *)in,
+                                                    (float *)out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cf(int nchain, int ld, const int32_t *n, const double *diag, const double *sub,
+                      const double *e, const double *ph, const double *scale, int nw,
+                      const double *wn, double *G, int *flag, cudaStream_t st)
+{
+    const int64_t total = (int64_t)nchain * nw;
+    int grid = (int)((total + 127) / 128);
+    if (grid < 1) grid = 1;
+    if (grid > 4096) grid = 4096;
+    cf_kernel<<<grid, 128, 0, st>>>(nchain, ld, n, diag, sub, e, ph, scale, nw, wn, G, flag);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_double_occ(int dtype, const HamDev &H, int mask_up, int mask_dn, const void *psi,
+                              double *partials, unsigned *counter, double *sums, int grid,
+                              cudaStream_t st)
+{
+    (void)mask_dn;
+    if (dtype == EDK_F64)
+        docc_kernel<double><<<grid, 256, 0, st>>>(H.dup, H.ddn, H.up.imp, H.dn.imp, mask_up,
+                                                  (const double *)psi, partials, counter, sums);
+    else
+        docc_kernel<float><<<grid, 256, 0, st>>>(H.dup, H.ddn, H.up.imp, H.dn.imp, mask_up,
+                                                 (const float *)psi, partials, counter, sums);
+    return cudaGetLastError();
+}
+
+}  // namespace edk

@@ -1,0 +1,392 @@
+"""ctypes binding of libedk.so (the C-ABI declared in include/edk.h).
+
+The library is the product: every call here goes to CUDA kernels through the
+C-ABI.  Importing this module on a machine without the built library raises;
+there is no CPU fallback.  Device buffers are torch tensors (plumbing only: the
+library sees raw pointers and the current torch stream).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from .model import AIMModel
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libedk.so")
+
+EDK_OK = 0
+EDK_ERR_INVALID = 1
+EDK_ERR_CUDA = 2
+EDK_ERR_NOMEM = 3
+EDK_KRYLOV_EXHAUSTED = 4
+EDK_ERR_ZERO_START = 5
+EDK_ERR_CF_ZERO_DEN = 6
+EDK_ERR_TIMEOUT = 7
+EDK_ERR_NOT_FINITE = 8
+EDK_ERR_UNSUPPORTED = 9
+EDK_F64 = 0
+EDK_F32 = 1
+
+
+class EdkError(RuntimeError):
+    def __init__(self, code, msg=""):
+        super().__init__(f"edk error {code}: {msg}")
+        self.code = code
+
+
+class _Model(C.Structure):
+    _fields_ = [("nc", C.c_int32), ("nb", C.c_int32), ("ec", C.c_void_p), ("eb", C.c_void_p),
+                ("vbc", C.c_void_p), ("u", C.c_void_p), ("jj", C.c_void_p),
+                ("jhund", C.c_double), ("cutoff_hamilt_param", C.c_double)]
+
+
+class _LanczosOpts(C.Structure):
+    _fields_ = [("nitermax", C.c_int32), ("neigen", C.c_int32), ("tolerance", C.c_double),
+                ("demax", C.c_double), ("cutoff_min_lanczos_vec", C.c_double), ("dtype", C.c_int32),
+                ("check_every", C.c_int32), ("ran_tab", C.c_void_p), ("start_dev", C.c_void_p)]
+
+
+class _LanczosResult(C.Structure):
+    _fields_ = [("nkept", C.c_int32), ("niter", C.c_int32), ("status", C.c_int32),
+                ("E", C.c_double * 64), ("converged", C.c_int32 * 64),
+                ("diag", C.c_void_p), ("subdiag", C.c_void_p), ("vecp", C.c_void_p)]
+
+
+_LIB = None
+
+
+def lib():
+    """Loads libedk.so; raises when it is missing (no fallback)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is not built; run `python -m ed_solver_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    P, I32, I64, D = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+    sig = {
+        "edk_binom": (I64, [C.c_int, C.c_int]),
+        "edk_basis": (C.c_int, [C.c_int, C.c_int, P]),
+        "edk_rank_table": (C.c_int, [C.c_int, P]),
+        "edk_build_table": (C.c_int, [P, C.c_int, C.c_int, P, P, P, P, P, P]),
+        "edk_default_ran_tab": (C.c_int, [P]),
+        "edk_ctx_create": (C.c_int, [C.c_int, P, P]),
+        "edk_ctx_destroy": (C.c_int, [P]),
+        "edk_ctx_set_stream": (C.c_int, [P, P]),
+        "edk_ctx_last_error": (C.c_char_p, [P]),
+        "edk_ctx_launch_count": (I64, [P]),
+        "edk_ctx_timing": (C.c_int, [P, C.c_int]),
+        "edk_ctx_timing_report": (C.c_int, [P, C.c_int, P, P]),
+        "edk_h_create": (C.c_int, [P, P, C.c_int, C.c_int, P]),
+        "edk_h_destroy": (C.c_int, [P]),
+        "edk_h_dims": (C.c_int, [P, P, P, P]),
+        "edk_h_table": (C.c_int, [P, C.c_int, P, P, P, P, P]),
+        "edk_hmult": (C.c_int, [P, C.c_int, I64, P, P]),
+        "edk_hmult_host": (C.c_int, [P, C.c_int, I64, P, P]),
+        "edk_lanczos_e0": (C.c_int, [P, P, P]),
+        "edk_lanczos_gs": (C.c_int, [P, P, I32, P, P]),
+        "edk_apply_c": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, P, P]),
+        "edk_green_chain": (C.c_int, [P, C.c_int, P, I32, D, C.c_int, I32, P, D, P, P, P, P]),
+        "edk_cf_eval": (C.c_int, [P, I32, I32, P, P, P, P, P, P, I32, P, P]),
+        "edk_double_occ": (C.c_int, [P, C.c_int, P, C.c_int, P, P]),
+        "edk_residual": (C.c_int, [P, P, D, P, P]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _LIB = L
+    return L
+
+
+def _ptr(a) -> int:
+    """Raw address of a numpy array or torch tensor."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()
+
+
+def model_struct(m: AIMModel):
+    arrs = m.arrays()
+    s = _Model(m.nc, m.nb, *[a.ctypes.data for a in arrs], float(m.jhund), float(m.cutoff))
+    return s, arrs
+
+
+# ---------------------------------------------------------------------------
+# host-only helpers (no GPU needed)
+# ---------------------------------------------------------------------------
+
+def binom(n: int, k: int) -> int:
+    return int(lib().edk_binom(n, k))
+
+
+def basis(ns: int, npart: int) -> np.ndarray:
+    out = np.zeros(max(binom(ns, npart), 1), np.uint64)
+    rc = lib().edk_basis(ns, npart, out.ctypes.data)
+    if rc:
+        raise EdkError(rc, "edk_basis")
+    return out[:binom(ns, npart)]
+
+
+def rank_table(ns: int) -> np.ndarray:
+    out = np.zeros(1 << ns, np.int32)
+    rc = lib().edk_rank_table(ns, out.ctypes.data)
+    if rc:
+        raise EdkError(rc, "edk_rank_table")
+    return out
+
+
+def default_ran_tab() -> np.ndarray:
+    out = np.zeros(10001)
+    rc = lib().edk_default_ran_tab(out.ctypes.data)
+    if rc:
+        raise EdkError(rc, "edk_default_ran_tab")
+    return out
+
+
+def build_table(m: AIMModel, spin: int, npart: int):
+    """tab_HAIM2 on the host: (ptr, tgt, val, diag)."""
+    ms, keep = model_struct(m)
+    dim = C.c_int64()
+    nnz = C.c_int64()
+    rc = lib().edk_build_table(C.byref(ms), spin, npart, C.byref(dim), C.byref(nnz), None, None, None, None)
+    if rc:
+        raise EdkError(rc, "edk_build_table")
+    ptr = np.zeros(dim.value + 1, np.int64)
+    tgt = np.zeros(max(nnz.value, 1), np.int32)
+    val = np.zeros(max(nnz.value, 1), np.float64)
+    diag = np.zeros(max(dim.value, 1), np.float64)
+    rc = lib().edk_build_table(C.byref(ms), spin, npart, C.byref(dim), C.byref(nnz), ptr.ctypes.data,
+                               tgt.ctypes.data, val.ctypes.data, diag.ctypes.data)
+    if rc:
+        raise EdkError(rc, "edk_build_table")
+    return ptr, tgt[:nnz.value], val[:nnz.value], diag[:dim.value]
+
+
+# ---------------------------------------------------------------------------
+# device objects
+# ---------------------------------------------------------------------------
+
+class Context:
+    """Device, stream and scratch buffers (edk_ctx)."""
+
+    def __init__(self, device: int = 0, stream=None):
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError("ed_solver_b200 needs a CUDA device")
+        torch.cuda.set_device(device)
+        torch.cuda.init()
+        self.device = device
+        if stream is None:
+            stream = torch.cuda.current_stream(device)
+        self._stream = stream
+        h = C.c_void_p()
+        rc = lib().edk_ctx_create(device, C.c_void_p(stream.cuda_stream), C.byref(h))
+        if rc:
+            raise EdkError(rc, "edk_ctx_create")
+        self.h = h
+
+    def check(self, rc, what=""):
+        if rc not in (EDK_OK,):
+            msg = lib().edk_ctx_last_error(self.h)
+            raise EdkError(rc, f"{what}: {msg.decode() if msg else ''}")
+
+    @property
+    def launches(self) -> int:
+        return int(lib().edk_ctx_launch_count(self.h))
+
+    def timing(self, enable: bool):
+        self.check(lib().edk_ctx_timing(self.h, int(enable)), "edk_ctx_timing")
+
+    def timing_report(self, which: int):
+        n, ms = C.c_int64(), C.c_double()
+        self.check(lib().edk_ctx_timing_report(self.h, which, C.byref(n), C.byref(ms)), "timing_report")
+        return n.value, ms.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().edk_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _dtype_code(dtype) -> int:
+    import torch
+    if dtype in (torch.float64, "f64", EDK_F64):
+        return EDK_F64
+    if dtype in (torch.float32, "f32", EDK_F32):
+        return EDK_F32
+    raise ValueError(dtype)
+
+
+def _torch_dtype(code: int):
+    import torch
+    return torch.float64 if code == EDK_F64 else torch.float32
+
+
+class Hamiltonian:
+    """One (N_up, N_dn) sector Hamiltonian on the device (new_H / delete_H)."""
+
+    def __init__(self, ctx: Context, model: AIMModel, nup: int, ndn: int):
+        self.ctx = ctx
+        self.model = model
+        self.nup, self.ndn = nup, ndn
+        ms, self._keep = model_struct(model)
+        h = C.c_void_p()
+        ctx.check(lib().edk_h_create(ctx.h, C.byref(ms), nup, ndn, C.byref(h)), "edk_h_create")
+        self.h = h
+        d, du, dd = C.c_int64(), C.c_int64(), C.c_int64()
+        lib().edk_h_dims(h, C.byref(d), C.byref(du), C.byref(dd))
+        self.dim, self.dup, self.ddn = d.value, du.value, dd.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().edk_h_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def table(self, spin: int):
+        nnz = C.c_int64()
+        lib().edk_h_table(self.h, spin, C.byref(nnz), None, None, None, None)
+        d = self.dup if spin == 0 else self.ddn
+        ptr = np.zeros(d + 1, np.int64)
+        tgt = np.zeros(max(nnz.value, 1), np.int32)
+        val = np.zeros(max(nnz.value, 1), np.float64)
+        diag = np.zeros(max(d, 1), np.float64)
+        lib().edk_h_table(self.h, spin, C.byref(nnz), ptr.ctypes.data, tgt.ctypes.data,
+                          val.ctypes.data, diag.ctypes.data)
+        return ptr, tgt[:nnz.value], val[:nnz.value], diag[:d]
+
+    def hmult(self, x, out=None):
+        """Hmult__: y = H x for a device tensor x (float64 or float32)."""
+        import torch
+        code = _dtype_code(x.dtype)
+        x = x.contiguous()
+        y = torch.empty_like(x) if out is None else out
+        self.ctx.check(lib().edk_hmult(self.h, code, self.dim, _ptr(x), _ptr(y)), "edk_hmult")
+        return y
+
+    def hmult_host(self, x: np.ndarray) -> np.ndarray:
+        code = EDK_F64 if x.dtype == np.float64 else EDK_F32
+        x = np.ascontiguousarray(x)
+        y = np.empty_like(x)
+        self.ctx.check(lib().edk_hmult_host(self.h, code, self.dim, x.ctypes.data, y.ctypes.data),
+                       "edk_hmult_host")
+        return y
+
+    # ---- Lanczos -------------------------------------------------------
+    def _opts(self, dtype, nitermax, neigen, tolerance, demax, cutoff, check_every, ran_tab, start):
+        self._tab = None if ran_tab is None else np.ascontiguousarray(ran_tab, np.float64)
+        return _LanczosOpts(int(nitermax), int(neigen), float(tolerance), float(demax), float(cutoff),
+                            _dtype_code(dtype), int(check_every),
+                            None if self._tab is None else self._tab.ctypes.data,
+                            None if start is None else _ptr(start))
+
+    def lanczos_e0(self, dtype="f64", nitermax=1000, neigen=1, tolerance=1e-12, demax=1e300,
+                   cutoff=1e-25, check_every=8, ran_tab=None, start=None):
+        """Pass 1 (Lanczos_fast_diagonalize). Returns a dict."""
+        o = self._opts(dtype, nitermax, neigen, tolerance, demax, cutoff, check_every, ran_tab, start)
+        cap = min(self.dim, nitermax) + 2
+        diag = np.zeros(cap)
+        sub = np.zeros(cap)
+        vecp = np.zeros(cap * max(neigen, 1))
+        r = _LanczosResult()
+        r.diag, r.subdiag, r.vecp = diag.ctypes.data, sub.ctypes.data, vecp.ctypes.data
+        self.ctx.check(lib().edk_lanczos_e0(self.h, C.byref(o), C.byref(r)), "edk_lanczos_e0")
+        n, k = r.niter, r.nkept
+        return dict(E=np.array(r.E[:k]), niter=n, status=r.status, conv=np.array(r.converged[:k]),
+                    diag=diag[:n].copy(), subdiag=sub[:n + 1].copy(),
+                    vecp=vecp[:k * n].reshape(k, n).copy())
+
+    def lanczos_gs(self, coef, dtype="f64", ran_tab=None, start=None, cutoff=1e-25):
+        """Pass 2 (Lanczos_get_GS_sector): normalised eigenvector as a device tensor."""
+        import torch
+        code = _dtype_code(dtype)
+        o = self._opts(code, 1, 1, 0.0, 0.0, cutoff, 1, ran_tab, start)
+        coef = np.ascontiguousarray(coef, np.float64)
+        psi = torch.zeros(self.dim, dtype=_torch_dtype(code), device=f"cuda:{self.ctx.device}")
+        self.ctx.check(lib().edk_lanczos_gs(self.h, C.byref(o), len(coef), coef.ctypes.data, _ptr(psi)),
+                       "edk_lanczos_gs")
+        return psi
+
+    # ---- observables ----------------------------------------------------
+    def double_occ(self, psi, site=0):
+        d, n = C.c_double(), C.c_double()
+        self.ctx.check(lib().edk_double_occ(self.h, _dtype_code(psi.dtype), _ptr(psi), site,
+                                            C.byref(d), C.byref(n)), "edk_double_occ")
+        return d.value, n.value
+
+    def residual(self, psi, e):
+        r, n = C.c_double(), C.c_double()
+        self.ctx.check(lib().edk_residual(self.h, _ptr(psi), float(e), C.byref(r), C.byref(n)),
+                       "edk_residual")
+        return r.value, n.value
+
+    # ---- c / c+ ----------------------------------------------------------
+    def apply_c(self, vec, site, spin, dagger, site2=-1, sign2=1):
+        """apply_Cupdo on vec (this sector) -> (tensor in target sector, (nup', ndn'))."""
+        import torch
+        ns = self.model.ns
+        d = 1 if dagger else -1
+        tnup, tndn = (self.nup + d, self.ndn) if spin == 0 else (self.nup, self.ndn + d)
+        if not (0 <= tnup <= ns and 0 <= tndn <= ns):
+            raise ValueError("target sector outside the Hilbert space")
+        n = binom(ns, tnup) * binom(ns, tndn)
+        out = torch.empty(n, dtype=vec.dtype, device=vec.device)
+        od = C.c_int64()
+        self.ctx.check(lib().edk_apply_c(self.h, _dtype_code(vec.dtype), site, spin, int(bool(dagger)),
+                                         site2, sign2, _ptr(vec), _ptr(out), C.byref(od)), "edk_apply_c")
+        return out, (tnup, tndn)
+
+    # ---- dynamic correlation ----------------------------------------------
+    def green_chain(self, start, nitergreen, e0, iph, wn, cutoff_dynamic=1e-8):
+        """compute_dynamic_cpu on this (target) sector. Returns (G, diag, subdiag, niter)."""
+        wn = np.ascontiguousarray(wn, np.float64)
+        G = np.zeros(2 * len(wn))
+        cap = min(nitergreen, self.dim) + 2
+        dg = np.zeros(cap)
+        sd = np.zeros(cap)
+        nd = C.c_int32()
+        self.ctx.check(lib().edk_green_chain(self.h, _dtype_code(start.dtype), _ptr(start), int(nitergreen),
+                                             float(e0), int(iph), len(wn), wn.ctypes.data,
+                                             float(cutoff_dynamic), G.ctypes.data, dg.ctypes.data,
+                                             sd.ctypes.data, C.byref(nd)), "edk_green_chain")
+        n = nd.value
+        return G[0::2] + 1j * G[1::2], dg[:n].copy(), sd[:n].copy(), n
+
+
+def cf_eval(ctx: Context, chains, wn, ld=None):
+    """Device continued fractions. chains: list of dict(diag, subdiag, e, ph, scale)."""
+    wn = np.ascontiguousarray(wn, np.float64)
+    nch = len(chains)
+    ld = ld or max(len(c["diag"]) for c in chains)
+    n = np.array([len(c["diag"]) for c in chains], np.int32)
+    diag = np.zeros((nch, ld))
+    sub = np.zeros((nch, ld))
+    for i, c in enumerate(chains):
+        diag[i, :len(c["diag"])] = c["diag"]
+        sub[i, :len(c["subdiag"])] = c["subdiag"][:ld]
+    e = np.array([c["e"] for c in chains], np.float64)
+    ph = np.array([c["ph"] for c in chains], np.float64)
+    sc = np.array([c["scale"] for c in chains], np.float64)
+    G = np.zeros((nch, len(wn), 2))
+    ctx.check(lib().edk_cf_eval(ctx.h, nch, ld, n.ctypes.data, diag.ctypes.data, sub.ctypes.data,
+                                e.ctypes.data, ph.ctypes.data, sc.ctypes.data, len(wn), wn.ctypes.data,
+                                G.ctypes.data), "edk_cf_eval")
+    return G[..., 0] + 1j * G[..., 1]

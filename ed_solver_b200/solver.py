@@ -1,0 +1,140 @@
+"""Drivers above the Krylov C-ABI, mirroring the reference's L4 layer.
+
+* ``solve_sector``   - get_eigen_energies + get_GS for one sector
+  (ed_solver/solver.h:98-237, ed_solver/Lanczos_plain.f90:33-229), with dense
+  diagonalisation below FULL_ED_SWITCH (ed_solver/ED_ARPACK.f90:590-715);
+* ``ground_states``  - the sector scan and global Boltzmann window
+  (ed_solver/eigen_class.f90:322-450, ed_solver/dmft_ed_solver.f90:1468);
+* ``green_impurity`` - compute_greenAA for the (c, c+) channel
+  (ed_solver/green_class_computeAA.f90:40-185) with the real-H symmetric
+  combinations (ed_solver/green_class_compute_symmetric_combination.f90:39-138)
+  and the off-diagonal reshuffle (..._AA.h:10-60).
+
+Every vector operation runs on the GPU through ``ed_solver_b200.edk``.
+"""
+from __future__ import annotations
+
+import math
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import edk
+from .model import AIMModel, matsubara
+
+FULL_ED_SWITCH = 40   # ed_solver/Global_Variables.f90:23
+
+
+class HCache:
+    """Keeps one device Hamiltonian per sector alive across calls."""
+
+    def __init__(self, ctx: edk.Context, model: AIMModel):
+        self.ctx, self.model = ctx, model
+        self._h: Dict[Tuple[int, int], edk.Hamiltonian] = {}
+
+    def get(self, sector) -> edk.Hamiltonian:
+        sector = tuple(sector)
+        if sector not in self._h:
+            self._h[sector] = edk.Hamiltonian(self.ctx, self.model, *sector)
+        return self._h[sector]
+
+    def close(self):
+        for h in self._h.values():
+            h.close()
+        self._h.clear()
+
+
+def _dense(h: edk.Hamiltonian, dtype="f64"):
+    """Dense H built column by column with Hmult__ on the device (ED_ARPACK.f90:620-626)."""
+    import torch
+    eye = torch.eye(h.dim, dtype=torch.float64, device=f"cuda:{h.ctx.device}")
+    cols = [h.hmult(eye[i].contiguous()) for i in range(h.dim)]
+    return torch.stack(cols, 1).cpu().numpy()
+
+
+def solve_sector(hc: HCache, sector, neigen=1, nitermax=1000, tolerance=1e-12, demax=1e300,
+                 dtype="f64", ran_tab=None, check_every=8):
+    """Eigenpairs of one sector: list of dict(E, psi (device tensor), niter)."""
+    import torch
+    h = hc.get(sector)
+    if h.dim == 0:
+        return []
+    if h.dim <= FULL_ED_SWITCH:
+        H = _dense(h)
+        w, v = np.linalg.eigh(H)
+        j = min(h.dim, neigen)
+        keep = [0] + [i for i in range(1, j) if w[i] <= w[0] + demax]
+        dev = f"cuda:{h.ctx.device}"
+        tdt = torch.float64 if dtype in ("f64", edk.EDK_F64) else torch.float32
+        return [dict(E=float(w[i]), psi=torch.tensor(v[:, i], dtype=tdt, device=dev), niter=0) for i in keep]
+    r = h.lanczos_e0(dtype=dtype, nitermax=nitermax, neigen=neigen, tolerance=tolerance, demax=demax,
+                     ran_tab=ran_tab, check_every=check_every)
+    out = []
+    for k in range(len(r["E"])):
+        psi = h.lanczos_gs(r["vecp"][k], dtype=dtype, ran_tab=ran_tab)
+        out.append(dict(E=float(r["E"][k]), psi=psi, niter=r["niter"]))
+    return out
+
+
+def ground_states(hc: HCache, sectors, beta: float, demax0: float, neigen=1, nitermax=1000,
+                  tolerance=1e-12, dtype="f64", ran_tab=None):
+    demax = demax0 / beta
+    found = []
+    for sec in sectors:
+        states = solve_sector(hc, sec, neigen=neigen, nitermax=nitermax, tolerance=tolerance,
+                              demax=demax, dtype=dtype, ran_tab=ran_tab)
+        if not states:
+            continue
+        es = min(s["E"] for s in states)
+        for s in states:
+            if s["E"] <= es + demax:
+                found.append(dict(sector=tuple(sec), **s))
+    e0 = min(f["E"] for f in found)
+    gs = [f for f in found if f["E"] <= e0 + demax]
+    z = sum(math.exp(-beta * (f["E"] - e0)) for f in gs)
+    for f in gs:
+        f["boltz"] = math.exp(-beta * (f["E"] - e0)) / z
+    return gs, e0, z
+
+
+def green_impurity(hc: HCache, gs, beta: float, nw: int, nitergreen: int, spin: int = 0,
+                   pairs: Optional[Sequence[Tuple[int, int]]] = None, cutoff_dynamic=1e-8,
+                   dtype=None):
+    """G_ij(i w_n) of the impurity orbitals for one spin (compute_greenAA, (c,c+) channel)."""
+    model = hc.model
+    nc = model.nc
+    if pairs is None:
+        pairs = [(i, i) for i in range(nc)]
+    wn = matsubara(beta, nw)
+    combos = sorted(set([(i, i) for (i, j) in pairs] + [(j, j) for (i, j) in pairs] +
+                        [(min(i, j), max(i, j)) for (i, j) in pairs if i != j]))
+    raw = {c: np.zeros(nw, complex) for c in combos}
+    ns = model.ns
+    for st in gs:
+        nu, nd = st["sector"]
+        h_src = hc.get(st["sector"])
+        psi = st["psi"]
+        if dtype is not None:
+            psi = psi.to(dtype)
+        for iph in (1, 2):
+            dagger = iph == 1
+            d = 1 if dagger else -1
+            tsec = (nu + d, nd) if spin == 0 else (nu, nd + d)
+            if not (0 <= tsec[0] <= ns and 0 <= tsec[1] <= ns):
+                continue
+            h_t = hc.get(tsec)
+            for (i, j) in combos:
+                if i == j:
+                    v, _ = h_src.apply_c(psi, i, spin, dagger)
+                else:
+                    v, _ = h_src.apply_c(psi, i, spin, dagger, site2=j, sign2=1)
+                G, _, _, _ = h_t.green_chain(v, nitergreen, st["E"], iph, wn, cutoff_dynamic)
+                raw[(i, j)] += st["boltz"] * G
+    out = {}
+    for (i, j) in pairs:
+        if i == j:
+            out[(i, j)] = raw[(i, i)]
+        else:
+            a, b = min(i, j), max(i, j)
+            out[(i, j)] = 0.5 * (raw[(a, b)] - raw[(a, a)] - raw[(b, b)])
+    return out

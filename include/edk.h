@@ -1,0 +1,186 @@
+/*
+ * edk.h -- C-ABI of the B200-native Krylov engine for the ed_solver
+ * exact-diagonalisation impurity solver.
+ *
+ * Every entry point returns an int status (EDK_OK = 0) and never exits the
+ * process.  Handles are opaque; one handle is used by one host thread at a
+ * time.  Vectors follow the reference layout: an (N_up, N_dn) sector vector
+ * is a dim_up x dim_dn Fortran array, up index fastest
+ * (rank = iup + ido*dim_up, 0-based here; the reference is 1-based,
+ * quantum_fermion_sector_class.f90:256-264).  Basis states of one spin species
+ * are the integers with the sector's popcount in increasing order
+ * (quantum_fermion_hilbert_class.f90:385-404); bath site k is bit k and
+ * impurity site c is bit nb+c (quantum_algebra_Anderson_Impurity_class.f90:73-87).
+ *
+ * Pointers named *_dev are device pointers on the context's device; *_host
+ * are host pointers.  Nothing here takes or returns a torch type.
+ */
+#ifndef EDK_H
+#define EDK_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define EDK_OK                 0
+#define EDK_ERR_INVALID        1   /* bad argument or inconsistent sizes (reference: STOP) */
+#define EDK_ERR_CUDA           2   /* a CUDA runtime call failed */
+#define EDK_ERR_NOMEM          3   /* device or host allocation failed */
+#define EDK_KRYLOV_EXHAUSTED   4   /* |w| fell below cutoff_min_lanczos_vec: the
+                                      tridiagonal was truncated (Lanczos_plain.h:85-91
+                                      STOPs there; here it is a normal early end) */
+#define EDK_ERR_ZERO_START     5   /* start vector of (near) zero norm */
+#define EDK_ERR_CF_ZERO_DEN    6   /* zero denominator in the continued fraction
+                                      (matrices_tridiag.f90:176-190) */
+#define EDK_ERR_TIMEOUT        7   /* a bounded device-side wait gave up */
+#define EDK_ERR_NOT_FINITE     8   /* NaN/Inf met in a Krylov coefficient */
+#define EDK_ERR_UNSUPPORTED    9
+
+/* ---- element types ----------------------------------------------------- */
+#define EDK_F64 0   /* FP64 vectors and arithmetic (the reference's REAL(DBL) path) */
+#define EDK_F32 1   /* FP32 vectors and H*v, FP64 accumulation of norms and alpha/beta */
+
+typedef struct edk_ctx edk_ctx;   /* device, stream, workspaces */
+typedef struct edk_h edk_h;       /* one (N_up, N_dn) sector Hamiltonian on the device */
+
+/* Anderson impurity model (replaces the AIM_type / JJmatrix globals read by
+ * new_HAIMupdo, HAIMupdo.f90:53-121).  Matrices are row-major, spin-major:
+ *   ec [2][nc][nc]  Ec_s(c,c')        eb [2][nb][nb]  Eb_s(k,k')
+ *   vbc[2][nb][nc]  Vbc_s(k,c)        u  [nc][nc]     U(c,c')
+ *   jj [nc][nc]     JJmatrix(c,c')    jhund           scalar gate |Jhund|>1e-5
+ * cutoff_hamilt_param drops off-diagonal one-body terms with |t| <= cutoff
+ * (HAIM_offdiag_arrays.f90:450,470,496). */
+typedef struct edk_model {
+    int32_t nc, nb;
+    const double *ec, *eb, *vbc, *u, *jj;
+    double jhund;
+    double cutoff_hamilt_param;
+} edk_model;
+
+/* ---- context ----------------------------------------------------------- */
+/* stream: a cudaStream_t (may be NULL for the legacy default stream). */
+int edk_ctx_create(int device, void *stream, edk_ctx **out);
+int edk_ctx_destroy(edk_ctx *ctx);
+int edk_ctx_set_stream(edk_ctx *ctx, void *stream);
+/* Human-readable text of the last error recorded on this context. */
+const char *edk_ctx_last_error(const edk_ctx *ctx);
+/* Number of kernels this library launched on the context since creation. */
+int64_t edk_ctx_launch_count(const edk_ctx *ctx);
+/* Per-kernel CUDA-event timing on the context's stream.  enable=1 starts
+ * recording every row-kernel launch (H*v and Lanczos steps), 0 stops; the
+ * report synchronises and returns, for kernel class `which` (0 = H*v,
+ * 1 = first Lanczos step, 2 = fused Lanczos step, 3 = residual; add 4 for
+ * FP32), the number of launches and their summed device time in ms. */
+int edk_ctx_timing(edk_ctx *ctx, int enable);
+int edk_ctx_timing_report(edk_ctx *ctx, int which, int64_t *launches, double *total_ms);
+
+/* ---- basis (quantum_fermion_hilbert_class.f90:346-421) ----------------- */
+int64_t edk_binom(int n, int k);
+/* states[binom(ns,npart)] in increasing order */
+int edk_basis(int ns, int npart, uint64_t *states_host);
+/* rank_host[2^ns]: 0-based position of each state inside its popcount class */
+int edk_rank_table(int ns, int32_t *rank_host);
+
+/* The library's default 10001-entry start-vector table (stands in for the
+ * reference's gfortran-seeded ran_tab, random.f90:684-704). Host-only. */
+int edk_default_ran_tab(double *tab_host);
+
+/* Host-only tab_HAIM2 (HAIM_offdiag_arrays.f90:210-606) for one spin species
+ * and particle number: call once with NULL arrays to get *dim and *nnz, then
+ * with ptr[dim+1], tgt[nnz], val[nnz], diag[dim] allocated.  Needs no GPU. */
+int edk_build_table(const edk_model *m, int spin, int npart, int64_t *dim, int64_t *nnz,
+                    int64_t *ptr_host, int32_t *tgt_host, double *val_host, double *diag_host);
+
+/* ---- sector Hamiltonian: new_H / delete_H / dimen_H (H_class.f90:28-58,149-152) */
+int edk_h_create(edk_ctx *ctx, const edk_model *m, int nup, int ndn, edk_h **out);
+int edk_h_destroy(edk_h *h);
+int edk_h_dims(const edk_h *h, int64_t *dim, int64_t *dim_up, int64_t *dim_dn);
+/* Export one spin species' table (tab_HAIM2, HAIM_offdiag_arrays.f90:210-606)
+ * as built for the device: CSR row pointer ptr[dim_s+1], 0-based target rank
+ * tgt[nnz], value val[nnz], diagonal diag[dim_s].  Any pointer may be NULL;
+ * *nnz receives the entry count. */
+int edk_h_table(const edk_h *h, int spin, int64_t *nnz, int64_t *ptr_host,
+                int32_t *tgt_host, double *val_host, double *diag_host);
+
+/* Hmult__ (H_class.f90:69-136 -> HAIMupdo_multr, HAIMupdo.f90:677-1195):
+ * y = H x on device buffers of n = dim elements.  In EDK_F64 the per-element
+ * order of additions is the reference's, so results are bit-identical to a
+ * sequential FP64 evaluation of HAIMupdo_multr. */
+int edk_hmult(edk_h *h, int dtype, int64_t n, const void *x_dev, void *y_dev);
+/* Same on host buffers: copies in, multiplies, copies out (synchronous). */
+int edk_hmult_host(edk_h *h, int dtype, int64_t n, const void *x_host, void *y_host);
+
+/* ---- Lanczos (Lanczos_plain.f90:33-229, Lanczos_plain.h:66-173) --------- */
+typedef struct edk_lanczos_opts {
+    int32_t nitermax;            /* Nitermax; Niter = min(dim-1, nitermax) */
+    int32_t neigen;              /* Neigen (<= 64) */
+    double tolerance;            /* eigenvalue change for convergence */
+    double demax;                /* keep eigenvalue k>1 if converged and <= E1+demax */
+    double cutoff_min_lanczos_vec;  /* breakdown threshold (reference 1e-25) */
+    int32_t dtype;               /* EDK_F64 or EDK_F32 */
+    int32_t check_every;         /* host convergence check cadence (steps), >=1 */
+    const double *ran_tab;       /* host, 10001 entries; NULL = the library's table */
+    const void *start_dev;       /* optional start vector (dtype, dim); overrides ran_tab */
+} edk_lanczos_opts;
+
+typedef struct edk_lanczos_result {
+    int32_t nkept;               /* eigenvalues kept (>=1) */
+    int32_t niter;               /* Lanczos iterations of pass 1 */
+    int32_t status;              /* EDK_OK or EDK_KRYLOV_EXHAUSTED */
+    double E[64];
+    int32_t converged[64];
+    double *diag;                /* host, capacity >= nitermax+1: alpha_k */
+    double *subdiag;             /* host, capacity >= nitermax+1: subdiag[0]=|v0|, [k]=beta_{k+1} */
+    double *vecp;                /* host, capacity >= neigen*(nitermax+1): column j = coefficients of E[j] */
+} edk_lanczos_result;
+
+/* Pass 1: eigenvalues and tridiagonal eigenvector coefficients. */
+int edk_lanczos_e0(edk_h *h, const edk_lanczos_opts *o, edk_lanczos_result *r);
+/* Pass 2 (Lanczos_get_GS_sector): psi = normalised sum_k coef[k] v_k, rebuilt
+ * from the same start vector; psi_dev has dtype o->dtype and dim elements. */
+int edk_lanczos_gs(edk_h *h, const edk_lanczos_opts *o, int32_t niter, const double *coef_host,
+                   void *psi_dev);
+
+/* ---- c / c+ (apply_Cupdo, apply_C.f90:497-653; Cup_sector/Cdo_sector :79-109)
+ * src: the sector of in_dev; out_dev receives c[+]_{site,spin} in in the
+ * target sector (N_spin +/- 1), fully overwritten.  site is the 0-based
+ * impurity site, spin 0 = up, 1 = down.  with_site2 >= 0 adds
+ * sign2 * c[+]_{site2,spin} (the symmetric combination of
+ * green_class_compute_symmetric_combination.f90:39-138 with sign2 = +1). */
+int edk_apply_c(edk_h *src, int dtype, int site, int spin, int dagger, int site2, int sign2,
+                const void *in_dev, void *out_dev, int64_t *out_dim);
+
+/* ---- dynamic correlation (compute_dynamic_cpu, green_class_compute_dynamic.f90:191-334)
+ * target: Hamiltonian of the sector start_dev lives in.  Runs exactly
+ * min(nitergreen, dim) steps from start/|start| (stops early only on
+ * breakdown), then dyn(w) = |start|^2 <0|(i wn - ph*(T-e0))^-1|0> with ph=+1
+ * (iph=1, particle) or -1 (iph=2, hole).  G_host is interleaved re/im,
+ * length 2*nw.  diag/subdiag (host, capacity nitergreen+1) may be NULL. */
+int edk_green_chain(edk_h *target, int dtype, const void *start_dev, int32_t nitergreen,
+                    double e0, int iph, int32_t nw, const double *wn_host,
+                    double cutoff_dynamic, double *G_host, double *diag_host,
+                    double *subdiag_host, int32_t *niter_done);
+
+/* invert_zmtridiag (matrices_tridiag.f90:163-198) for nchain tridiagonals of
+ * n[c] levels each (diag/subdiag packed with stride ld) at nw frequencies,
+ * scaled by scale[c] and the shift/sign of compute_dynamic:
+ * G[c][w] = scale[c] * <0|(i wn[w] - ph[c]*(T_c - e[c]))^-1|0>.  Device-side. */
+int edk_cf_eval(edk_ctx *ctx, int32_t nchain, int32_t ld, const int32_t *n_host,
+                const double *diag_host, const double *subdiag_host, const double *e_host,
+                const double *ph_host, const double *scale_host, int32_t nw,
+                const double *wn_host, double *G_host);
+
+/* ---- observables --------------------------------------------------------
+ * <psi| n_{site,up} n_{site,dn} |psi> (the double occupancy of
+ * correlations_write.h:93-95) and |psi|^2 in one pass. */
+int edk_double_occ(edk_h *h, int dtype, const void *psi_dev, int site, double *docc, double *norm2);
+/* |H psi - e psi| and |psi| with the FP64 matvec (psi in FP64). */
+int edk_residual(edk_h *h, const void *psi_dev, double e, double *res_norm, double *psi_norm);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EDK_H */

@@ -1,0 +1,523 @@
+"""Python side of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Wraps ``oracle/_build/liborc.so`` (the C restatement in ``edk_oracle.c``) and
+adds, in numpy:
+
+* ``dense_sector_h``: an independent second-quantised build of the sector
+  Hamiltonian (standard Jordan-Wigner algebra, Kanamori terms), used to pin the
+  C restatement of HAIMupdo_multr element by element;
+* the drivers that sit above the Krylov primitives in the reference:
+  the sector scan and Boltzmann window of get_eigen_energies
+  (ed_solver/solver.h:98-237, ed_solver/eigen_class.f90:322-450) and the
+  Green-function loop of compute_greenAA (ed_solver/green_class_computeAA.f90:40-185,
+  ed_solver/green_class_computeAA.h:101-302) with the symmetric combinations of
+  ed_solver/green_class_compute_symmetric_combination.f90:39-138 and the
+  off-diagonal reshuffle of ed_solver/green_class_compute_symmetric_combination_AA.h:10-60.
+
+Only tests, ``__graft_entry__.smoke`` and bench.py's CPU-baseline leg import
+this module; the product never does.  Parity of this oracle is pinned by the
+reference's golden output test/2b/bm/g_bm (see tests/golden) plus analytic
+limits and dense diagonalisation; the reference's gfortran start-vector table
+is not reproducible, so its exact Lanczos coefficient sequence is unpinned.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+import subprocess
+import sys
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_REPO = os.path.dirname(_HERE)
+if _REPO not in sys.path:
+    sys.path.insert(0, _REPO)
+
+from ed_solver_b200.model import AIMModel, default_ran_tab, matsubara  # noqa: E402
+
+_LIB = None
+
+
+def build():
+    subprocess.check_call(["make", "-s", "-C", _HERE])
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "_build", "liborc.so")
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        P = C.c_void_p
+        d = C.c_double
+        i32 = C.c_int
+        i64 = C.c_int64
+        L.orc_binom.restype = i64
+        L.orc_binom.argtypes = [i32, i32]
+        L.orc_basis.restype = i64
+        L.orc_basis.argtypes = [i32, i32, P]
+        L.orc_rank_table.argtypes = [i32, P]
+        L.orc_h_new.restype = P
+        L.orc_h_new.argtypes = [P, i32, i32]
+        L.orc_h_free.argtypes = [P]
+        for f in ("orc_h_dim", "orc_h_dup", "orc_h_ddn"):
+            getattr(L, f).restype = i64
+            getattr(L, f).argtypes = [P]
+        L.orc_h_table.restype = i64
+        L.orc_h_table.argtypes = [P, i32, P, P, P, P, P]
+        L.orc_hmult.argtypes = [P, P, P]
+        L.orc_tridiag_eig.restype = i32
+        L.orc_tridiag_eig.argtypes = [i32, P, P, P, P]
+        L.orc_fix_initial_vector.argtypes = [i64, P, P]
+        L.orc_lanczos_e0.restype = i32
+        L.orc_lanczos_e0.argtypes = [P, P, i32, i32, d, d, d, P, P, P, P, P, P]
+        L.orc_lanczos_gs.restype = i32
+        L.orc_lanczos_gs.argtypes = [P, P, i32, P, d, P]
+        L.orc_apply_c.restype = i32
+        L.orc_apply_c.argtypes = [i32, i32, i32, i32, i32, i32, i32, P, P]
+        L.orc_cf.restype = i32
+        L.orc_cf.argtypes = [i32, P, P, d, d, P, P]
+        L.orc_green_chain.restype = i32
+        L.orc_green_chain.argtypes = [P, P, i32, d, i32, i32, P, d, d, P, P, P]
+        L.orc_double_occ.restype = d
+        L.orc_double_occ.argtypes = [P, P, i32]
+        L.orc_num_threads.restype = i32
+        _LIB = L
+    return _LIB
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class _CModel(C.Structure):
+    _fields_ = [("nc", C.c_int32), ("nb", C.c_int32), ("ec", C.c_void_p), ("eb", C.c_void_p),
+                ("vbc", C.c_void_p), ("u", C.c_void_p), ("jj", C.c_void_p),
+                ("jhund", C.c_double), ("cutoff", C.c_double)]
+
+
+def _cmodel(m: AIMModel):
+    arrs = m.arrays()
+    cm = _CModel(m.nc, m.nb, *[a.ctypes.data for a in arrs], float(m.jhund), float(m.cutoff))
+    return cm, arrs
+
+
+# ---------------------------------------------------------------------------
+# basis
+# ---------------------------------------------------------------------------
+
+def binom(n, k) -> int:
+    return int(lib().orc_binom(n, k))
+
+
+def basis(ns: int, np_: int) -> np.ndarray:
+    out = np.zeros(max(binom(ns, np_), 1), dtype=np.uint64)
+    n = lib().orc_basis(ns, np_, _p(out))
+    return out[:n]
+
+
+def rank_table(ns: int) -> np.ndarray:
+    out = np.zeros(1 << ns, dtype=np.int32)
+    lib().orc_rank_table(ns, _p(out))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# sector Hamiltonian
+# ---------------------------------------------------------------------------
+
+class OracleH:
+    """new_H / Hmult__ / delete_H for one (N_up, N_dn) sector (HAIMupdo.f90:53-121,677-1195)."""
+
+    def __init__(self, model: AIMModel, nup: int, ndn: int):
+        self.model = model
+        self.nup, self.ndn = nup, ndn
+        cm, self._keep = _cmodel(model)
+        self._cm = cm
+        self.h = lib().orc_h_new(C.byref(cm), nup, ndn)
+        if not self.h:
+            raise ValueError("unsupported model")
+        self.dim = int(lib().orc_h_dim(self.h))
+        self.dup = int(lib().orc_h_dup(self.h))
+        self.ddn = int(lib().orc_h_ddn(self.h))
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            lib().orc_h_free(h)
+            self.h = None
+
+    def hmult(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(self.dim, dtype=np.float64)
+        lib().orc_hmult(self.h, _p(x), _p(y))
+        return y
+
+    def table(self, spin: int):
+        d = self.dup if spin == 0 else self.ddn
+        nnz = int(lib().orc_h_table(self.h, spin, None, None, None, None, None))
+        st = np.zeros(d, np.uint64)
+        ptr = np.zeros(d + 1, np.int64)
+        tgt = np.zeros(max(nnz, 1), np.int32)
+        val = np.zeros(max(nnz, 1), np.float64)
+        diag = np.zeros(d, np.float64)
+        lib().orc_h_table(self.h, spin, _p(st), _p(ptr), _p(tgt), _p(val), _p(diag))
+        return st, ptr, tgt[:nnz], val[:nnz], diag
+
+    def dense(self) -> np.ndarray:
+        """Dense matrix built column by column from Hmult__ (ED_diago, ED_ARPACK.f90:620-626)."""
+        H = np.zeros((self.dim, self.dim))
+        e = np.zeros(self.dim)
+        for i in range(self.dim):
+            e[i] = 1.0
+            H[:, i] = self.hmult(e)
+            e[i] = 0.0
+        return H
+
+    def double_occ(self, psi: np.ndarray, site: int = 0) -> float:
+        psi = np.ascontiguousarray(psi, dtype=np.float64)
+        return float(lib().orc_double_occ(self.h, _p(psi), site))
+
+
+def start_vector(dim: int, ran_tab: Optional[np.ndarray] = None) -> np.ndarray:
+    tab = default_ran_tab() if ran_tab is None else np.ascontiguousarray(ran_tab, np.float64)
+    v = np.empty(dim, dtype=np.float64)
+    lib().orc_fix_initial_vector(dim, _p(tab), _p(v))
+    return v
+
+
+def tridiag_eig(d: np.ndarray, e: np.ndarray, vectors: bool = False):
+    n = len(d)
+    d = np.ascontiguousarray(d, np.float64)
+    e = np.ascontiguousarray(e, np.float64) if n > 1 else np.zeros(1)
+    w = np.empty(n)
+    z = np.empty((n, n)) if vectors else None
+    lib().orc_tridiag_eig(n, _p(d), _p(e), _p(w), _p(z) if vectors else None)
+    if vectors:
+        return w, z.T.copy()   # columns are eigenvectors
+    return w
+
+
+def lanczos_e0(h: OracleH, v0=None, nitermax=1000, neigen=1, tolerance=1e-12, demax=1e300,
+               cutoff_min=1e-25):
+    """Pass 1 (Lanczos_plain.f90:33-134). Returns dict with E, niter, diag, subdiag, vecp, conv."""
+    if v0 is None:
+        v0 = start_vector(h.dim)
+    v0 = np.ascontiguousarray(v0, np.float64)
+    nmax = max(1, min(h.dim - 1, nitermax))
+    E = np.zeros(64)
+    niter = np.zeros(1, np.int32)
+    diag = np.zeros(nmax + 1)
+    sub = np.zeros(nmax + 1)
+    vecp = np.zeros(64 * (nmax + 1))
+    conv = np.zeros(64, np.int32)
+    k = lib().orc_lanczos_e0(h.h, _p(v0), nitermax, neigen, tolerance, demax, cutoff_min,
+                             _p(E), _p(niter), _p(diag), _p(sub), _p(vecp), _p(conv))
+    if k < 0:
+        raise RuntimeError(f"orc_lanczos_e0 failed ({k})")
+    it = int(niter[0])
+    return dict(E=E[:k].copy(), niter=it, diag=diag[:it].copy(), subdiag=sub[:it].copy(),
+                vecp=vecp[:k * it].reshape(k, it).copy(), conv=conv[:k].copy())
+
+
+def lanczos_gs(h: OracleH, coef: np.ndarray, v0=None, cutoff_min=1e-25) -> np.ndarray:
+    """Pass 2 (Lanczos_plain.f90:156-229)."""
+    if v0 is None:
+        v0 = start_vector(h.dim)
+    v0 = np.ascontiguousarray(v0, np.float64)
+    coef = np.ascontiguousarray(coef, np.float64)
+    psi = np.empty(h.dim)
+    lib().orc_lanczos_gs(h.h, _p(v0), len(coef), _p(coef), cutoff_min, _p(psi))
+    return psi
+
+
+def apply_c(model: AIMModel, nup: int, ndn: int, site: int, spin: int, dagger: bool,
+            vec: np.ndarray) -> Tuple[np.ndarray, Tuple[int, int]]:
+    """apply_Cupdo (apply_C.f90:497-653). Returns (vector, target sector)."""
+    ns = model.ns
+    tnup = nup + ((1 if dagger else -1) if spin == 0 else 0)
+    tndn = ndn + ((1 if dagger else -1) if spin == 1 else 0)
+    if not (0 <= tnup <= ns and 0 <= tndn <= ns):
+        raise ValueError("target sector out of range")
+    out = np.zeros(binom(ns, tnup) * binom(ns, tndn))
+    vec = np.ascontiguousarray(vec, np.float64)
+    lib().orc_apply_c(ns, model.nb, nup, ndn, site, spin, int(dagger), _p(vec), _p(out))
+    return out, (tnup, tndn)
+
+
+def cf(diag: np.ndarray, subdiag: np.ndarray, z: complex) -> complex:
+    d = np.ascontiguousarray(diag, np.float64)
+    s = np.ascontiguousarray(subdiag, np.float64)
+    r = np.zeros(1)
+    i = np.zeros(1)
+    if lib().orc_cf(len(d), _p(d), _p(s), z.real, z.imag, _p(r), _p(i)):
+        raise ZeroDivisionError("zero denominator in continued fraction")
+    return complex(r[0], i[0])
+
+
+def green_chain(h: OracleH, opm: np.ndarray, nitergreen: int, e0: float, iph: int,
+                wn: np.ndarray, cutoff_dynamic=1e-8, cutoff_min=1e-25):
+    """compute_dynamic_cpu (green_class_compute_dynamic.f90:191-334). Returns (G, diag, subdiag)."""
+    opm = np.ascontiguousarray(opm, np.float64)
+    wn = np.ascontiguousarray(wn, np.float64)
+    G = np.zeros(2 * len(wn))
+    nmax = max(1, min(nitergreen, h.dim))
+    dg = np.zeros(nmax)
+    sd = np.zeros(nmax)
+    n = lib().orc_green_chain(h.h, _p(opm), nitergreen, e0, iph, len(wn), _p(wn),
+                              cutoff_dynamic, cutoff_min, _p(G), _p(dg), _p(sd))
+    return G[0::2] + 1j * G[1::2], dg[:n].copy(), sd[:n].copy()
+
+
+# ---------------------------------------------------------------------------
+# independent dense build (second quantisation, numpy) for small sectors
+# ---------------------------------------------------------------------------
+
+def dense_sector_h(model: AIMModel, nup: int, ndn: int) -> np.ndarray:
+    """Sector Hamiltonian from explicit fermion operators, per-spin Jordan-Wigner.
+
+    H = sum_s sum_{a!=b} t^s_ab c+_{a s} c_{b s} + sum_s sum_a t^s_aa n_{a s}
+      + sum_c U_cc n_c,up n_c,dn + sum_{c<c'} U_cc' n_c n_c'
+      - sum_{c<c'} J_cc' (n_c,up n_c',up + n_c,dn n_c',dn)
+      + [spin flip  J c+_{c,up} c_{c',up} c+_{c',dn} c_{c,dn}  + h.c.]
+      + [pair hop   J c+_{c,up} c_{c',up} c+_{c,dn} c_{c',dn}  for c != c']
+    with the Hund terms active only when |jhund| > 1e-5 and U has an
+    off-diagonal element.  The hopping matrix t^s collects Ec, Eb and Vbc in
+    the bit layout of the library; off-diagonal entries with |t| <= cutoff
+    are dropped, as tab_HAIM2 does.
+    """
+    nc, nb, ns = model.nc, model.nb, model.ns
+    su = [s for s in range(1 << ns) if bin(s).count("1") == nup]
+    sd = [s for s in range(1 << ns) if bin(s).count("1") == ndn]
+    ru = {s: i for i, s in enumerate(su)}
+    rd = {s: i for i, s in enumerate(sd)}
+    dup = len(su)
+    D = dup * len(sd)
+    H = np.zeros((D, D))
+
+    def tmat(spin):
+        t = np.zeros((ns, ns))
+        t[nb:, nb:] = model.ec[spin]
+        t[:nb, :nb] = model.eb[spin]
+        t[:nb, nb:] = model.vbc[spin]
+        t[nb:, :nb] = model.vbc[spin].T
+        for a in range(ns):
+            for b in range(ns):
+                if a != b and not (abs(t[a, b]) > model.cutoff):
+                    t[a, b] = 0.0
+        return t
+
+    def hop(s, a, b):
+        """c+_a c_b |s> with per-species JW sign; returns (sign, state) or None."""
+        if not (s >> b) & 1:
+            return None
+        s1 = s & ~(1 << b)
+        sg = -1 if bin(s1 >> (b + 1)).count("1") & 1 else 1
+        if (s1 >> a) & 1:
+            return None
+        s2 = s1 | (1 << a)
+        if bin(s2 >> (a + 1)).count("1") & 1:
+            sg = -sg
+        return sg, s2
+
+    tt = [tmat(0), tmat(1)]
+    U, JJ = model.u, model.jj
+    offc = any(U[a, b] != 0 for a in range(nc) for b in range(nc) if a != b)
+    hund = abs(model.jhund) > 1e-5 and offc
+    occ = lambda s, p: (s >> p) & 1
+    for iu, s_u in enumerate(su):
+        for id_, s_d in enumerate(sd):
+            i = iu + id_ * dup
+            e = 0.0
+            for a in range(ns):
+                e += tt[0][a, a] * occ(s_u, a) + tt[1][a, a] * occ(s_d, a)
+            for c in range(nc):
+                e += U[c, c] * occ(s_u, nb + c) * occ(s_d, nb + c)
+            for c in range(nc):
+                for c2 in range(c + 1, nc):
+                    n1 = occ(s_u, nb + c) + occ(s_d, nb + c)
+                    n2 = occ(s_u, nb + c2) + occ(s_d, nb + c2)
+                    if U[c, c2] != 0:
+                        e += U[c, c2] * n1 * n2
+                        e -= JJ[c, c2] * (occ(s_u, nb + c) * occ(s_u, nb + c2) +
+                                          occ(s_d, nb + c) * occ(s_d, nb + c2))
+            H[i, i] += e
+            for spin, s, rk in ((0, s_u, ru), (1, s_d, rd)):
+                t = tt[spin]
+                for a in range(ns):
+                    for b in range(ns):
+                        if a == b or t[a, b] == 0:
+                            continue
+                        r = hop(s, a, b)
+                        if r is None:
+                            continue
+                        sg, s2 = r
+                        j = (rk[s2] + id_ * dup) if spin == 0 else (iu + rk[s2] * dup)
+                        H[j, i] += t[a, b] * sg
+            if hund:
+                for c in range(nc):
+                    for c2 in range(nc):
+                        if c == c2 or U[c, c2] == 0:
+                            continue
+                        pc, pc2 = nb + c, nb + c2
+                        # spin flip: up c2 -> c, down c -> c2
+                        ru_ = hop(s_u, pc, pc2)
+                        rd_ = hop(s_d, pc2, pc)
+                        if ru_ and rd_:
+                            j = ru[ru_[1]] + rd[rd_[1]] * dup
+                            H[j, i] += JJ[c, c2] * ru_[0] * rd_[0]
+                        # pair hop: up and down c2 -> c
+                        ru_ = hop(s_u, pc, pc2)
+                        rd_ = hop(s_d, pc, pc2)
+                        if ru_ and rd_:
+                            j = ru[ru_[1]] + rd[rd_[1]] * dup
+                            H[j, i] += JJ[c, c2] * ru_[0] * rd_[0]
+    return H
+
+
+# ---------------------------------------------------------------------------
+# drivers above the Krylov primitives
+# ---------------------------------------------------------------------------
+
+FULL_ED_SWITCH = 40   # ed_solver/Global_Variables.f90:23
+
+
+def solve_sector(model: AIMModel, nup: int, ndn: int, neigen=1, nitermax=1000, tolerance=1e-12,
+                 demax=1e300, ran_tab=None):
+    """Eigenpairs of one sector as get_eigen_energies/get_GS would produce them.
+
+    dim <= FULL_ED_SWITCH: dense diagonalisation (ED_diago, ED_ARPACK.f90:590-715);
+    otherwise Lanczos pass 1 + pass 2.  Returns list of (E, psi).
+    """
+    h = OracleH(model, nup, ndn)
+    if h.dim == 0:
+        return h, []
+    if h.dim <= FULL_ED_SWITCH:
+        w, v = np.linalg.eigh(h.dense())
+        j = min(h.dim, neigen)
+        keep = [0]
+        for i in range(1, j):
+            if w[i] <= w[0] + demax:
+                keep.append(i)
+            else:
+                break
+        return h, [(float(w[i]), v[:, i].copy()) for i in keep]
+    v0 = start_vector(h.dim, ran_tab)
+    r = lanczos_e0(h, v0, nitermax=nitermax, neigen=neigen, tolerance=tolerance, demax=demax)
+    out = []
+    for k in range(len(r["E"])):
+        psi = lanczos_gs(h, r["vecp"][k], v0)
+        out.append((float(r["E"][k]), psi))
+    return h, out
+
+
+def ground_states(model: AIMModel, sectors: Sequence[Tuple[int, int]], beta: float, demax0: float,
+                  neigen=1, nitermax=1000, tolerance=1e-12, ran_tab=None):
+    """Sector scan + global Boltzmann window [E0, E0 + demax0/beta]
+    (solver.h:98-237, eigen_sector_class.f90:274-470, dmft_ed_solver.f90:1468)."""
+    demax = demax0 / beta
+    found = []
+    for (nu, nd) in sectors:
+        h, states = solve_sector(model, nu, nd, neigen=neigen, nitermax=nitermax,
+                                 tolerance=tolerance, demax=demax, ran_tab=ran_tab)
+        if states:
+            e_s = min(e for e, _ in states)
+            for e, psi in states:
+                if e <= e_s + demax:
+                    found.append(dict(sector=(nu, nd), E=e, psi=psi))
+    e0 = min(f["E"] for f in found)
+    gs = [f for f in found if f["E"] <= e0 + demax]
+    z = sum(math.exp(-beta * (f["E"] - e0)) for f in gs)
+    for f in gs:
+        f["boltz"] = math.exp(-beta * (f["E"] - e0)) / z
+    return gs, e0, z
+
+
+def green_impurity(model: AIMModel, gs, beta: float, nw: int, nitergreen: int, spin: int = 0,
+                   pairs: Optional[Sequence[Tuple[int, int]]] = None, cutoff_dynamic=1e-8):
+    """G_ij(i w_n) for impurity orbitals of one spin, the (c, c+) channel of compute_greenAA.
+
+    For each state |psi> with weight boltz: particle part with |phi> = (c+_i [+ c+_j])|psi>,
+    hole part with (c_i [+ c_j])|psi> (real-H symmetric combination), then
+    G_ij = (G_{i+j} - G_ii - G_jj) / 2 for i != j.  Returns dict {(i,j): array(nw)}.
+    """
+    nc = model.nc
+    if pairs is None:
+        pairs = [(i, i) for i in range(nc)]
+    wn = matsubara(beta, nw)
+    combos = sorted(set([(i, i) for (i, j) in pairs] + [(j, j) for (i, j) in pairs] +
+                        [(min(i, j), max(i, j)) for (i, j) in pairs if i != j]))
+    raw = {c: np.zeros(nw, complex) for c in combos}
+    hcache: Dict[Tuple[int, int], OracleH] = {}
+    for st in gs:
+        nu, nd = st["sector"]
+        psi = st["psi"]
+        for iph in (1, 2):
+            dagger = iph == 1
+            for (i, j) in combos:
+                vi, tsec = _try_apply(model, nu, nd, i, spin, dagger, psi)
+                if vi is None:
+                    continue
+                if i != j:
+                    vj, _ = _try_apply(model, nu, nd, j, spin, dagger, psi)
+                    v = vi + vj
+                else:
+                    v = vi
+                if tsec not in hcache:
+                    hcache[tsec] = OracleH(model, *tsec)
+                G, _, _ = green_chain(hcache[tsec], v, nitergreen, st["E"], iph, wn,
+                                      cutoff_dynamic=cutoff_dynamic)
+                raw[(i, j)] += st["boltz"] * G
+    out = {}
+    for (i, j) in pairs:
+        if i == j:
+            out[(i, j)] = raw[(i, i)]
+        else:
+            a, b = min(i, j), max(i, j)
+            out[(i, j)] = 0.5 * (raw[(a, b)] - raw[(a, a)] - raw[(b, b)])
+    return out
+
+
+def _try_apply(model, nu, nd, site, spin, dagger, psi):
+    try:
+        return apply_c(model, nu, nd, site, spin, dagger, psi)
+    except ValueError:
+        return None, None
+
+
+def lehmann_green(model: AIMModel, sectors, beta: float, wn: np.ndarray, site=0, spin=0,
+                  demax=None):
+    """Exact finite-temperature G_ii(i w_n) by full diagonalisation of small sectors."""
+    ns = model.ns
+    eig = {}
+    for (nu, nd) in sectors:
+        H = dense_sector_h(model, nu, nd)
+        w, v = np.linalg.eigh(H)
+        eig[(nu, nd)] = (w, v)
+    e0 = min(w[0] for w, _ in eig.values())
+    z = 0.0
+    G = np.zeros(len(wn), complex)
+    for (nu, nd), (w, v) in eig.items():
+        for n in range(len(w)):
+            if demax is not None and w[n] > e0 + demax:
+                continue
+            z += math.exp(-beta * (w[n] - e0))
+    for (nu, nd), (w, v) in eig.items():
+        tnu, tnd = (nu + 1, nd) if spin == 0 else (nu, nd + 1)
+        if (tnu, tnd) not in eig:
+            continue
+        wt, vt = eig[(tnu, tnd)]
+        for n in range(len(w)):
+            bn = math.exp(-beta * (w[n] - e0))
+            for m in range(len(wt)):
+                bm = math.exp(-beta * (wt[m] - e0))
+                if bn < 1e-300 and bm < 1e-300:
+                    continue
+                phi, _ = apply_c(model, nu, nd, site, spin, True, v[:, n])
+                amp = float(vt[:, m] @ phi) ** 2
+                G += amp * (bn + bm) / (1j * wn - (wt[m] - w[n]))
+    return G / z

@@ -1,0 +1,90 @@
+"""H*v on the device against the CPU oracle: FP64 bit-exact, FP32 within tolerance."""
+import numpy as np
+import pytest
+
+import oracle as O
+from ed_solver_b200 import edk
+from ed_solver_b200.model import star_model, workload
+
+pytestmark = pytest.mark.gpu
+
+
+def _models():
+    rng = np.random.default_rng(21)
+    m1 = star_model(-0.7, 2.0, rng.uniform(-1, 1, 5), rng.uniform(0.2, 0.6, 5))
+    m2 = star_model(-1.0, 3.0, rng.uniform(-1, 1, 4), rng.uniform(0.2, 0.6, 4), orbital_of_bath=[0, 1, 1, 0],
+                    nc=2, J=0.5)
+    m2.ec[:, 0, 1] = m2.ec[:, 1, 0] = 0.3
+    m2.eb[:, 0, 2] = m2.eb[:, 2, 0] = 0.25
+    m3 = star_model([-1.2, -0.8, -1.0], 2.5, rng.uniform(-1, 1, 3), rng.uniform(0.2, 0.6, 3),
+                    orbital_of_bath=[0, 1, 2], nc=3, J=0.3)
+    return [m1, m2, m3]
+
+
+SECTORS = [(3, 3), (2, 4), (4, 1), (0, 3), (5, 5), (1, 0)]
+
+
+@pytest.mark.parametrize("mi", [0, 1, 2])
+def test_hmult_fp64_bit_exact(ctx, mi):
+    import torch
+    m = _models()[mi]
+    rng = np.random.default_rng(mi)
+    for nu, nd in SECTORS:
+        if nu > m.ns or nd > m.ns:
+            continue
+        h = edk.Hamiltonian(ctx, m, nu, nd)
+        ho = O.OracleH(m, nu, nd)
+        x = rng.normal(size=h.dim)
+        y = h.hmult(torch.tensor(x, device="cuda")).cpu().numpy()
+        y_ref = ho.hmult(x)
+        assert np.array_equal(y, y_ref), (nu, nd, np.abs(y - y_ref).max())
+
+
+@pytest.mark.parametrize("mi", [0, 1])
+def test_hmult_fp32(ctx, mi):
+    import torch
+    m = _models()[mi]
+    rng = np.random.default_rng(7)
+    for nu, nd in [(3, 3), (2, 4)]:
+        h = edk.Hamiltonian(ctx, m, nu, nd)
+        x = rng.normal(size=h.dim)
+        y = h.hmult(torch.tensor(x, dtype=torch.float32, device="cuda")).double().cpu().numpy()
+        y_ref = O.OracleH(m, nu, nd).hmult(x.astype(np.float32).astype(np.float64))
+        assert np.abs(y - y_ref).max() <= 2e-6 * np.abs(y_ref).max()
+
+
+def test_hmult_large_rows_c3_sector_bit_exact(ctx):
+    """The ns=14 sector (3432 x 3432 rows): staged rows, packed up table, row schedule."""
+    import torch
+    m = workload("c3").model
+    h = edk.Hamiltonian(ctx, m, 7, 7)
+    ho = O.OracleH(m, 7, 7)
+    rng = np.random.default_rng(3)
+    x = rng.normal(size=h.dim)
+    y = h.hmult(torch.tensor(x, device="cuda")).cpu().numpy()
+    assert np.array_equal(y, ho.hmult(x))
+
+
+def test_hmult_host_buffers(ctx):
+    m = workload("c1").model
+    h = edk.Hamiltonian(ctx, m, 4, 4)
+    x = np.random.default_rng(1).normal(size=h.dim)
+    assert np.array_equal(h.hmult_host(x), O.OracleH(m, 4, 4).hmult(x))
+
+
+def test_hmult_rejects_bad_sizes(ctx):
+    import torch
+    h = edk.Hamiltonian(ctx, workload("c1").model, 4, 4)
+    with pytest.raises(edk.EdkError):
+        edk.lib()  # loaded
+        ctx.check(edk.lib().edk_hmult(h.h, 0, h.dim + 1, torch.zeros(1, device="cuda").data_ptr(),
+                                      torch.zeros(1, device="cuda").data_ptr()), "size")
+
+
+def test_tables_on_device_match_host_builder(ctx):
+    m = workload("c2").model
+    h = edk.Hamiltonian(ctx, m, 5, 4)
+    for spin in (0, 1):
+        p, t, v, d = h.table(spin)
+        p2, t2, v2, d2 = edk.build_table(m, spin, 5 if spin == 0 else 4)
+        assert np.array_equal(t, t2) and np.array_equal(v, v2) and np.array_equal(d, d2)

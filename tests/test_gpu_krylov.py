@@ -1,0 +1,153 @@
+"""Lanczos, c/c+ maps and Green chains on the device against the CPU oracle."""
+import math
+
+import numpy as np
+import pytest
+
+import oracle as O
+from ed_solver_b200 import edk, solver
+from ed_solver_b200.model import star_model, workload, matsubara
+
+pytestmark = pytest.mark.gpu
+
+
+def test_lanczos_e0_and_vector_fp64(ctx):
+    w = workload("c1")
+    m = w.model
+    h = edk.Hamiltonian(ctx, m, 4, 4)
+    ho = O.OracleH(m, 4, 4)
+    r = h.lanczos_e0(nitermax=1000, neigen=1, tolerance=1e-12, check_every=4)
+    ro = O.lanczos_e0(ho, nitermax=1000, neigen=1, tolerance=1e-12)
+    assert abs(r["E"][0] - ro["E"][0]) <= 1e-11 * abs(ro["E"][0])
+    # same start vector -> same Krylov coefficients early on
+    n = min(20, r["niter"], ro["niter"])
+    assert np.allclose(r["diag"][:n], ro["diag"][:n], rtol=1e-9, atol=1e-11)
+    assert np.allclose(r["subdiag"][1:n], ro["subdiag"][1:n], rtol=1e-9, atol=1e-11)
+    assert abs(r["niter"] - ro["niter"]) <= 2
+    psi = h.lanczos_gs(r["vecp"][0]).cpu().numpy()
+    psio = O.lanczos_gs(ho, ro["vecp"][0])
+    s = np.sign(psi @ psio)
+    assert np.abs(psi - s * psio).max() < 1e-7
+    ev = np.linalg.eigvalsh(ho.dense()) if ho.dim <= 5000 else None
+    if ev is not None:
+        assert abs(r["E"][0] - ev[0]) < 1e-10
+    res, nrm = h.residual(h.lanczos_gs(r["vecp"][0]), r["E"][0])
+    assert abs(nrm - 1.0) < 1e-12 and res < 1e-6
+
+
+def test_lanczos_neigen_window(ctx):
+    m = workload("c2").model
+    h = edk.Hamiltonian(ctx, m, 5, 5)
+    ho = O.OracleH(m, 5, 5)
+    r = h.lanczos_e0(neigen=3, tolerance=1e-10, demax=5.0)
+    ro = O.lanczos_e0(ho, neigen=3, tolerance=1e-10, demax=5.0)
+    k = min(len(r["E"]), len(ro["E"]))
+    assert k >= 1
+    assert np.allclose(r["E"][:k], ro["E"][:k], rtol=1e-10, atol=1e-10)
+
+
+def test_lanczos_fp32_then_fp64_residual(ctx):
+    import torch
+    m = workload("c1").model
+    h = edk.Hamiltonian(ctx, m, 4, 4)
+    e64 = h.lanczos_e0(dtype="f64")["E"][0]
+    r = h.lanczos_e0(dtype="f32", tolerance=1e-7)
+    assert abs(r["E"][0] - e64) < 1e-5 * abs(e64)
+    psi = h.lanczos_gs(r["vecp"][0], dtype="f32")
+    res, nrm = h.residual(psi.double(), r["E"][0])
+    assert res < 1e-3
+
+
+def test_zero_start_vector_is_an_error_not_a_fault(ctx):
+    import torch
+    m = workload("c1").model
+    h = edk.Hamiltonian(ctx, m, 4, 4)
+    z = torch.zeros(h.dim, dtype=torch.float64, device="cuda")
+    with pytest.raises(edk.EdkError) as ei:
+        h.lanczos_e0(start=z)
+    assert ei.value.code == edk.EDK_ERR_ZERO_START
+
+
+def test_apply_c_bit_exact(ctx):
+    import torch
+    m = workload("c2").model
+    rng = np.random.default_rng(4)
+    for (nu, nd) in [(5, 5), (0, 3), (10, 2)]:
+        h = edk.Hamiltonian(ctx, m, nu, nd)
+        x = rng.normal(size=h.dim)
+        xt = torch.tensor(x, device="cuda")
+        for spin in (0, 1):
+            for dag in (True, False):
+                for site in (0, 1):
+                    try:
+                        yo, tsec = O.apply_c(m, nu, nd, site, spin, dag, x)
+                    except ValueError:
+                        continue
+                    y, tsec2 = h.apply_c(xt, site, spin, dag)
+                    assert tsec == tsec2
+                    assert np.array_equal(y.cpu().numpy(), yo)
+                y, _ = h.apply_c(xt, 0, spin, True, site2=1, sign2=1) if (nu if spin == 0 else nd) < m.ns else (None, None)
+                if y is not None:
+                    a, _ = O.apply_c(m, nu, nd, 0, spin, True, x)
+                    b, _ = O.apply_c(m, nu, nd, 1, spin, True, x)
+                    assert np.array_equal(y.cpu().numpy(), a + b)
+
+
+def test_green_chain_against_oracle(ctx):
+    import torch
+    w = workload("c1")
+    m = w.model
+    ho = O.OracleH(m, 4, 4)
+    ro = O.lanczos_e0(ho)
+    psi = O.lanczos_gs(ho, ro["vecp"][0])
+    e0 = ro["E"][0]
+    wn = matsubara(w.beta, 256)
+    for iph, dag in ((1, True), (2, False)):
+        phi, tsec = O.apply_c(m, 4, 4, 0, 0, dag, psi)
+        Go, dgo, sdo = O.green_chain(O.OracleH(m, *tsec), phi, 200, e0, iph, wn)
+        ht = edk.Hamiltonian(ctx, m, *tsec)
+        G, dg, sd, n = ht.green_chain(torch.tensor(phi, device="cuda"), 200, e0, iph, wn)
+        assert n == len(dgo)
+        assert np.allclose(dg[:30], dgo[:30], rtol=1e-9, atol=1e-10)
+        assert np.abs(G - Go).max() < 1e-9
+
+
+def test_cf_eval_against_oracle(ctx):
+    rng = np.random.default_rng(8)
+    chains = []
+    for n in (1, 5, 50):
+        chains.append(dict(diag=rng.normal(size=n), subdiag=np.concatenate([[0.0], rng.uniform(0.2, 1, n - 1)]),
+                           e=-1.3, ph=1.0 if n % 2 else -1.0, scale=0.7))
+    wn = matsubara(20.0, 64)
+    G = edk.cf_eval(ctx, chains, wn)
+    for c, g in zip(chains, G):
+        td = c["ph"] * (c["diag"] - c["e"])
+        ref = np.array([O.cf(td, c["subdiag"], 1j * x) for x in wn]) * c["scale"]
+        assert np.abs(g - ref).max() < 1e-12
+
+
+def test_full_green_c1_against_oracle_driver(ctx):
+    w = workload("c1")
+    m = w.model
+    hc = solver.HCache(ctx, m)
+    gs, e0, z = solver.ground_states(hc, w.sectors, w.beta, w.demax0)
+    gso, e0o, zo = O.ground_states(m, w.sectors, w.beta, w.demax0)
+    assert abs(e0 - e0o) < 1e-11 * abs(e0o)
+    G = solver.green_impurity(hc, gs, w.beta, 256, w.nitergreen)[(0, 0)]
+    Go = O.green_impurity(m, gso, w.beta, 256, w.nitergreen)[(0, 0)]
+    assert np.abs(G - Go).max() < 1e-8
+    d, n = hc.get((4, 4)).double_occ(gs[0]["psi"])
+    assert abs(d - O.OracleH(m, 4, 4).double_occ(gso[0]["psi"])) < 1e-9
+
+
+def test_reference_golden_through_the_device(ctx):
+    import os
+    g = np.loadtxt(os.path.join(os.path.dirname(__file__), "golden", "g_bm_2b.txt"))
+    m = star_model(-5.0, 10.0, [0.0, 0.0], [math.sqrt(0.2), math.sqrt(0.3)], orbital_of_bath=[0, 1], nc=2,
+                   Uprime=2.0, J=0.0, cutoff=1e-8)
+    hc = solver.HCache(ctx, m)
+    secs = [(a, b) for a in range(5) for b in range(5)]
+    gs, e0, z = solver.ground_states(hc, secs, 50.0, 50.0, neigen=40, tolerance=1e-13)
+    G = solver.green_impurity(hc, gs, 50.0, len(g), 400, pairs=[(0, 0), (1, 1)])
+    assert np.abs(G[(0, 0)] - (g[:, 1] + 1j * g[:, 2])).max() < 2e-8
+    assert np.abs(G[(1, 1)] - (g[:, 3] + 1j * g[:, 4])).max() < 2e-8
