@@ -1,0 +1,319 @@
+"""Headline benchmark: E0 + G(i w_n) solves of the ns=16 half-filled sector.
+
+One step = one impurity solve of the 1 impurity + 15 bath-site Anderson model
+(1.66e8 states in the (8,8) sector): mixed-precision Lanczos ground state with
+FP64 residual check and one FP64 refinement restart, then the four Green
+chains (c_up, c+_up, c_dn, c+_dn) of 300 steps each and the 512-point
+Matsubara continued fractions (beta = 50).  Every solve goes through the C-ABI
+entry point edk_solve.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Multi-GPU: independent replicas (one solve per rank per step, no collective
+in the data path); value = total solves / max-over-ranks device time.
+The reference arm times the CPU restatement of the reference's FP64 Lanczos
+(OpenMP, all host threads) on a bounded sample of Lanczos steps of the same
+sector and converts it to the same unit with the step count of an FP64 solve.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(name="ns16_halffilled_E0_G512", nc=1, nb=15, sector=(8, 8), beta=50.0, nw=512,
+                nitergreen=300, nitermax=1000, tolerance=1e-12, tolerance_lowprec=1e-6,
+                residual_tol=1e-9, spins=(0, 1), pairs=[(0, 0)], demax0=5.0)
+# H*v applications of one plain FP64 solve of this workload (eigen part + Green part),
+# measured on B200 with the library's start-vector table; used to convert a
+# per-step CPU time into solves/s for the reference arm.
+FP64_STEPS_PER_SOLVE = None
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "row_fast_kernel_step_ns16_f32.txt")
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _traffic_per_launch():
+    """dram__bytes_read.sum + dram__bytes_write.sum of one fused-step launch (ncu summary)."""
+    try:
+        with open(PROFILE_TRAFFIC) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_launch:"):
+                    return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons every 200 ms during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx.append(float(f[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, f[5:9]):
+                    if v.lower() in ("active", "1"):
+                        reasons.add(n)
+        finally:
+            try:
+                os.unlink(self.path)
+            except OSError:
+                pass
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _model():
+    from ed_solver_b200.model import workload
+    return workload("c5").model
+
+
+def _solve(ctx, model, dtype):
+    from ed_solver_b200 import edk
+    w = WORKLOAD
+    return edk.solve(ctx, model, [w["sector"]], w["beta"], w["nw"], dtype=dtype, neigen=1,
+                     nitermax=w["nitermax"], tolerance=w["tolerance"], tolerance_lowprec=w["tolerance_lowprec"],
+                     demax0=w["demax0"], nitergreen=w["nitergreen"], spins=w["spins"], pairs=w["pairs"],
+                     residual_tol=w["residual_tol"])
+
+
+def _cpu_step_time(model, nsteps=2):
+    """Seconds per FP64 Lanczos step of the CPU restatement (all host threads)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    h = O.OracleH(model, *WORKLOAD["sector"])
+    v0 = O.start_vector(h.dim)
+    O.lanczos_steps(h, 1, v0)                      # warm the pages
+    t0 = time.perf_counter()
+    O.lanczos_steps(h, nsteps, v0)
+    dt = (time.perf_counter() - t0) / nsteps
+    return dt, O.num_threads()
+
+
+def run_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    model = _model()
+    steps_per_solve = FP64_STEPS_PER_SOLVE or 1500
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    h = O.OracleH(model, *WORKLOAD["sector"])
+    v0 = O.start_vector(h.dim)
+    for _ in range(args.warmup):
+        O.lanczos_steps(h, 1, v0)
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.lanczos_steps(h, 1, v0)
+        ts.append(time.perf_counter() - t0)
+    t_step = statistics.median(ts)
+    value = 1.0 / (t_step * steps_per_solve)
+    line = {
+        "impl": "reference", "metric": "impurity solves/s (E0 + G(iw_n), ns=16 sector)", "value": value,
+        "unit": "solves/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_step * steps_per_solve * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD["name"], "dim": h.dim, "nw": WORKLOAD["nw"], "beta": WORKLOAD["beta"]},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
+                         "sample": f"{args.steps} FP64 Lanczos steps of the (8,8) sector, median "
+                                   f"{t_step:.3f} s/step, x {steps_per_solve} steps per FP64 solve"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    from ed_solver_b200 import edk
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    ctx = edk.Context(local)
+    model = _model()
+    stream = torch.cuda.current_stream(local)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(local)
+
+    # ---- warm-up (tables built once and kept on the context) ----
+    for _ in range(args.warmup):
+        res = _solve(ctx, model, "f32")
+    barrier()
+    ctx.timing(True)
+    launches0 = ctx.launches
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        ev0.record(stream)
+        results = [_solve(ctx, model, "f32") for _ in range(args.steps)]
+        ev1.record(stream)
+        barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = ctx.launches - launches0
+    n6, t6, e6 = ctx.timing_report(6)          # fused Lanczos step, FP32
+    n5, t5, e5 = ctx.timing_report(5)          # first Lanczos step, FP32
+    ctx.timing(False)
+    clocks = clk.summary()
+    t_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = ws * args.steps / (t_max * 1e-3)
+    res = results[-1]
+
+    out = None
+    if rank == 0:
+        peak, peak_kind = _peaks()
+        step_bytes = 3.0 * 4.0 * e6                      # read v_k, read v_{k-1}, write w per element (FP32)
+        achieved = step_bytes / (t6 * 1e-3) / 1e9 if t6 > 0 else None
+        traffic = _traffic_per_launch()
+        # ---- plain FP64 solve: accuracy reference and speed-up ----
+        torch.cuda.synchronize()
+        e_a, e_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        _solve(ctx, model, "f64")                        # builds FP64 workspace
+        e_a.record(stream)
+        r64 = _solve(ctx, model, "f64")
+        e_b.record(stream)
+        torch.cuda.synchronize()
+        t64 = e_a.elapsed_time(e_b) * 1e-3
+        steps64 = r64["lanczos_steps"] + r64["green_steps"]
+        dG = float(np.abs(res["G"] - r64["G"]).max())
+        dE = abs(res["e0"] - r64["e0"]) / abs(r64["e0"])
+        # ---- end to end: tables rebuilt and uploaded from host arrays every solve ----
+        h2d0, d2h0 = ctx.transfer_bytes()
+        t0 = time.perf_counter()
+        ne2e = 2
+        for _ in range(ne2e):
+            ctx.clear_cache()
+            _solve(ctx, model, "f32")
+        torch.cuda.synchronize()
+        t_e2e = (time.perf_counter() - t0) / ne2e
+        h2d1, d2h1 = ctx.transfer_bytes()
+        # ---- CPU baseline: the CPU restatement on this host ----
+        cpu = None
+        if ws == 1 and not args.no_cpu:
+            t_cpu, cores = _cpu_step_time(model, nsteps=2)
+            cpu = {"value": 1.0 / (t_cpu * steps64), "unit": "solves/s", "cores": cores, "kind": "port",
+                   "sample": f"2 FP64 Lanczos steps of the (8,8) sector ({t_cpu:.3f} s/step) x {steps64} "
+                             f"H*v per FP64 solve"}
+        out = {
+            "metric": "impurity solves/s (E0 + G(iw_n), ns=16 sector)",
+            "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 vectors, f64 alpha/beta/CF (mixed)", "data": "synthetic",
+            "config": {"workload": WORKLOAD["name"], "sector": list(WORKLOAD["sector"]), "dim": 12870 * 12870,
+                       "nw": WORKLOAD["nw"], "beta": WORKLOAD["beta"], "nitergreen": WORKLOAD["nitergreen"],
+                       "chains": 4, "parallelism": f"replicas{ws}",
+                       "l2": "vectors (662 MB FP32) exceed L2 (126 MB); no flush needed"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
+                         "traffic": traffic, "kernel": "row_fast_kernel<float> fused Lanczos step",
+                         "launches": n6, "avg_launch_ms": (t6 / n6) if n6 else None,
+                         "algorithmic_bytes_per_launch": (step_bytes / n6) if n6 else None},
+            "cpu_baseline": cpu,
+            "e2e": {"value": 1.0 / t_e2e, "unit": "solves/s",
+                    "h2d_bytes_per_step": (h2d1 - h2d0) // ne2e, "d2h_bytes_per_step": (d2h1 - d2h0) // ne2e},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "fp64": {"solve_s": t64, "solves_per_s": 1.0 / t64, "hv_steps": steps64},
+            "speedup_mixed_vs_fp64": t64 / (t_max * 1e-3 / args.steps),
+            "accuracy_vs_fp64": {"rel_dE0": dE, "max_abs_dG": dG, "residual": res["residual"],
+                                 "docc": float(res["docc"][0]), "docc_fp64": float(r64["docc"][0])},
+            "mixed": {"hv_steps": res["lanczos_steps"] + res["green_steps"], "e0": res["e0"]},
+        }
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    ctx.close()
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -68,7 +68,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
             if r.returncode != 0:
                 raise RuntimeError(f"compile failed: {cmd[-3]}")
     if jobs or force or not os.path.exists(OUT) or any(os.path.getmtime(o) > os.path.getmtime(OUT) for o in objs):
-        link = [nvcc] + ARCH + ["-shared", "-cudart", "static", "-o", OUT] + objs
+        link = [nvcc] + ARCH + ["-shared", "-cudart", "static", "-Xlinker", "--no-undefined",
+                                "-o", OUT] + objs
         r = subprocess.run(link, capture_output=True, text=True)
         if r.returncode != 0:
             sys.stderr.write(" ".join(link) + "\n" + r.stdout + r.stderr)

@@ -1,0 +1,204 @@
+// Device helpers shared by the row kernels (edk_kernels.cu, edk_rows_fast.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstring>
+#include "edk_internal.h"
+
+namespace edk {
+
+// ---------------------------------------------------------------------------
+// arithmetic without contraction
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double fmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double fadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double fsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+
+template <typename T> __device__ __forceinline__ const T *tab_val(const SpinTabDev &t);
+template <> __device__ __forceinline__ const double *tab_val<double>(const SpinTabDev &t) { return t.val; }
+template <> __device__ __forceinline__ const float *tab_val<float>(const SpinTabDev &t) { return t.valf; }
+template <typename T> __device__ __forceinline__ const T *tab_diag(const SpinTabDev &t);
+template <> __device__ __forceinline__ const double *tab_diag<double>(const SpinTabDev &t) { return t.diag; }
+template <> __device__ __forceinline__ const float *tab_diag<float>(const SpinTabDev &t) { return t.diagf; }
+template <typename T> __device__ __forceinline__ const T *int_coef(const HamDev &h);
+template <> __device__ __forceinline__ const double *int_coef<double>(const HamDev &h) { return h.int_coef; }
+template <> __device__ __forceinline__ const float *int_coef<float>(const HamDev &h) { return h.int_coeff; }
+template <typename T> __device__ __forceinline__ const T *jj_of(const HamDev &h);
+template <> __device__ __forceinline__ const double *jj_of<double>(const HamDev &h) { return h.jj; }
+template <> __device__ __forceinline__ const float *jj_of<float>(const HamDev &h) { return h.jjf; }
+
+// ---------------------------------------------------------------------------
+// deterministic block / grid reductions of NQ doubles
+// ---------------------------------------------------------------------------
+template <int NQ>
+__device__ __forceinline__ void block_sum(double (&v)[NQ], double (*red)[32])
+{
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) red[q][warp] = v[q];
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            double t = lane < nw ? red[q][lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+            v[q] = t;
+        }
+    }
+}
+
+// Writes this block's NQ partial sums; the last block to arrive sums all
+// partials in block order into `out` and returns true (in thread 0 only).
+template <int NQ>
+__device__ bool grid_sum(double (&v)[NQ], double *partials, unsigned *counter, double *out)
+{
+    __shared__ double red[NQ][32];
+    __shared__ bool last;
+    block_sum<NQ>(v, red);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) partials[(size_t)blockIdx.x * NQ + q] = v[q];
+        __threadfence();
+        unsigned t = atomicAdd(counter, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            double t = 0.0;
+            for (unsigned b = lane; b < gridDim.x; b += 32)
+                t += __ldcg(&partials[(size_t)b * NQ + q]);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+            if (lane == 0) out[q] = t;
+        }
+    }
+    if (threadIdx.x == 0) *counter = 0u;
+    return threadIdx.x == 0;
+}
+
+// ---------------------------------------------------------------------------
+// row staging: 16-byte global loads, scalar shared stores (any alignment)
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void stage_row(T *dst, const T *src, int64_t n)
+{
+    constexpr int V = 16 / sizeof(T);
+    const uintptr_t addr = reinterpret_cast<uintptr_t>(src);
+    int64_t head = (int64_t)(((16u - (addr & 15u)) & 15u) / sizeof(T));
+    if (head > n) head = n;
+    for (int64_t i = threadIdx.x; i < head; i += blockDim.x) dst[i] = __ldg(src + i);
+    const int64_t nv = (n - head) / V;
+    const int4 *sv = reinterpret_cast<const int4 *>(src + head);
+    for (int64_t i = threadIdx.x; i < nv; i += blockDim.x) {
+        int4 q = __ldg(sv + i);
+        T tmp[V];
+        memcpy(tmp, &q, 16);
+#pragma unroll
+        for (int v = 0; v < V; ++v) dst[head + i * V + v] = tmp[v];
+    }
+    for (int64_t i = head + nv * V + threadIdx.x; i < n; i += blockDim.x) dst[i] = __ldg(src + i);
+}
+
+
+template <typename T> __device__ __forceinline__ const T *ell_val(const SpinTabDev &t);
+template <> __device__ __forceinline__ const double *ell_val<double>(const SpinTabDev &t) { return t.ell_val; }
+template <> __device__ __forceinline__ const float *ell_val<float>(const SpinTabDev &t) { return t.ell_valf; }
+template <typename T> __device__ __forceinline__ const T *pal_of(const SpinTabDev &t);
+template <> __device__ __forceinline__ const double *pal_of<double>(const SpinTabDev &t) { return t.pal; }
+template <> __device__ __forceinline__ const float *pal_of<float>(const SpinTabDev &t) { return t.palf; }
+
+// L2 eviction-priority policies (createpolicy) and loads/stores carrying them.
+__device__ __forceinline__ uint64_t l2_keep()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t l2_stream()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ float2 ld2(const float *p, uint64_t pol)
+{
+    float2 v;
+    asm volatile("ld.global.nc.L2::cache_hint.v2.f32 {%0,%1}, [%2], %3;" : "=f"(v.x), "=f"(v.y) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ double2 ld2(const double *p, uint64_t pol)
+{
+    double2 v;
+    asm volatile("ld.global.nc.L2::cache_hint.v2.f64 {%0,%1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ void st2(float *p, float a, float b, uint64_t pol)
+{
+    asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1,%2}, %3;" :: "l"(p), "f"(a), "f"(b), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void st2(double *p, double a, double b, uint64_t pol)
+{
+    asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1,%2}, %3;" :: "l"(p), "d"(a), "d"(b), "l"(pol) : "memory");
+}
+__device__ __forceinline__ float ld1(const float *p, uint64_t pol)
+{
+    float v;
+    asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ double ld1(const double *p, uint64_t pol)
+{
+    double v;
+    asm volatile("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ void st1(float *p, float a, uint64_t pol)
+{
+    asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" :: "l"(p), "f"(a), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void st1(double *p, double a, uint64_t pol)
+{
+    asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" :: "l"(p), "d"(a), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void prefetch_l2(const void *p)
+{
+    asm volatile("prefetch.global.L2::evict_last [%0];" :: "l"(p));
+}
+__device__ __forceinline__ uint2 ldu2(const uint32_t *p)
+{
+    return __ldg(reinterpret_cast<const uint2 *>(p));
+}
+
+// Lanczos coefficients from the three grid sums, written by thread 0 of the
+// last block: alpha_{slot+1} = <w,v>, beta_{slot+2}^2 = |w|^2 - 2 alpha <w,v> + alpha^2 |v|^2.
+__device__ __forceinline__ void lanczos_finalize(const RowArgs &a)
+{
+    const double sww = a.sums_out[0], swv = a.sums_out[1], svv = a.sums_out[2];
+    const double al = swv;
+    const double b2 = sww - 2.0 * al * swv + al * al * svv;
+    const int slot = (a.mode == kModeFirst) ? 0 : a.k;
+    double b = b2 > 0.0 ? sqrt(b2) : 0.0;
+    const bool finite = isfinite(al) && isfinite(b2);
+    if (!finite) { a.flags[1] = 1; b = 0.0; }
+    if (b2 <= 1e-28 * sww) b = 0.0;          // relative breakdown: subtraction at rounding level
+    a.tri_diag[slot] = finite ? al : 0.0;
+    a.tri_sub[slot + 1] = b;
+    if (!(b >= a.cutoff) && a.flags[0] == 0) a.flags[0] = slot + 1;
+}
+
+}  // namespace edk

@@ -86,15 +86,25 @@ struct edk_ctx {
     // reduction scratch (partials, counter, sums, flags) and Lanczos coefficients
     DevBuf partials, counter, sums, flags, tri_diag, tri_sub, coef, ran_tab, ran_tab_user;
     DevBuf cf_n, cf_diag, cf_sub, cf_e, cf_ph, cf_scale, cf_wn, cf_G, cf_flag;
+    // Krylov workspace shared by all sector Hamiltonians of this context:
+    // v_{k-1}, v_k, s, s', scratch (per element type), grown on demand
+    DevBuf work[2][5];
     size_t tri_cap = 0;
     int reduce_grid = 0;
+    int kernel_path = 0;     // 0 = fastest applicable row kernel, 1 = generic row kernel only,
+                             // 2/3 = fast kernel launch shape 0/1 when applicable
     // optional event timing of row-kernel launches: (class, start, stop)
     bool timing = false;
-    struct Timed { int cls; cudaEvent_t a, b; };
+    struct Timed { int cls; cudaEvent_t a, b; double elems; };
     std::vector<Timed> timed;
     std::vector<cudaEvent_t> event_pool;
     int64_t t_count[8] = {0};
     double t_ms[8] = {0};
+    double t_elems[8] = {0};
+    // host<->device bytes moved by the library (explicit copies)
+    int64_t h2d_bytes = 0, d2h_bytes = 0;
+    // sector Hamiltonians kept by edk_solve between calls (key: model hash, nup, ndn)
+    std::vector<std::pair<std::string, edk_h *>> hcache;
     cudaEvent_t get_event() {
         if (!event_pool.empty()) { cudaEvent_t e = event_pool.back(); event_pool.pop_back(); return e; }
         cudaEvent_t e = nullptr;
@@ -107,6 +117,7 @@ struct edk_ctx {
             if (cudaEventSynchronize(t.b) == cudaSuccess && cudaEventElapsedTime(&ms, t.a, t.b) == cudaSuccess) {
                 t_ms[t.cls] += ms;
                 t_count[t.cls] += 1;
+                t_elems[t.cls] += t.elems;
             }
             event_pool.push_back(t.a);
             event_pool.push_back(t.b);
@@ -191,8 +202,6 @@ struct edk_h {
     } sd[2];
     DevBuf int_off_d, int_coef_d, int_coeff_d, jj_d, jjf_d, umask_d, row_order_d;
     HamDev H;
-    // Krylov workspace: v_{k-1}, v_k, s, s', psi (per element type)
-    DevBuf work[2][5];
     // apply_c maps keyed by (spin, dagger, site)
     struct CMap {
         int spin, dagger, site;
@@ -277,9 +286,9 @@ int work_ptrs(edk_h *h, int dtype, void *(&w)[5])
 {
     const size_t es = dtype == EDK_F64 ? 8 : 4;
     for (int i = 0; i < 5; ++i) {
-        int rc = h->ctx->cuda(h->work[dtype][i].ensure(es * (size_t)h->dim), "alloc Krylov workspace");
+        int rc = h->ctx->cuda(h->ctx->work[dtype][i].ensure(es * (size_t)h->dim), "alloc Krylov workspace");
         if (rc) return rc;
-        w[i] = h->work[dtype][i].p;
+        w[i] = h->ctx->work[dtype][i].p;
     }
     return EDK_OK;
 }
@@ -300,17 +309,24 @@ RowArgs base_args(edk_h *h)
 int rows(edk_h *h, int dtype, const RowArgs &a)
 {
     edk_ctx *c = h->ctx;
-    LaunchCfg cfg = plan_rows(h->H, dtype == EDK_F64 ? 8 : 4, c->num_sms);
-    cudaEvent_t ea = nullptr, eb = nullptr;
+    const int eb = dtype == EDK_F64 ? 8 : 4;
+    LaunchCfg cfg = plan_rows(h->H, eb, c->num_sms);
+    // the fast kernel uses 2-element vector accesses: every vector must be
+    // aligned to twice the element size
+    auto al = [&](const void *p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) % (2 * eb)) == 0; };
+    const bool aligned = al(a.x) && al(a.y) && al(a.vk) && al(a.vkm1) && al(a.vout) && al(a.psi);
+    cfg.fast = c->kernel_path != 1 && aligned && fast_rows_ok(h->H, eb);
+    cfg.fast_variant = c->kernel_path >= 2 ? c->kernel_path - 2 : -1;
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr;
     if (c->timing) {
-        ea = c->get_event();
-        eb = c->get_event();
-        cudaEventRecord(ea, c->stream);
+        ev_a = c->get_event();
+        ev_b = c->get_event();
+        cudaEventRecord(ev_a, c->stream);
     }
     cudaError_t e = launch_rows(h->H, dtype, a, cfg, c->stream);
     if (c->timing) {
-        cudaEventRecord(eb, c->stream);
-        c->timed.push_back({a.mode + (dtype == EDK_F32 ? 4 : 0), ea, eb});
+        cudaEventRecord(ev_b, c->stream);
+        c->timed.push_back({a.mode + (dtype == EDK_F32 ? 4 : 0), ev_a, ev_b, (double)h->dim});
         if (c->timed.size() > 4096) c->drain_timing();
     }
     c->launches++;
@@ -404,6 +420,7 @@ struct TriHost {
 
 int fetch_tri(edk_ctx *c, int n, TriHost &t)
 {
+    c->d2h_bytes += (int64_t)sizeof(double) * (2 * n + 3) + 8;
     t.diag.resize(n + 1);
     t.sub.resize(n + 2);
     int rc = c->cuda(cudaMemcpyAsync(t.diag.data(), c->tri_diag.p, sizeof(double) * (n + 1),
@@ -512,6 +529,7 @@ int edk_ctx_destroy(edk_ctx *ctx)
 {
     if (!ctx) return EDK_OK;
     cudaStreamSynchronize(ctx->stream);
+    edk_ctx_clear_cache(ctx);
     delete ctx;
     return EDK_OK;
 }
@@ -527,12 +545,23 @@ const char *edk_ctx_last_error(const edk_ctx *ctx) { return ctx ? ctx->last_erro
 
 int64_t edk_ctx_launch_count(const edk_ctx *ctx) { return ctx ? ctx->launches : 0; }
 
+cudaStream_t edk_internal_stream(edk_ctx *ctx) { return ctx->stream; }
+
+int edk_internal_fail(edk_ctx *ctx, int code, const char *msg) { return ctx->fail(code, "%s", msg); }
+
+int edk_ctx_set_kernel_path(edk_ctx *ctx, int path)
+{
+    if (!ctx || path < 0 || path > 3) return EDK_ERR_INVALID;
+    ctx->kernel_path = path;
+    return EDK_OK;
+}
+
 int edk_ctx_timing(edk_ctx *ctx, int enable)
 {
     if (!ctx) return EDK_ERR_INVALID;
     if (enable && !ctx->timing) {
         ctx->drain_timing();
-        for (int i = 0; i < 8; ++i) { ctx->t_count[i] = 0; ctx->t_ms[i] = 0.0; }
+        for (int i = 0; i < 8; ++i) { ctx->t_count[i] = 0; ctx->t_ms[i] = 0.0; ctx->t_elems[i] = 0.0; }
     }
     ctx->timing = enable != 0;
     return EDK_OK;
@@ -545,6 +574,49 @@ int edk_ctx_timing_report(edk_ctx *ctx, int which, int64_t *launches, double *to
     if (launches) *launches = ctx->t_count[which];
     if (total_ms) *total_ms = ctx->t_ms[which];
     return EDK_OK;
+}
+
+int edk_ctx_timing_elements(edk_ctx *ctx, int which, double *elements)
+{
+    if (!ctx || which < 0 || which > 7 || !elements) return EDK_ERR_INVALID;
+    ctx->drain_timing();
+    *elements = ctx->t_elems[which];
+    return EDK_OK;
+}
+
+int edk_ctx_transfer_bytes(const edk_ctx *ctx, int64_t *h2d, int64_t *d2h)
+{
+    if (!ctx) return EDK_ERR_INVALID;
+    if (h2d) *h2d = ctx->h2d_bytes;
+    if (d2h) *d2h = ctx->d2h_bytes;
+    return EDK_OK;
+}
+
+int edk_ctx_clear_cache(edk_ctx *ctx)
+{
+    if (!ctx) return EDK_ERR_INVALID;
+    for (auto &kv : ctx->hcache) edk_h_destroy(kv.second);
+    ctx->hcache.clear();
+    return EDK_OK;
+}
+
+edk_h *edk_internal_cache_get(edk_ctx *ctx, const char *key, size_t len)
+{
+    const std::string k(key, len);
+    for (auto &kv : ctx->hcache)
+        if (kv.first == k) return kv.second;
+    return nullptr;
+}
+
+void edk_internal_cache_put(edk_ctx *ctx, const char *key, size_t len, edk_h *h)
+{
+    ctx->hcache.push_back({std::string(key, len), h});
+}
+
+void edk_internal_count(edk_ctx *ctx, int64_t h2d, int64_t d2h)
+{
+    ctx->h2d_bytes += h2d;
+    ctx->d2h_bytes += d2h;
 }
 
 int edk_h_create(edk_ctx *ctx, const edk_model *m, int nup, int ndn, edk_h **out)
@@ -607,6 +679,8 @@ int edk_h_create(edk_ctx *ctx, const edk_model *m, int nup, int ndn, edk_h **out
     H.nmove = mh.nc * (mh.nc - 1);
     H.hund = h->hund;
     H.ncfg = 1 << mh.nc;
+    for (int64_t r = 0; r < h->ddn; ++r)
+        H.dn_kmax = std::max<int>(H.dn_kmax, h->tab[1].ptr[r + 1] - h->tab[1].ptr[r]);
     H.int_off = h->int_off_d.as<int32_t>();
     H.int_coef = h->int_coef_d.as<double>();
     H.int_coeff = h->int_coeff_d.as<float>();
@@ -614,6 +688,18 @@ int edk_h_create(edk_ctx *ctx, const edk_model *m, int nup, int ndn, edk_h **out
     H.jjf = h->jjf_d.as<float>();
     H.umask = h->umask_d.as<uint8_t>();
     H.row_order = h->row_order_d.as<int32_t>();
+    {
+        // bytes of the device tables just uploaded
+        int64_t b = 0;
+        for (int s = 0; s < 2; ++s) {
+            const SpinTableHost &t = h->tab[s];
+            b += (int64_t)(t.ptr.size() * 4 + t.tgt.size() * 4 + t.val.size() * 12 + t.diag.size() * 12 +
+                           t.imp.size() + t.move.size() * 4 + t.ell.size() * 4 + t.ell_val.size() * 12 +
+                           t.palette.size() * 12);
+        }
+        b += (int64_t)(order.size() * 4 + h->int_coef.size() * 12 + h->int_off.size() * 4);
+        ctx->h2d_bytes += b;
+    }
     *out = h.release();
     return EDK_OK;
 }
@@ -699,7 +785,8 @@ int edk_lanczos_e0(edk_h *h, const edk_lanczos_opts *o, edk_lanczos_result *r)
     std::vector<double> last(ne, 1e300), valp(ne), rdist(ne);
     std::vector<int> conv(ne, 0);
     TriHost T;
-    int checked = 0, stop_at = 0, status = EDK_OK;
+    int checked = 0, stop_at = 0, status = EDK_OK, target_rank = 0;
+    if (o->use_target) ne = 1;
     while (!stop_at) {
         const int target = std::min(niter_max, K.k + every);
         while (K.k < target)
@@ -708,12 +795,29 @@ int edk_lanczos_e0(edk_h *h, const edk_lanczos_opts *o, edk_lanczos_result *r)
         if (T.flags[1]) return c->fail(EDK_ERR_NOT_FINITE, "non-finite Lanczos coefficient");
         for (int it = checked + 1; it <= K.k; ++it) {
             const int m = std::min(ne, it);
-            tridiag_lowest(it, T.diag.data(), T.sub.data() + 1, m, valp.data());
+            if (o->use_target) {
+                // refinement restart: follow the Ritz value nearest the target
+                std::vector<double> all(it);
+                tridiag_lowest(it, T.diag.data(), T.sub.data() + 1, it, all.data());
+                int best = 0;
+                for (int q = 1; q < it; ++q)
+                    if (std::fabs(all[q] - o->target) < std::fabs(all[best] - o->target)) best = q;
+                valp[0] = all[best];
+                target_rank = best;
+            } else {
+                tridiag_lowest(it, T.diag.data(), T.sub.data() + 1, m, valp.data());
+            }
             bool all = true;
             for (int j = 0; j < ne; ++j) {
                 if (j < m) {
                     rdist[j] = valp[j] - last[j];
                     conv[j] = (std::fabs(rdist[j]) < o->tolerance) && it > 2;
+                    if (conv[j] && o->residual_tol > 0.0) {
+                        // Ritz residual |H V y - theta V y| = beta_{it+1} |y_it|
+                        std::vector<double> y(it);
+                        tridiag_vector(it, T.diag.data(), T.sub.data() + 1, valp[j], nullptr, 0, y.data());
+                        conv[j] = std::fabs(T.sub[it] * y[it - 1]) < o->residual_tol;
+                    }
                 }
                 if (!(j < m && conv[j])) all = false;
             }
@@ -732,7 +836,13 @@ int edk_lanczos_e0(edk_h *h, const edk_lanczos_opts *o, edk_lanczos_result *r)
     const int n = stop_at;
     const int m = std::min(ne, n);
     std::vector<double> w(m), vecs((size_t)m * n);
-    tridiag_lowest(n, T.diag.data(), T.sub.data() + 1, m, w.data());
+    if (o->use_target) {
+        std::vector<double> all(n);
+        tridiag_lowest(n, T.diag.data(), T.sub.data() + 1, std::min(n, target_rank + 1), all.data());
+        w[0] = all[std::min(n, target_rank + 1) - 1];
+    } else {
+        tridiag_lowest(n, T.diag.data(), T.sub.data() + 1, m, w.data());
+    }
     int kept = 0;
     for (int j = 0; j < m; ++j) {
         const bool inwin = w[j] >= w[0] && w[j] <= w[0] + o->demax;
@@ -921,6 +1031,8 @@ int edk_cf_eval(edk_ctx *c, int32_t nchain, int32_t ld, const int32_t *n_host, c
     if ((rc = up(c->cf_ph, ph_host, sizeof(double) * nchain))) return rc;
     if ((rc = up(c->cf_scale, scale_host, sizeof(double) * nchain))) return rc;
     if ((rc = up(c->cf_wn, wn_host, sizeof(double) * nw))) return rc;
+    c->h2d_bytes += (int64_t)(sizeof(int32_t) * nchain + sizeof(double) * ((size_t)2 * nchain * ld + 3 * nchain + nw));
+    c->d2h_bytes += (int64_t)(sizeof(double) * 2 * (size_t)nchain * nw);
     if ((rc = c->cuda(c->cf_G.ensure(sizeof(double) * 2 * (size_t)nchain * nw), "alloc"))) return rc;
     if ((rc = c->cuda(c->cf_flag.ensure(sizeof(int)), "alloc"))) return rc;
     if ((rc = c->cuda(cudaMemsetAsync(c->cf_flag.p, 0, sizeof(int), st), "memset"))) return rc;

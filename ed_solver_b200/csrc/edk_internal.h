@@ -48,6 +48,7 @@ struct HamDev {
     int nc = 0, nmove = 0;
     int hund = 0;                      // spin flip / pair hopping active
     int ncfg = 0;                      // 1 << nc
+    int dn_kmax = 0;                   // longest down-table row
     SpinTabDev up, dn;
     const int32_t *int_off = nullptr;  // ncfg*ncfg+1 offsets into the coefficient lists
     const double *int_coef = nullptr;  // per (cfg_up, cfg_dn): the ordered density terms
@@ -87,15 +88,21 @@ struct RowArgs {
 };
 
 struct LaunchCfg {
-    int grid = 0, block = 0, rows = 1;
+    int grid = 0, block = 0, rows = 1, km = 0, num_sms = 1;
+    int64_t groups = 0;
     size_t smem = 0;
     bool stage = true;
+    bool fast = false;       // use row_fast_kernel (edk_rows_fast.cu)
+    int fast_variant = -1;   // -1 = default launch shape of the fast kernel
 };
 
 // ---- kernel launchers (edk_kernels.cu) ------------------------------------
 LaunchCfg plan_rows(const HamDev &H, int elem_bytes, int num_sms);
 cudaError_t launch_rows(const HamDev &H, int dtype, const RowArgs &a, const LaunchCfg &cfg,
                         cudaStream_t st);
+bool fast_rows_ok(const HamDev &H, int elem_bytes);
+cudaError_t launch_rows_fast(const HamDev &H, int dtype, const RowArgs &a, int num_sms, int variant,
+                             cudaStream_t st);
 cudaError_t launch_start_vector(int dtype, int64_t n, const double *ran_tab_dev,
                                 const void *user_start, void *v, double *partials,
                                 unsigned *counter, double *sums_out, int grid, cudaStream_t st);

@@ -34,115 +34,9 @@
 #include <cstdint>
 #include <cstring>
 #include "edk_internal.h"
+#include "edk_device.cuh"
 
 namespace edk {
-
-// ---------------------------------------------------------------------------
-// arithmetic without contraction
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ double fmul(double a, double b) { return __dmul_rn(a, b); }
-__device__ __forceinline__ double fadd(double a, double b) { return __dadd_rn(a, b); }
-__device__ __forceinline__ double fsub(double a, double b) { return __dsub_rn(a, b); }
-__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
-__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
-__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
-
-template <typename T> __device__ __forceinline__ const T *tab_val(const SpinTabDev &t);
-template <> __device__ __forceinline__ const double *tab_val<double>(const SpinTabDev &t) { return t.val; }
-template <> __device__ __forceinline__ const float *tab_val<float>(const SpinTabDev &t) { return t.valf; }
-template <typename T> __device__ __forceinline__ const T *tab_diag(const SpinTabDev &t);
-template <> __device__ __forceinline__ const double *tab_diag<double>(const SpinTabDev &t) { return t.diag; }
-template <> __device__ __forceinline__ const float *tab_diag<float>(const SpinTabDev &t) { return t.diagf; }
-template <typename T> __device__ __forceinline__ const T *int_coef(const HamDev &h);
-template <> __device__ __forceinline__ const double *int_coef<double>(const HamDev &h) { return h.int_coef; }
-template <> __device__ __forceinline__ const float *int_coef<float>(const HamDev &h) { return h.int_coeff; }
-template <typename T> __device__ __forceinline__ const T *jj_of(const HamDev &h);
-template <> __device__ __forceinline__ const double *jj_of<double>(const HamDev &h) { return h.jj; }
-template <> __device__ __forceinline__ const float *jj_of<float>(const HamDev &h) { return h.jjf; }
-
-// ---------------------------------------------------------------------------
-// deterministic block / grid reductions of NQ doubles
-// ---------------------------------------------------------------------------
-template <int NQ>
-__device__ __forceinline__ void block_sum(double (&v)[NQ], double (*red)[32])
-{
-#pragma unroll
-    for (int q = 0; q < NQ; ++q)
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0)
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) red[q][warp] = v[q];
-    __syncthreads();
-    if (warp == 0) {
-        const int nw = (blockDim.x + 31) >> 5;
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) {
-            double t = lane < nw ? red[q][lane] : 0.0;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
-            v[q] = t;
-        }
-    }
-}
-
-// Writes this block's NQ partial sums; the last block to arrive sums all
-// partials in block order into `out` and returns true (in thread 0 only).
-template <int NQ>
-__device__ bool grid_sum(double (&v)[NQ], double *partials, unsigned *counter, double *out)
-{
-    __shared__ double red[NQ][32];
-    __shared__ bool last;
-    block_sum<NQ>(v, red);
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) partials[(size_t)blockIdx.x * NQ + q] = v[q];
-        __threadfence();
-        unsigned t = atomicAdd(counter, 1u);
-        last = (t == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (!last) return false;
-    __threadfence();
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) {
-            double t = 0.0;
-            for (unsigned b = lane; b < gridDim.x; b += 32)
-                t += __ldcg(&partials[(size_t)b * NQ + q]);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
-            if (lane == 0) out[q] = t;
-        }
-    }
-    if (threadIdx.x == 0) *counter = 0u;
-    return threadIdx.x == 0;
-}
-
-// ---------------------------------------------------------------------------
-// row staging: 16-byte global loads, scalar shared stores (any alignment)
-// ---------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ void stage_row(T *dst, const T *src, int64_t n)
-{
-    constexpr int V = 16 / sizeof(T);
-    const uintptr_t addr = reinterpret_cast<uintptr_t>(src);
-    int64_t head = (int64_t)(((16u - (addr & 15u)) & 15u) / sizeof(T));
-    if (head > n) head = n;
-    for (int64_t i = threadIdx.x; i < head; i += blockDim.x) dst[i] = __ldg(src + i);
-    const int64_t nv = (n - head) / V;
-    const int4 *sv = reinterpret_cast<const int4 *>(src + head);
-    for (int64_t i = threadIdx.x; i < nv; i += blockDim.x) {
-        int4 q = __ldg(sv + i);
-        T tmp[V];
-        memcpy(tmp, &q, 16);
-#pragma unroll
-        for (int v = 0; v < V; ++v) dst[head + i * V + v] = tmp[v];
-    }
-    for (int64_t i = head + nv * V + threadIdx.x; i < n; i += blockDim.x) dst[i] = __ldg(src + i);
-}
 
 // one electron of one spin moved between impurity sites a -> b
 __device__ __forceinline__ int move_index(int a, int b, int nc)
@@ -198,20 +92,22 @@ __device__ __forceinline__ T hund_terms(const HamDev &H, const T *x, int64_t iup
 // ---------------------------------------------------------------------------
 // fused row kernel
 // ---------------------------------------------------------------------------
-template <typename T> __device__ __forceinline__ const T *ell_val(const SpinTabDev &t);
-template <> __device__ __forceinline__ const double *ell_val<double>(const SpinTabDev &t) { return t.ell_val; }
-template <> __device__ __forceinline__ const float *ell_val<float>(const SpinTabDev &t) { return t.ell_valf; }
-template <typename T> __device__ __forceinline__ const T *pal_of(const SpinTabDev &t);
-template <> __device__ __forceinline__ const double *pal_of<double>(const SpinTabDev &t) { return t.pal; }
-template <> __device__ __forceinline__ const float *pal_of<float>(const SpinTabDev &t) { return t.palf; }
 
-template <int R> struct RowBounds { static constexpr int kThreads = R >= 8 ? 512 : 1024; };
-
-template <typename T, int R, bool STAGE, bool PACKED>
-__global__ void __launch_bounds__(RowBounds<R>::kThreads, 1) row_kernel(const HamDev H, const RowArgs a)
+// Row kernel.  T: element type; R: rows per group (register accumulators);
+// STAGE: rows staged in shared memory; PACKED: 24+8-bit up-table entries;
+// KM: compile-time bound on up-table width and down-table row length (8 or 16;
+// 0 = dynamic loops for wide generic tables).  With KM > 0 every table entry
+// and every neighbour-row element of a column is loaded before the in-order
+// accumulation starts, so each thread keeps R*KM independent loads in flight.
+template <typename T, int R, bool STAGE, bool PACKED, int KM>
+__global__ void __launch_bounds__(512, 1) row_kernel(const HamDev H, const RowArgs a)
 {
+    constexpr int KB = KM > 0 ? KM : 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ T pal_s[256];
+    __shared__ int s_nd[R];
+    __shared__ int s_jd[R][KB];
+    __shared__ T s_hd[R][KB];
     T *xs = reinterpret_cast<T *>(smem_raw);
     const int64_t dup = H.dup, ddn = H.ddn;
     const T *__restrict__ x = static_cast<const T *>(a.x);
@@ -219,7 +115,8 @@ __global__ void __launch_bounds__(RowBounds<R>::kThreads, 1) row_kernel(const Ha
     double alpha = 0.0, beta_k = 0.0, beta_k1 = 0.0, inv_b = 0.0, cpsi = 0.0;
     if (a.mode == kModeStep) {
         beta_k1 = a.tri_sub[a.k];
-        if (!(beta_k1 >= a.cutoff)) return;            // breakdown recorded by the previous launch
+        // the chain already ended (breakdown recorded by an earlier launch)
+        if (!(beta_k1 >= a.cutoff) || a.flags[0] != 0) return;            // breakdown recorded by the previous launch
         alpha = a.tri_diag[a.k - 1];
         beta_k = a.k >= 2 ? a.tri_sub[a.k - 1] : 0.0;
         inv_b = 1.0 / beta_k1;
@@ -228,7 +125,6 @@ __global__ void __launch_bounds__(RowBounds<R>::kThreads, 1) row_kernel(const Ha
     if (PACKED) {
         const T *p = pal_of<T>(H.up);
         for (int i = threadIdx.x; i < H.up.npal; i += blockDim.x) pal_s[i] = p[i];
-        if (!STAGE) __syncthreads();
     }
 
     const uint32_t *__restrict__ ell = H.up.ell;
@@ -252,54 +148,117 @@ __global__ void __launch_bounds__(RowBounds<R>::kThreads, 1) row_kernel(const Ha
             dd[r] = row[r] >= 0 ? dnd[row[r]] : T(0);
             cd[r] = row[r] >= 0 ? (int)H.dn.imp[row[r]] : 0;
         }
+        __syncthreads();                                 // previous group done with shared data
+        if (KM > 0) {
+            for (int t = threadIdx.x; t < R * KM; t += blockDim.x) {
+                const int r = t / KM, f = t % KM;
+                int nd = 0, jd = 0;
+                T hd = T(0);
+                if (row[r] >= 0) {
+                    const int f0 = H.dn.ptr[row[r]];
+                    nd = H.dn.ptr[row[r] + 1] - f0;
+                    if (f < nd) { jd = H.dn.tgt[f0 + f]; hd = dnv[f0 + f]; }
+                }
+                s_jd[r][f] = jd;
+                s_hd[r][f] = hd;
+                if (f == 0) s_nd[r] = nd;
+            }
+        }
         if (STAGE) {
-            __syncthreads();
 #pragma unroll
             for (int r = 0; r < R; ++r)
                 if (row[r] >= 0) stage_row<T>(xs + (size_t)r * dup, x + (int64_t)row[r] * dup, dup);
-            __syncthreads();
         }
+        __syncthreads();
         for (int64_t c = threadIdx.x; c < dup; c += blockDim.x) {
             const int cu = H.up.imp[c];
             const T du = upd[c];
             T acc[R], xo[R];
+            if (KM > 0) {
+                // ---- issue every load of this column first ----
+                uint32_t ent[KB];
+                T hv[KB];
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                if (row[r] < 0) { acc[r] = T(0); xo[r] = T(0); continue; }
-                xo[r] = STAGE ? xs[(size_t)r * dup + c] : __ldg(x + (int64_t)row[r] * dup + c);
-                // ordered density terms (U, U', -J) for this pair of impurity configurations
-                const int cfg = cu * H.ncfg + cd[r];
-                const int o0 = H.int_off[cfg], o1 = H.int_off[cfg + 1];
-                T ac = T(0);
-                for (int o = o0; o < o1; ++o) ac = fadd(ac, fmul(icoef[o], xo[r]));
-                acc[r] = fadd(ac, fmul(fadd(du, dd[r]), xo[r]));
-            }
-            // up-spin hops: targets inside the same row (column-major padded table)
-            for (int k = 0; k < K; ++k) {
-                const uint32_t ent = __ldg(ell + (int64_t)k * dup + c);
-                int64_t j;
-                T h;
-                if (PACKED) { j = (int64_t)(ent & 0xFFFFFFu); h = pal_s[ent >> 24]; }
-                else { j = (int64_t)(int32_t)ent; h = __ldg(ellv + (int64_t)k * dup + c); }
+                for (int k = 0; k < KB; ++k) {
+                    if (k < K) {
+                        ent[k] = __ldg(ell + (int64_t)k * dup + c);
+                        if (!PACKED) hv[k] = __ldg(ellv + (int64_t)k * dup + c);
+                    } else {
+                        ent[k] = (uint32_t)c;
+                        if (!PACKED) hv[k] = T(0);
+                    }
+                }
+                T xd[R][KB];
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+#pragma unroll
+                    for (int f = 0; f < KB; ++f)
+                        xd[r][f] = (row[r] >= 0 && f < s_nd[r]) ? __ldg(x + (int64_t)s_jd[r][f] * dup + c) : T(0);
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    xo[r] = row[r] < 0 ? T(0) : (STAGE ? xs[(size_t)r * dup + c] : __ldg(x + (int64_t)row[r] * dup + c));
+                // ---- accumulate in the reference order ----
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int cfg = cu * H.ncfg + cd[r];
+                    const int o0 = H.int_off[cfg], o1 = H.int_off[cfg + 1];
+                    T ac = T(0);
+                    for (int o = o0; o < o1; ++o) ac = fadd(ac, fmul(icoef[o], xo[r]));
+                    acc[r] = fadd(ac, fmul(fadd(du, dd[r]), xo[r]));
+                }
+#pragma unroll
+                for (int k = 0; k < KB; ++k) {
+                    if (k >= K) break;
+                    const int64_t j = PACKED ? (int64_t)(ent[k] & 0xFFFFFFu) : (int64_t)(int32_t)ent[k];
+                    const T h = PACKED ? pal_s[ent[k] >> 24] : hv[k];
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const T xj = STAGE ? xs[(size_t)r * dup + j] : __ldg(x + (int64_t)row[r] * dup + j);
+                        acc[r] = fadd(acc[r], fmul(h, xj));
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+#pragma unroll
+                    for (int f = 0; f < KB; ++f)
+                        if (f < s_nd[r]) acc[r] = fadd(acc[r], fmul(s_hd[r][f], xd[r][f]));
+                    if (H.hund && row[r] >= 0) acc[r] = hund_terms<T>(H, x, c, row[r], cu, cd[r], acc[r]);
+                }
+            } else {
+                // ---- generic tables: dynamic loops ----
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    if (row[r] < 0) { acc[r] = T(0); xo[r] = T(0); continue; }
+                    xo[r] = STAGE ? xs[(size_t)r * dup + c] : __ldg(x + (int64_t)row[r] * dup + c);
+                    const int cfg = cu * H.ncfg + cd[r];
+                    const int o0 = H.int_off[cfg], o1 = H.int_off[cfg + 1];
+                    T ac = T(0);
+                    for (int o = o0; o < o1; ++o) ac = fadd(ac, fmul(icoef[o], xo[r]));
+                    acc[r] = fadd(ac, fmul(fadd(du, dd[r]), xo[r]));
+                }
+                for (int k = 0; k < K; ++k) {
+                    const uint32_t ent = __ldg(ell + (int64_t)k * dup + c);
+                    const int64_t j = PACKED ? (int64_t)(ent & 0xFFFFFFu) : (int64_t)(int32_t)ent;
+                    const T h = PACKED ? pal_s[ent >> 24] : __ldg(ellv + (int64_t)k * dup + c);
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        if (row[r] < 0) continue;
+                        const T xj = STAGE ? xs[(size_t)r * dup + j] : __ldg(x + (int64_t)row[r] * dup + j);
+                        acc[r] = fadd(acc[r], fmul(h, xj));
+                    }
+                }
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     if (row[r] < 0) continue;
-                    const T xj = STAGE ? xs[(size_t)r * dup + j] : __ldg(x + (int64_t)row[r] * dup + j);
-                    acc[r] = fadd(acc[r], fmul(h, xj));
+                    const int f0 = H.dn.ptr[row[r]], f1 = H.dn.ptr[row[r] + 1];
+                    for (int f = f0; f < f1; ++f) {
+                        const int64_t jd = H.dn.tgt[f];
+                        acc[r] = fadd(acc[r], fmul(dnv[f], __ldg(x + jd * dup + c)));
+                    }
+                    if (H.hund) acc[r] = hund_terms<T>(H, x, c, row[r], cu, cd[r], acc[r]);
                 }
             }
-            // down-spin hops: whole neighbour rows, coalesced along c
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                if (row[r] < 0) continue;
-                const int f0 = H.dn.ptr[row[r]], f1 = H.dn.ptr[row[r] + 1];
-                for (int f = f0; f < f1; ++f) {
-                    const int64_t jd = H.dn.tgt[f];
-                    acc[r] = fadd(acc[r], fmul(dnv[f], __ldg(x + jd * dup + c)));
-                }
-                if (H.hund) acc[r] = hund_terms<T>(H, x, c, row[r], cu, cd[r], acc[r]);
-            }
-            // epilogue
+            // ---- epilogue ----
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 if (row[r] < 0) continue;
@@ -336,23 +295,8 @@ __global__ void __launch_bounds__(RowBounds<R>::kThreads, 1) row_kernel(const Ha
     if (a.mode == kModeHv) return;
 
     double v[4] = {s0, s1, s2, s3};
-    if (grid_sum<4>(v, a.partials, a.counter, a.sums_out)) {
-        // thread 0 of the last block: Lanczos coefficients for the next launch
-        if (a.mode == kModeFirst || a.mode == kModeStep) {
-            const double sww = a.sums_out[0], swv = a.sums_out[1], svv = a.sums_out[2];
-            const double al = swv;
-            const double b2 = sww - 2.0 * al * swv + al * al * svv;
-            const int slot = (a.mode == kModeFirst) ? 0 : a.k;       // alpha_{slot+1}
-            double b = b2 > 0.0 ? sqrt(b2) : 0.0;
-            const bool finite = isfinite(al) && isfinite(b2);
-            if (!finite) { a.flags[1] = 1; b = 0.0; }
-            // relative breakdown: the subtraction is at rounding level
-            if (b2 <= 1e-28 * sww) b = 0.0;
-            a.tri_diag[slot] = finite ? al : 0.0;
-            a.tri_sub[slot + 1] = b;
-            if (!(b >= a.cutoff) && a.flags[0] == 0) a.flags[0] = slot + 1;
-        }
-    }
+    if (grid_sum<4>(v, a.partials, a.counter, a.sums_out))
+        if (a.mode == kModeFirst || a.mode == kModeStep) lanczos_finalize(a);
 }
 
 // ---------------------------------------------------------------------------
@@ -509,76 +453,103 @@ LaunchCfg plan_rows(const HamDev &H, int elem_bytes, int num_sms)
 {
     LaunchCfg c;
     const int64_t rowbytes = H.dup * (int64_t)elem_bytes;
-    int R;
-    if (rowbytes <= kMaxSmemBytes) {
-        int64_t cap = kMaxSmemBytes / (rowbytes > 0 ? rowbytes : 1);
-        R = cap >= 8 ? 8 : cap >= 4 ? 4 : cap >= 2 ? 2 : 1;
+    const int kmax = H.up.ell_k > H.dn_kmax ? H.up.ell_k : H.dn_kmax;
+    c.km = kmax <= 8 ? 8 : kmax <= 16 ? 16 : 0;
+    // register budget: R*KM loaded values per thread under a 64-register cap
+    int rcap = elem_bytes == 4 ? (c.km == 16 ? 2 : 4) : (c.km == 16 ? 1 : 2);
+    if (c.km == 0) rcap = 4;
+    // two blocks per SM when the staged rows fit in half of the shared memory
+    const int64_t half = kMaxSmemBytes / 2;
+    int R = 0;
+    if (rowbytes <= half) {
+        const int64_t cap = half / (rowbytes > 0 ? rowbytes : 1);
+        R = cap >= 4 ? 4 : cap >= 2 ? 2 : 1;
+        c.stage = true;
+    } else if (rowbytes <= kMaxSmemBytes) {
+        R = 1;
         c.stage = true;
     } else {
-        R = 4;
+        R = 2;
         c.stage = false;
     }
+    if (R > rcap) R = rcap;
     while (R > 1 && (H.ddn + R - 1) / R < num_sms) R >>= 1;   // keep every SM busy
     c.rows = R;
-    const int maxb = R >= 8 ? 512 : 1024;
-    int block = maxb;
-    if (H.dup < maxb) block = (int)(((H.dup + 31) / 32) * 32);
+    int block = 512;
+    if (H.dup < block) block = (int)(((H.dup + 31) / 32) * 32);
     if (block < 64) block = 64;
     c.block = block;
     c.smem = c.stage ? (size_t)R * (size_t)rowbytes : 0;
     const int64_t groups = (H.ddn + R - 1) / R;
-    int per_sm = 2048 / block;
+    int per_sm = 1024 / block;
     if (per_sm > 16) per_sm = 16;
     if (c.smem > 0) {
-        int by_smem = (int)((228 * 1024) / (c.smem + 1024));
+        int by_smem = (int)((228 * 1024) / (c.smem + 4096));
         if (by_smem < per_sm) per_sm = by_smem;
     }
     if (per_sm < 1) per_sm = 1;
     int64_t grid = (int64_t)num_sms * per_sm;
     if (grid > groups) grid = groups;
     if (grid < 1) grid = 1;
-    c.grid = (int)grid;
+    c.grid = (int)grid;          // upper bound; the launcher trims it to the resident blocks
+    c.groups = groups;
+    c.num_sms = num_sms;
     return c;
 }
 
-template <typename T, int R, bool S>
-static cudaError_t launch_rows_t(const HamDev &H, const RowArgs &a, const LaunchCfg &cfg,
-                                 cudaStream_t st)
+template <typename T, int R, bool S, bool P, int KM>
+static cudaError_t launch_rows_k(const HamDev &H, const RowArgs &a, const LaunchCfg &cfg, cudaStream_t st)
 {
-    auto k = H.up.packed ? row_kernel<T, R, S, true> : row_kernel<T, R, S, false>;
-    if (cfg.smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)cfg.smem);
+    auto k = row_kernel<T, R, S, P, KM>;
+    if (cfg.smem > 0) {
+        // static + dynamic shared memory may exceed the 48 KB default
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem);
         if (e != cudaSuccess) return e;
     }
-    k<<<cfg.grid, cfg.block, cfg.smem, st>>>(H, a);
+    // grid = resident blocks (registers and shared memory of this instance)
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, cfg.block, cfg.smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    int64_t grid = (int64_t)cfg.num_sms * per_sm;
+    if (grid > cfg.groups) grid = cfg.groups;
+    if (grid > cfg.grid) grid = cfg.grid;
+    if (grid < 1) grid = 1;
+    k<<<(int)grid, cfg.block, cfg.smem, st>>>(H, a);
     return cudaGetLastError();
 }
 
+template <typename T, int R, bool S>
+static cudaError_t launch_rows_t(const HamDev &H, const RowArgs &a, const LaunchCfg &cfg, cudaStream_t st)
+{
+    const bool p = H.up.packed != 0;
+    switch (cfg.km) {
+        case 8: return p ? launch_rows_k<T, R, S, true, 8>(H, a, cfg, st) : launch_rows_k<T, R, S, false, 8>(H, a, cfg, st);
+        case 16: return p ? launch_rows_k<T, R, S, true, 16>(H, a, cfg, st) : launch_rows_k<T, R, S, false, 16>(H, a, cfg, st);
+        default: return p ? launch_rows_k<T, R, S, true, 0>(H, a, cfg, st) : launch_rows_k<T, R, S, false, 0>(H, a, cfg, st);
+    }
+}
+
 template <typename T>
-static cudaError_t launch_rows_r(const HamDev &H, const RowArgs &a, const LaunchCfg &cfg,
-                                 cudaStream_t st)
+static cudaError_t launch_rows_r(const HamDev &H, const RowArgs &a, const LaunchCfg &cfg, cudaStream_t st)
 {
     if (cfg.stage) {
         switch (cfg.rows) {
-            case 8: return launch_rows_t<T, 8, true>(H, a, cfg, st);
             case 4: return launch_rows_t<T, 4, true>(H, a, cfg, st);
             case 2: return launch_rows_t<T, 2, true>(H, a, cfg, st);
             default: return launch_rows_t<T, 1, true>(H, a, cfg, st);
         }
     }
     switch (cfg.rows) {
-        case 4: return launch_rows_t<T, 4, false>(H, a, cfg, st);
         case 2: return launch_rows_t<T, 2, false>(H, a, cfg, st);
         default: return launch_rows_t<T, 1, false>(H, a, cfg, st);
     }
 }
 
-cudaError_t launch_rows(const HamDev &H, int dtype, const RowArgs &a, const LaunchCfg &cfg,
-                        cudaStream_t st)
+cudaError_t launch_rows(const HamDev &H, int dtype, const RowArgs &a, const LaunchCfg &cfg, cudaStream_t st)
 {
-    return dtype == EDK_F64 ? launch_rows_r<double>(H, a, cfg, st)
-                            : launch_rows_r<float>(H, a, cfg, st);
+    if (cfg.fast) return launch_rows_fast(H, dtype, a, cfg.num_sms, cfg.fast_variant, st);
+    return dtype == EDK_F64 ? launch_rows_r<double>(H, a, cfg, st) : launch_rows_r<float>(H, a, cfg, st);
 }
 
 cudaError_t launch_start_vector(int dtype, int64_t n, const double *tab, const void *user, void *v,

@@ -1,0 +1,344 @@
+// edk_solve: the impurity-solver driver above the Krylov entry points.
+//
+// Restates, for the (N_up, N_dn) basis, the chain the reference runs for one
+// DMFT iteration of the solver:
+//   get_eigen_energies / get_GS (solver.h:11-237): sector scan, Lanczos pass 1
+//     and pass 2 (dense diagonalisation below FULL_ED_SWITCH, ED_ARPACK.f90:590-715),
+//     then the global window [E0, E0 + dEmax] and Boltzmann weights
+//     (eigen_class.f90:322-450, eigen_sector_class.f90:431-446);
+//   compute_greenAA (green_class_computeAA.f90:40-185) for the (c, c+)
+//     channel of the requested impurity orbital pairs and spins: particle and
+//     hole chains from (c+_i [+ c+_j])|psi> and (c_i [+ c_j])|psi>
+//     (green_class_compute_symmetric_combination.f90:39-138), continued
+//     fractions on the Matsubara axis, and the off-diagonal reshuffle
+//     G_ij = (G_{i+j} - G_ii - G_jj)/2 (green_class_compute_symmetric_combination_AA.h:10-60);
+//   the double occupancy of each impurity orbital (correlations_write.h:93-95).
+// Mixed precision (dtype EDK_F32): both Lanczos passes and the Green chains
+// run on FP32 vectors; every ground state is checked with the FP64 matvec and
+// refined once by an FP64 Lanczos restart from the FP32 vector.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "edk_internal.h"
+#include "edk_tridiag.h"
+
+namespace {
+
+struct DBuf {
+    void *p = nullptr;
+    DBuf() = default;
+    explicit DBuf(size_t bytes) { if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) p = nullptr; }
+    DBuf(DBuf &&o) noexcept : p(o.p) { o.p = nullptr; }
+    DBuf &operator=(DBuf &&o) noexcept { std::swap(p, o.p); return *this; }
+    DBuf(const DBuf &) = delete;
+    ~DBuf() { if (p) cudaFree(p); }
+};
+
+struct State {
+    int nup, ndn;
+    double E;
+    int dtype;                 // element type of psi
+    DBuf psi;
+    double boltz = 0.0;
+};
+
+}  // namespace
+
+#include <string>
+
+extern "C" {
+
+edk_h *edk_internal_cache_get(edk_ctx *ctx, const char *key, size_t len);
+void edk_internal_cache_put(edk_ctx *ctx, const char *key, size_t len, edk_h *h);
+cudaStream_t edk_internal_stream(edk_ctx *ctx);
+int edk_internal_fail(edk_ctx *ctx, int code, const char *msg);
+void edk_internal_count(edk_ctx *ctx, int64_t h2d, int64_t d2h);
+
+int edk_convert(edk_ctx *ctx, int from_dtype, int to_dtype, int64_t n, const void *in_dev, void *out_dev)
+{
+    if (!ctx || !in_dev || !out_dev || n < 0) return EDK_ERR_INVALID;
+    cudaError_t e = edk::launch_convert(from_dtype, to_dtype, n, in_dev, out_dev, edk_internal_stream(ctx));
+    if (e != cudaSuccess) return edk_internal_fail(ctx, EDK_ERR_CUDA, cudaGetErrorString(e));
+    return EDK_OK;
+}
+
+int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_solve_result *r)
+{
+    if (!ctx || !m || !o || !r || !o->sectors || o->nsectors < 1 || o->nw < 0 || o->beta <= 0)
+        return EDK_ERR_INVALID;
+    if (o->dtype != EDK_F64 && o->dtype != EDK_F32) return edk_internal_fail(ctx, EDK_ERR_INVALID, "dtype");
+    if (o->npairs > 0 && !o->pairs) return edk_internal_fail(ctx, EDK_ERR_INVALID, "pairs");
+    const int ns = m->nc + m->nb;
+    cudaStream_t st = edk_internal_stream(ctx);
+    const double demax = o->demax0 / o->beta;
+    const size_t ebytes = o->dtype == EDK_F64 ? 8 : 4;
+    int rc;
+
+    // sector Hamiltonians are kept on the context, keyed by the model's bytes and the sector
+    std::string mkey;
+    {
+        auto put = [&](const void *p, size_t n) { mkey.append(static_cast<const char *>(p), n); };
+        put(&m->nc, 4); put(&m->nb, 4);
+        put(m->ec, sizeof(double) * 2 * m->nc * m->nc);
+        if (m->nb > 0) { put(m->eb, sizeof(double) * 2 * m->nb * m->nb); put(m->vbc, sizeof(double) * 2 * m->nb * m->nc); }
+        put(m->u, sizeof(double) * m->nc * m->nc);
+        put(m->jj, sizeof(double) * m->nc * m->nc);
+        put(&m->jhund, 8); put(&m->cutoff_hamilt_param, 8);
+    }
+    auto getH = [&](int nu, int nd, edk_h **out) -> int {
+        std::string key = mkey;
+        key.append(reinterpret_cast<const char *>(&nu), 4);
+        key.append(reinterpret_cast<const char *>(&nd), 4);
+        if (edk_h *h = edk_internal_cache_get(ctx, key.data(), key.size())) { *out = h; return EDK_OK; }
+        edk_h *h = nullptr;
+        int rc2 = edk_h_create(ctx, m, nu, nd, &h);
+        if (rc2) return rc2;
+        edk_internal_cache_put(ctx, key.data(), key.size(), h);
+        *out = h;
+        return EDK_OK;
+    };
+
+    // ---------------- eigenstates ----------------
+    std::vector<std::unique_ptr<State>> states;
+    int64_t lanczos_steps = 0;
+    double e0_low = 1e300;
+    const int cap = std::max(4, o->nitermax + 4);
+    std::vector<double> diag(cap), sub(cap), vecp((size_t)cap * std::max(1, o->neigen));
+    for (int s = 0; s < o->nsectors; ++s) {
+        const int nu = o->sectors[2 * s], nd = o->sectors[2 * s + 1];
+        if (nu < 0 || nu > ns || nd < 0 || nd > ns) return edk_internal_fail(ctx, EDK_ERR_INVALID, "sector");
+        edk_h *h = nullptr;
+        if ((rc = getH(nu, nd, &h))) return rc;
+        int64_t dim = 0;
+        edk_h_dims(h, &dim, nullptr, nullptr);
+        if (dim == 0) continue;
+        std::vector<std::unique_ptr<State>> found;
+        if (dim <= 40) {
+            // dense H from Hmult__ on unit vectors, FP64
+            DBuf ecol((size_t)dim * 8), hcol((size_t)dim * dim * 8);
+            std::vector<double> unit(dim, 0.0), Hd((size_t)dim * dim);
+            for (int64_t i = 0; i < dim; ++i) {
+                unit.assign(dim, 0.0);
+                unit[i] = 1.0;
+                cudaMemcpyAsync(ecol.p, unit.data(), dim * 8, cudaMemcpyHostToDevice, st);
+                edk_internal_count(ctx, dim * 8, 0);
+                if ((rc = edk_hmult(h, EDK_F64, dim, ecol.p, (char *)hcol.p + (size_t)i * dim * 8))) return rc;
+                cudaStreamSynchronize(st);
+            }
+            cudaMemcpy(Hd.data(), hcol.p, (size_t)dim * dim * 8, cudaMemcpyDeviceToHost);
+            lanczos_steps += dim;
+            // Hd holds columns; H is symmetric so the row-major reading is the same matrix
+            std::vector<double> w, V;
+            edk::dense_eigh((int)dim, Hd, w, V);
+            const int j = (int)std::min<int64_t>(dim, o->neigen);
+            for (int k = 0; k < j; ++k) {
+                if (k > 0 && !(w[k] <= w[0] + demax)) break;
+                auto stt = std::make_unique<State>();
+                stt->nup = nu; stt->ndn = nd; stt->E = w[k]; stt->dtype = EDK_F64;
+                stt->psi = DBuf((size_t)dim * 8);
+                std::vector<double> col(dim);
+                for (int64_t q = 0; q < dim; ++q) col[q] = V[(size_t)q * dim + k];
+                cudaMemcpy(stt->psi.p, col.data(), dim * 8, cudaMemcpyHostToDevice);
+                found.push_back(std::move(stt));
+            }
+        } else {
+            edk_lanczos_opts lo{};
+            lo.nitermax = o->nitermax;
+            lo.neigen = std::max(1, o->neigen);
+            lo.tolerance = o->dtype == EDK_F32 ? std::max(o->tolerance, o->tolerance_lowprec) : o->tolerance;
+            lo.demax = demax;
+            lo.cutoff_min_lanczos_vec = 1e-25;
+            lo.dtype = o->dtype;
+            lo.check_every = o->check_every > 0 ? o->check_every : 8;
+            lo.ran_tab = o->ran_tab;
+            lo.residual_tol = o->dtype == EDK_F64 ? o->residual_tol : 0.0;
+            edk_lanczos_result lr{};
+            lr.diag = diag.data();
+            lr.subdiag = sub.data();
+            lr.vecp = vecp.data();
+            if ((rc = edk_lanczos_e0(h, &lo, &lr))) return rc;
+            lanczos_steps += lr.niter;
+            for (int k = 0; k < lr.nkept; ++k) {
+                auto stt = std::make_unique<State>();
+                stt->nup = nu; stt->ndn = nd; stt->E = lr.E[k]; stt->dtype = o->dtype;
+                stt->psi = DBuf((size_t)dim * ebytes);
+                if (!stt->psi.p) return edk_internal_fail(ctx, EDK_ERR_NOMEM, "state vector");
+                if ((rc = edk_lanczos_gs(h, &lo, lr.niter, lr.vecp + (size_t)k * lr.niter, stt->psi.p))) return rc;
+                lanczos_steps += lr.niter;
+                if (o->dtype == EDK_F32) {
+                    // FP64 refinement restart from the FP32 eigenvector
+                    e0_low = std::min(e0_low, stt->E);
+                    DBuf p64((size_t)dim * 8);
+                    if ((rc = edk_convert(ctx, EDK_F32, EDK_F64, dim, stt->psi.p, p64.p))) return rc;
+                    edk_lanczos_opts ro = lo;
+                    ro.dtype = EDK_F64;
+                    ro.tolerance = o->tolerance;
+                    ro.neigen = 1;
+                    ro.start_dev = p64.p;
+                    ro.ran_tab = nullptr;
+                    ro.use_target = 1;
+                    ro.target = stt->E;
+                    ro.check_every = 4;
+                    ro.residual_tol = o->residual_tol > 0.0 ? o->residual_tol : 1e-9 * std::max(1.0, std::fabs(stt->E));
+                    edk_lanczos_result rr{};
+                    rr.diag = diag.data();
+                    rr.subdiag = sub.data();
+                    rr.vecp = vecp.data();
+                    if ((rc = edk_lanczos_e0(h, &ro, &rr))) return rc;
+                    lanczos_steps += rr.niter;
+                    DBuf q64((size_t)dim * 8);
+                    if ((rc = edk_lanczos_gs(h, &ro, rr.niter, rr.vecp, q64.p))) return rc;
+                    lanczos_steps += rr.niter;
+                    stt->E = rr.E[0];
+                    // the Green chains run on FP32 vectors: keep the refined state as FP32
+                    if ((rc = edk_convert(ctx, EDK_F64, EDK_F32, dim, q64.p, stt->psi.p))) return rc;
+                    stt->dtype = EDK_F32;
+                }
+                found.push_back(std::move(stt));
+            }
+        }
+        if (!found.empty()) {
+            double es = 1e300;
+            for (auto &f : found) es = std::min(es, f->E);
+            for (auto &f : found)
+                if (f->E <= es + demax) states.push_back(std::move(f));
+        }
+    }
+    if (states.empty()) return edk_internal_fail(ctx, EDK_ERR_INVALID, "no eigenstate found");
+    double e0 = 1e300;
+    for (auto &s : states) e0 = std::min(e0, s->E);
+    std::vector<std::unique_ptr<State>> gs;
+    for (auto &s : states)
+        if (s->E <= e0 + demax) gs.push_back(std::move(s));
+    double z = 0.0;
+    for (auto &s : gs) z += std::exp(-o->beta * (s->E - e0));
+    for (auto &s : gs) s->boltz = std::exp(-o->beta * (s->E - e0)) / z;
+    r->e0 = e0;
+    r->z = z;
+    r->e0_lowprec = o->dtype == EDK_F32 ? e0_low : e0;
+    r->nstates = (int)gs.size();
+    for (size_t k = 0; k < gs.size() && k < 64; ++k) {
+        if (r->energies) r->energies[k] = gs[k]->E;
+        if (r->state_sectors) { r->state_sectors[2 * k] = gs[k]->nup; r->state_sectors[2 * k + 1] = gs[k]->ndn; }
+    }
+    // FP64 residual |H psi0 - E0 psi0| of the ground state
+    for (auto &s : gs)
+        if (s->E == e0) {
+            edk_h *h = nullptr;
+            if ((rc = getH(s->nup, s->ndn, &h))) return rc;
+            int64_t dim = 0;
+            edk_h_dims(h, &dim, nullptr, nullptr);
+            DBuf p64;
+            const void *p = s->psi.p;
+            if (s->dtype != EDK_F64) {
+                p64 = DBuf((size_t)dim * 8);
+                if ((rc = edk_convert(ctx, s->dtype, EDK_F64, dim, s->psi.p, p64.p))) return rc;
+                p = p64.p;
+            }
+            double res = 0, nrm = 0;
+            if ((rc = edk_residual(h, p, s->E, &res, &nrm))) return rc;
+            r->residual = res / (nrm > 0 ? nrm : 1.0);
+            break;
+        }
+    // ---------------- double occupancy ----------------
+    if (r->docc)
+        for (int c = 0; c < m->nc; ++c) {
+            double acc = 0.0;
+            for (auto &s : gs) {
+                edk_h *h = nullptr;
+                if ((rc = getH(s->nup, s->ndn, &h))) return rc;
+                double d = 0, n2 = 0;
+                if ((rc = edk_double_occ(h, s->dtype, s->psi.p, c, &d, &n2))) return rc;
+                acc += s->boltz * d / n2;
+            }
+            r->docc[c] = acc;
+        }
+    // ---------------- Green functions ----------------
+    int64_t green_steps = 0;
+    const int nw = o->nw;
+    if (nw > 0 && o->npairs > 0 && r->G) {
+        std::vector<double> wn(nw);
+        for (int n = 0; n < nw; ++n) wn[n] = (2.0 * M_PI / o->beta) * (n + 1) - M_PI / o->beta;
+        std::memset(r->G, 0, sizeof(double) * 2 * (size_t)o->npairs * nw * 2);
+        // combinations needed: (i,i) for every orbital in a pair, (min,max) for off-diagonal pairs
+        std::vector<std::pair<int, int>> combos;
+        auto add = [&](int i, int j) {
+            if (std::find(combos.begin(), combos.end(), std::make_pair(i, j)) == combos.end()) combos.push_back({i, j});
+        };
+        for (int p = 0; p < o->npairs; ++p) {
+            const int i = o->pairs[2 * p], j = o->pairs[2 * p + 1];
+            if (i < 0 || j < 0 || i >= m->nc || j >= m->nc) return edk_internal_fail(ctx, EDK_ERR_INVALID, "pair");
+            add(i, i);
+            add(j, j);
+            if (i != j) add(std::min(i, j), std::max(i, j));
+        }
+        std::vector<double> raw((size_t)combos.size() * nw * 2);
+        std::vector<double> Gc((size_t)2 * nw);
+        const int gdt = o->dtype;
+        for (int spin = 0; spin < 2; ++spin) {
+            if (!((o->spin_mask >> spin) & 1)) continue;
+            std::fill(raw.begin(), raw.end(), 0.0);
+            for (auto &s : gs) {
+                edk_h *hs_src = nullptr;
+                if ((rc = getH(s->nup, s->ndn, &hs_src))) return rc;
+                int64_t sdim = 0;
+                edk_h_dims(hs_src, &sdim, nullptr, nullptr);
+                // the state in the chain precision
+                DBuf conv;
+                const void *psi = s->psi.p;
+                if (s->dtype != gdt) {
+                    conv = DBuf((size_t)sdim * (gdt == EDK_F64 ? 8 : 4));
+                    if ((rc = edk_convert(ctx, s->dtype, gdt, sdim, s->psi.p, conv.p))) return rc;
+                    psi = conv.p;
+                }
+                for (int iph = 1; iph <= 2; ++iph) {
+                    const int d = iph == 1 ? 1 : -1;
+                    const int tnu = s->nup + (spin == 0 ? d : 0), tnd = s->ndn + (spin == 1 ? d : 0);
+                    if (tnu < 0 || tnu > ns || tnd < 0 || tnd > ns) continue;
+                    edk_h *ht = nullptr;
+                    if ((rc = getH(tnu, tnd, &ht))) return rc;
+                    int64_t tdim = 0;
+                    edk_h_dims(ht, &tdim, nullptr, nullptr);
+                    if (tdim == 0) continue;
+                    DBuf phi((size_t)tdim * (gdt == EDK_F64 ? 8 : 4));
+                    for (size_t q = 0; q < combos.size(); ++q) {
+                        const int i = combos[q].first, j = combos[q].second;
+                        int64_t od = 0;
+                        if ((rc = edk_apply_c(hs_src, gdt, i, spin, iph == 1, i == j ? -1 : j, 1, psi, phi.p, &od)))
+                            return rc;
+                        int32_t nd = 0;
+                        if ((rc = edk_green_chain(ht, gdt, phi.p, o->nitergreen, s->E, iph, nw, wn.data(),
+                                                  o->cutoff_dynamic, Gc.data(), nullptr, nullptr, &nd)))
+                            return rc;
+                        green_steps += nd;
+                        for (int w = 0; w < 2 * nw; ++w) raw[q * 2 * nw + w] += s->boltz * Gc[w];
+                    }
+                }
+            }
+            auto idx = [&](int i, int j) {
+                return (size_t)(std::find(combos.begin(), combos.end(), std::make_pair(i, j)) - combos.begin());
+            };
+            for (int p = 0; p < o->npairs; ++p) {
+                const int i = o->pairs[2 * p], j = o->pairs[2 * p + 1];
+                double *out = r->G + ((size_t)spin * o->npairs + p) * 2 * nw;
+                if (i == j) {
+                    std::memcpy(out, &raw[idx(i, i) * 2 * nw], sizeof(double) * 2 * nw);
+                } else {
+                    const size_t a = idx(std::min(i, j), std::max(i, j)), b = idx(i, i), cc = idx(j, j);
+                    for (int w = 0; w < 2 * nw; ++w)
+                        out[w] = 0.5 * (raw[a * 2 * nw + w] - raw[b * 2 * nw + w] - raw[cc * 2 * nw + w]);
+                }
+            }
+        }
+    }
+    edk_internal_count(ctx, 0, (int64_t)sizeof(double) * 2 * o->npairs * nw * 2);
+    r->lanczos_steps = (int32_t)lanczos_steps;
+    r->green_steps = (int32_t)green_steps;
+    return cudaStreamSynchronize(st) == cudaSuccess ? EDK_OK : edk_internal_fail(ctx, EDK_ERR_CUDA, "sync");
+}
+
+}  // extern "C"

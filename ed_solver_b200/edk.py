@@ -47,13 +47,29 @@ class _Model(C.Structure):
 class _LanczosOpts(C.Structure):
     _fields_ = [("nitermax", C.c_int32), ("neigen", C.c_int32), ("tolerance", C.c_double),
                 ("demax", C.c_double), ("cutoff_min_lanczos_vec", C.c_double), ("dtype", C.c_int32),
-                ("check_every", C.c_int32), ("ran_tab", C.c_void_p), ("start_dev", C.c_void_p)]
+                ("check_every", C.c_int32), ("ran_tab", C.c_void_p), ("start_dev", C.c_void_p),
+                ("use_target", C.c_int32), ("target", C.c_double), ("residual_tol", C.c_double)]
 
 
 class _LanczosResult(C.Structure):
     _fields_ = [("nkept", C.c_int32), ("niter", C.c_int32), ("status", C.c_int32),
                 ("E", C.c_double * 64), ("converged", C.c_int32 * 64),
                 ("diag", C.c_void_p), ("subdiag", C.c_void_p), ("vecp", C.c_void_p)]
+
+
+class _SolveOpts(C.Structure):
+    _fields_ = [("dtype", C.c_int32), ("nsectors", C.c_int32), ("sectors", C.c_void_p), ("neigen", C.c_int32),
+                ("nitermax", C.c_int32), ("tolerance", C.c_double), ("tolerance_lowprec", C.c_double),
+                ("check_every", C.c_int32), ("beta", C.c_double), ("demax0", C.c_double),
+                ("nitergreen", C.c_int32), ("nw", C.c_int32), ("spin_mask", C.c_int32), ("npairs", C.c_int32),
+                ("pairs", C.c_void_p), ("cutoff_dynamic", C.c_double), ("ran_tab", C.c_void_p),
+                ("residual_tol", C.c_double)]
+
+
+class _SolveResult(C.Structure):
+    _fields_ = [("e0", C.c_double), ("z", C.c_double), ("e0_lowprec", C.c_double), ("residual", C.c_double),
+                ("nstates", C.c_int32), ("lanczos_steps", C.c_int32), ("green_steps", C.c_int32),
+                ("G", C.c_void_p), ("docc", C.c_void_p), ("energies", C.c_void_p), ("state_sectors", C.c_void_p)]
 
 
 _LIB = None
@@ -80,6 +96,10 @@ def lib():
         "edk_ctx_last_error": (C.c_char_p, [P]),
         "edk_ctx_launch_count": (I64, [P]),
         "edk_ctx_timing": (C.c_int, [P, C.c_int]),
+        "edk_ctx_set_kernel_path": (C.c_int, [P, C.c_int]),
+        "edk_ctx_timing_elements": (C.c_int, [P, C.c_int, P]),
+        "edk_ctx_transfer_bytes": (C.c_int, [P, P, P]),
+        "edk_ctx_clear_cache": (C.c_int, [P]),
         "edk_ctx_timing_report": (C.c_int, [P, C.c_int, P, P]),
         "edk_h_create": (C.c_int, [P, P, C.c_int, C.c_int, P]),
         "edk_h_destroy": (C.c_int, [P]),
@@ -94,6 +114,8 @@ def lib():
         "edk_cf_eval": (C.c_int, [P, I32, I32, P, P, P, P, P, P, I32, P, P]),
         "edk_double_occ": (C.c_int, [P, C.c_int, P, C.c_int, P, P]),
         "edk_residual": (C.c_int, [P, P, D, P, P]),
+        "edk_convert": (C.c_int, [P, C.c_int, C.c_int, I64, P, P]),
+        "edk_solve": (C.c_int, [P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -201,13 +223,27 @@ class Context:
     def launches(self) -> int:
         return int(lib().edk_ctx_launch_count(self.h))
 
+    def set_kernel_path(self, path: int):
+        """0: fastest applicable row kernel (default); 1: generic row kernel only."""
+        self.check(lib().edk_ctx_set_kernel_path(self.h, int(path)), "edk_ctx_set_kernel_path")
+
     def timing(self, enable: bool):
         self.check(lib().edk_ctx_timing(self.h, int(enable)), "edk_ctx_timing")
 
     def timing_report(self, which: int):
-        n, ms = C.c_int64(), C.c_double()
+        """(launches, total device ms, summed elements) of row-kernel class `which`."""
+        n, ms, el = C.c_int64(), C.c_double(), C.c_double()
         self.check(lib().edk_ctx_timing_report(self.h, which, C.byref(n), C.byref(ms)), "timing_report")
-        return n.value, ms.value
+        self.check(lib().edk_ctx_timing_elements(self.h, which, C.byref(el)), "timing_elements")
+        return n.value, ms.value, el.value
+
+    def transfer_bytes(self):
+        a, b = C.c_int64(), C.c_int64()
+        self.check(lib().edk_ctx_transfer_bytes(self.h, C.byref(a), C.byref(b)), "transfer_bytes")
+        return a.value, b.value
+
+    def clear_cache(self):
+        self.check(lib().edk_ctx_clear_cache(self.h), "clear_cache")
 
     def close(self):
         if getattr(self, "h", None):
@@ -291,17 +327,21 @@ class Hamiltonian:
         return y
 
     # ---- Lanczos -------------------------------------------------------
-    def _opts(self, dtype, nitermax, neigen, tolerance, demax, cutoff, check_every, ran_tab, start):
+    def _opts(self, dtype, nitermax, neigen, tolerance, demax, cutoff, check_every, ran_tab, start,
+              target=None, residual_tol=0.0):
         self._tab = None if ran_tab is None else np.ascontiguousarray(ran_tab, np.float64)
         return _LanczosOpts(int(nitermax), int(neigen), float(tolerance), float(demax), float(cutoff),
                             _dtype_code(dtype), int(check_every),
                             None if self._tab is None else self._tab.ctypes.data,
-                            None if start is None else _ptr(start))
+                            None if start is None else _ptr(start),
+                            0 if target is None else 1, 0.0 if target is None else float(target),
+                            float(residual_tol))
 
     def lanczos_e0(self, dtype="f64", nitermax=1000, neigen=1, tolerance=1e-12, demax=1e300,
-                   cutoff=1e-25, check_every=8, ran_tab=None, start=None):
+                   cutoff=1e-25, check_every=8, ran_tab=None, start=None, target=None, residual_tol=0.0):
         """Pass 1 (Lanczos_fast_diagonalize). Returns a dict."""
-        o = self._opts(dtype, nitermax, neigen, tolerance, demax, cutoff, check_every, ran_tab, start)
+        o = self._opts(dtype, nitermax, neigen, tolerance, demax, cutoff, check_every, ran_tab, start, target,
+                       residual_tol)
         cap = min(self.dim, nitermax) + 2
         diag = np.zeros(cap)
         sub = np.zeros(cap)
@@ -390,3 +430,36 @@ def cf_eval(ctx: Context, chains, wn, ld=None):
                                 e.ctypes.data, ph.ctypes.data, sc.ctypes.data, len(wn), wn.ctypes.data,
                                 G.ctypes.data), "edk_cf_eval")
     return G[..., 0] + 1j * G[..., 1]
+
+
+def solve(ctx: Context, model: AIMModel, sectors, beta: float, nw: int, dtype="f64", neigen=1,
+          nitermax=1000, tolerance=1e-12, tolerance_lowprec=1e-6, demax0=5.0, nitergreen=200,
+          spins=(0, 1), pairs=None, cutoff_dynamic=1e-8, check_every=8, ran_tab=None, residual_tol=0.0):
+    """One impurity solve through the C-ABI (edk_solve): host inputs, host outputs.
+
+    Returns dict(e0, z, residual, nstates, lanczos_steps, green_steps, G (2, npairs, nw) complex,
+    docc (nc,), energies, sectors, e0_lowprec).
+    """
+    if pairs is None:
+        pairs = [(i, i) for i in range(model.nc)]
+    sec = np.ascontiguousarray(np.array(sectors, np.int32).reshape(-1))
+    pr = np.ascontiguousarray(np.array(pairs, np.int32).reshape(-1))
+    tab = None if ran_tab is None else np.ascontiguousarray(ran_tab, np.float64)
+    mask = sum(1 << s for s in spins)
+    o = _SolveOpts(_dtype_code(dtype), len(sec) // 2, sec.ctypes.data, int(neigen), int(nitermax), float(tolerance),
+                   float(tolerance_lowprec), int(check_every), float(beta), float(demax0), int(nitergreen),
+                   int(nw), int(mask), len(pr) // 2, pr.ctypes.data, float(cutoff_dynamic),
+                   None if tab is None else tab.ctypes.data, float(residual_tol))
+    G = np.zeros((2, len(pr) // 2, nw, 2))
+    docc = np.zeros(model.nc)
+    en = np.zeros(64)
+    ss = np.zeros(128, np.int32)
+    r = _SolveResult()
+    r.G, r.docc, r.energies, r.state_sectors = G.ctypes.data, docc.ctypes.data, en.ctypes.data, ss.ctypes.data
+    ms, keep = model_struct(model)
+    ctx.check(lib().edk_solve(ctx.h, C.byref(ms), C.byref(o), C.byref(r)), "edk_solve")
+    n = r.nstates
+    return dict(e0=r.e0, z=r.z, residual=r.residual, nstates=n, lanczos_steps=r.lanczos_steps,
+                green_steps=r.green_steps, G=G[..., 0] + 1j * G[..., 1], docc=docc,
+                energies=en[:min(n, 64)].copy(), sectors=[tuple(ss[2 * k:2 * k + 2]) for k in range(min(n, 64))],
+                e0_lowprec=r.e0_lowprec)

@@ -1,0 +1,174 @@
+! edk_fortran -- ISO_C_BINDING interface to libedk.so for the ed_solver code.
+!
+! The bind(C) interfaces mirror include/edk.h one to one.  The wrappers at
+! the bottom (edk_new_H, edk_Hmult_real, edk_delete_H) show how the module
+! procedures of H_class.f90 (new_H :28, Hmult__/Hmultr :69-136, delete_H :48)
+! forward to the library; see the integration notes for the call-site edits.
+! Vectors handed to edk_hmult must be device pointers (c_devptr from CUDA
+! Fortran, or cudaMalloc'd memory); edk_hmult_host takes host arrays.
+module edk_fortran
+  use iso_c_binding
+  implicit none
+
+  integer(c_int), parameter :: EDK_OK = 0, EDK_F64 = 0, EDK_F32 = 1
+  integer(c_int), parameter :: EDK_KRYLOV_EXHAUSTED = 4
+
+  type, bind(C) :: edk_model
+    integer(c_int32_t) :: nc, nb
+    type(c_ptr) :: ec, eb, vbc, u, jj
+    real(c_double) :: jhund
+    real(c_double) :: cutoff_hamilt_param
+  end type
+
+  type, bind(C) :: edk_lanczos_opts
+    integer(c_int32_t) :: nitermax, neigen
+    real(c_double) :: tolerance, demax, cutoff_min_lanczos_vec
+    integer(c_int32_t) :: dtype, check_every
+    type(c_ptr) :: ran_tab, start_dev
+    integer(c_int32_t) :: use_target
+    real(c_double) :: target, residual_tol
+  end type
+
+  type, bind(C) :: edk_lanczos_result
+    integer(c_int32_t) :: nkept, niter, status
+    real(c_double) :: E(64)
+    integer(c_int32_t) :: converged(64)
+    type(c_ptr) :: diag, subdiag, vecp
+  end type
+
+  interface
+    integer(c_int) function edk_ctx_create(device, stream, ctx) bind(C, name="edk_ctx_create")
+      import :: c_int, c_ptr
+      integer(c_int), value :: device
+      type(c_ptr), value :: stream
+      type(c_ptr) :: ctx
+    end function
+    integer(c_int) function edk_ctx_destroy(ctx) bind(C, name="edk_ctx_destroy")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+    end function
+    integer(c_int) function edk_h_create(ctx, m, nup, ndn, h) bind(C, name="edk_h_create")
+      import :: c_int, c_ptr, edk_model
+      type(c_ptr), value :: ctx
+      type(edk_model), intent(in) :: m
+      integer(c_int), value :: nup, ndn
+      type(c_ptr) :: h
+    end function
+    integer(c_int) function edk_h_destroy(h) bind(C, name="edk_h_destroy")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function edk_h_dims(h, dim, dim_up, dim_dn) bind(C, name="edk_h_dims")
+      import :: c_int, c_ptr, c_int64_t
+      type(c_ptr), value :: h
+      integer(c_int64_t) :: dim, dim_up, dim_dn
+    end function
+    integer(c_int) function edk_hmult(h, dtype, n, x, y) bind(C, name="edk_hmult")
+      import :: c_int, c_ptr, c_int64_t
+      type(c_ptr), value :: h
+      integer(c_int), value :: dtype
+      integer(c_int64_t), value :: n
+      type(c_ptr), value :: x, y
+    end function
+    integer(c_int) function edk_hmult_host(h, dtype, n, x, y) bind(C, name="edk_hmult_host")
+      import :: c_int, c_ptr, c_int64_t, c_double
+      type(c_ptr), value :: h
+      integer(c_int), value :: dtype
+      integer(c_int64_t), value :: n
+      real(c_double), intent(in) :: x(*)
+      real(c_double), intent(out) :: y(*)
+    end function
+    integer(c_int) function edk_lanczos_e0(h, o, r) bind(C, name="edk_lanczos_e0")
+      import :: c_int, c_ptr, edk_lanczos_opts, edk_lanczos_result
+      type(c_ptr), value :: h
+      type(edk_lanczos_opts), intent(in) :: o
+      type(edk_lanczos_result), intent(inout) :: r
+    end function
+    integer(c_int) function edk_lanczos_gs(h, o, niter, coef, psi) bind(C, name="edk_lanczos_gs")
+      import :: c_int, c_ptr, c_int32_t, c_double, edk_lanczos_opts
+      type(c_ptr), value :: h
+      type(edk_lanczos_opts), intent(in) :: o
+      integer(c_int32_t), value :: niter
+      real(c_double), intent(in) :: coef(*)
+      type(c_ptr), value :: psi
+    end function
+    integer(c_int) function edk_apply_c(src, dtype, site, spin, dagger, site2, sign2, vin, vout, out_dim) &
+        bind(C, name="edk_apply_c")
+      import :: c_int, c_ptr, c_int64_t
+      type(c_ptr), value :: src
+      integer(c_int), value :: dtype, site, spin, dagger, site2, sign2
+      type(c_ptr), value :: vin, vout
+      integer(c_int64_t) :: out_dim
+    end function
+    integer(c_int) function edk_green_chain(t, dtype, start, nitergreen, e0, iph, nw, wn, cutoff_dynamic, &
+        G, diag, subdiag, niter_done) bind(C, name="edk_green_chain")
+      import :: c_int, c_ptr, c_int32_t, c_double
+      type(c_ptr), value :: t
+      integer(c_int), value :: dtype, iph
+      type(c_ptr), value :: start
+      integer(c_int32_t), value :: nitergreen, nw
+      real(c_double), value :: e0, cutoff_dynamic
+      real(c_double), intent(in) :: wn(*)
+      real(c_double), intent(out) :: G(*), diag(*), subdiag(*)
+      integer(c_int32_t) :: niter_done
+    end function
+  end interface
+
+  ! one sector Hamiltonian at a time, as H_class.f90 keeps sector_h (H_class.f90:11)
+  type(c_ptr), save :: edk_ctx_handle = c_null_ptr, edk_h_handle = c_null_ptr
+
+contains
+
+  ! new_H(AIM, sector) for an (nup, ndn) sector: Ec/Eb/Vbc per spin, U, JJ from the AIM type
+  subroutine edk_new_H(nc, nb, ec, eb, vbc, u, jj, jhund, cutoff, nup, ndn)
+    integer, intent(in) :: nc, nb, nup, ndn
+    real(c_double), intent(in), target :: ec(nc, nc, 2), eb(nb, nb, 2), vbc(nb, nc, 2), u(nc, nc), jj(nc, nc)
+    real(c_double), intent(in) :: jhund, cutoff
+    ! the C side reads row-major matrices: pass transposes of the Fortran arrays
+    real(c_double), allocatable, target, save :: ec_t(:, :, :), eb_t(:, :, :), vbc_t(:, :, :), u_t(:, :), jj_t(:, :)
+    type(edk_model) :: m
+    integer :: s, ierr
+    if (.not. c_associated(edk_ctx_handle)) then
+      ierr = edk_ctx_create(0_c_int, c_null_ptr, edk_ctx_handle)
+      if (ierr /= EDK_OK) stop 'edk_ctx_create failed'
+    end if
+    if (allocated(ec_t)) deallocate(ec_t, eb_t, vbc_t, u_t, jj_t)
+    allocate(ec_t(nc, nc, 2), eb_t(nb, nb, 2), vbc_t(nc, nb, 2), u_t(nc, nc), jj_t(nc, nc))
+    do s = 1, 2
+      ec_t(:, :, s) = transpose(ec(:, :, s))
+      eb_t(:, :, s) = transpose(eb(:, :, s))
+      vbc_t(:, :, s) = transpose(vbc(:, :, s))
+    end do
+    u_t = transpose(u)
+    jj_t = transpose(jj)
+    m%nc = nc
+    m%nb = nb
+    m%ec = c_loc(ec_t)
+    m%eb = c_loc(eb_t)
+    m%vbc = c_loc(vbc_t)
+    m%u = c_loc(u_t)
+    m%jj = c_loc(jj_t)
+    m%jhund = jhund
+    m%cutoff_hamilt_param = cutoff
+    if (c_associated(edk_h_handle)) ierr = edk_h_destroy(edk_h_handle)
+    ierr = edk_h_create(edk_ctx_handle, m, int(nup, c_int), int(ndn, c_int), edk_h_handle)
+    if (ierr /= EDK_OK) stop 'edk_h_create failed'
+  end subroutine
+
+  ! Hmult__ on host arrays (REAL(DBL) build of H_class.f90:109)
+  subroutine edk_Hmult_real(n, vec_out, vec_in)
+    integer, intent(in) :: n
+    real(c_double), intent(out) :: vec_out(n)
+    real(c_double), intent(in) :: vec_in(n)
+    integer(c_int) :: ierr
+    ierr = edk_hmult_host(edk_h_handle, EDK_F64, int(n, c_int64_t), vec_in, vec_out)
+    if (ierr /= EDK_OK) stop 'edk_hmult_host failed'
+  end subroutine
+
+  subroutine edk_delete_H()
+    integer(c_int) :: ierr
+    if (c_associated(edk_h_handle)) ierr = edk_h_destroy(edk_h_handle)
+    edk_h_handle = c_null_ptr
+  end subroutine
+
+end module edk_fortran

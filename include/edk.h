@@ -75,7 +75,20 @@ int64_t edk_ctx_launch_count(const edk_ctx *ctx);
  * 1 = first Lanczos step, 2 = fused Lanczos step, 3 = residual; add 4 for
  * FP32), the number of launches and their summed device time in ms. */
 int edk_ctx_timing(edk_ctx *ctx, int enable);
+/* Row-kernel selection: 0 = the fastest kernel whose preconditions hold
+ * (default), 1 = always the generic kernel (for A/B checks), 2/3 = the fast
+ * kernel with launch shape 0 (two columns per thread, one block per SM) or 1
+ * (one column per thread, two blocks per SM) when its preconditions hold. */
+int edk_ctx_set_kernel_path(edk_ctx *ctx, int path);
 int edk_ctx_timing_report(edk_ctx *ctx, int which, int64_t *launches, double *total_ms);
+/* Sum over the timed launches of class `which` of the sector dimension each
+ * processed (for algorithmic-byte accounting). */
+int edk_ctx_timing_elements(edk_ctx *ctx, int which, double *elements);
+/* Bytes the library copied host->device and device->host on this context. */
+int edk_ctx_transfer_bytes(const edk_ctx *ctx, int64_t *h2d, int64_t *d2h);
+/* Destroys the sector Hamiltonians edk_solve keeps on the context between
+ * calls (they are reused when the same model and sector come back). */
+int edk_ctx_clear_cache(edk_ctx *ctx);
 
 /* ---- basis (quantum_fermion_hilbert_class.f90:346-421) ----------------- */
 int64_t edk_binom(int n, int k);
@@ -124,6 +137,12 @@ typedef struct edk_lanczos_opts {
     int32_t check_every;         /* host convergence check cadence (steps), >=1 */
     const double *ran_tab;       /* host, 10001 entries; NULL = the library's table */
     const void *start_dev;       /* optional start vector (dtype, dim); overrides ran_tab */
+    int32_t use_target;          /* 1: follow the Ritz value nearest `target` instead of the
+                                    lowest ones (refinement restart of an excited state) */
+    double target;
+    double residual_tol;         /* > 0: also require the Ritz residual beta_{k+1}|y_k| below
+                                    this (an eigenvector criterion; the reference stops on the
+                                    eigenvalue change alone) */
 } edk_lanczos_opts;
 
 typedef struct edk_lanczos_result {
@@ -179,6 +198,56 @@ int edk_cf_eval(edk_ctx *ctx, int32_t nchain, int32_t ld, const int32_t *n_host,
 int edk_double_occ(edk_h *h, int dtype, const void *psi_dev, int site, double *docc, double *norm2);
 /* |H psi - e psi| and |psi| with the FP64 matvec (psi in FP64). */
 int edk_residual(edk_h *h, const void *psi_dev, double e, double *res_norm, double *psi_norm);
+
+/* Element-type conversion of a device vector (FP32 <-> FP64, or a copy). */
+int edk_convert(edk_ctx *ctx, int from_dtype, int to_dtype, int64_t n, const void *in_dev, void *out_dev);
+
+/* ---- solver driver -------------------------------------------------------
+ * One solve of the impurity problem for the (N_up, N_dn) basis: the sector
+ * scan and ground states of get_eigen_energies/get_GS (solver.h:11-237), the
+ * Boltzmann window (eigen_class.f90:322-450), double occupancies
+ * (correlations_write.h:93-95) and the (c, c+) Green functions of
+ * compute_greenAA (green_class_computeAA.f90:40-185) for the requested
+ * impurity orbital pairs and spins.  All inputs and outputs are host buffers;
+ * vectors live on the device only.  dtype EDK_F32 = mixed precision: FP32
+ * Krylov vectors and H*v with FP64 alpha/beta, FP32 passes refined by one FP64
+ * Lanczos restart per state, FP64 residual check, FP64 continued fractions. */
+typedef struct edk_solve_opts {
+    int32_t dtype;
+    int32_t nsectors;
+    const int32_t *sectors;      /* 2*nsectors: (nup, ndn) scanned for eigenstates */
+    int32_t neigen;              /* Neigen per sector */
+    int32_t nitermax;            /* Nitermax */
+    double tolerance;            /* eigenvalue tolerance (FP64 passes) */
+    double tolerance_lowprec;    /* eigenvalue tolerance of the FP32 pass (mixed) */
+    int32_t check_every;         /* Lanczos convergence check cadence */
+    double beta;
+    double demax0;               /* window dEmax = demax0/beta (dmft_ed_solver.f90:1468) */
+    int32_t nitergreen;          /* Nitergreenmax */
+    int32_t nw;                  /* fermionic Matsubara points i(2n-1)pi/beta */
+    int32_t spin_mask;           /* bit 0: G of spin up, bit 1: spin down */
+    int32_t npairs;
+    const int32_t *pairs;        /* 2*npairs impurity orbital pairs (i,j) */
+    double cutoff_dynamic;       /* skip |A psi|^2 below this (reference 1e-8) */
+    const double *ran_tab;       /* start-vector table, NULL = library table */
+    double residual_tol;         /* > 0: eigenvector criterion of the FP64 passes (see
+                                    edk_lanczos_opts); mixed precision always refines to it */
+} edk_solve_opts;
+
+typedef struct edk_solve_result {
+    double e0, z;
+    double e0_lowprec;           /* mixed: lowest FP32 eigenvalue before refinement */
+    double residual;             /* |H psi0 - E0 psi0| / |psi0| with the FP64 matvec */
+    int32_t nstates;             /* eigenstates in the Boltzmann window */
+    int32_t lanczos_steps;       /* H*v applications of the eigen part */
+    int32_t green_steps;         /* H*v applications of the Green part */
+    double *G;                   /* host [2][npairs][nw][2] (spin, pair, w, re/im) or NULL */
+    double *docc;                /* host [nc] or NULL */
+    double *energies;            /* host [64] or NULL */
+    int32_t *state_sectors;      /* host [128] or NULL */
+} edk_solve_result;
+
+int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_solve_result *r);
 
 #ifdef __cplusplus
 }

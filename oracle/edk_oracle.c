@@ -860,3 +860,22 @@ int orc_num_threads(void)
     return 1;
 #endif
 }
+
+/* CPU-baseline sample: runs `nsteps` iterations of lanc_opt (Lanczos_plain.h:66-173)
+ * from v0 on sector h; returns the number of iterations completed. */
+int orc_lanczos_steps(const orc_h *h, const double *v0, int nsteps, double *diag, double *subdiag)
+{
+    const int64_t n = h->dim;
+    double *vin = (double *)malloc(sizeof(double) * n);
+    double *tmp = (double *)calloc((size_t)n, sizeof(double));
+    double *vout = (double *)malloc(sizeof(double) * n);
+    memcpy(vin, v0, sizeof(double) * n);
+    orc_lanc_state st = {0, 0};
+    int done = 0;
+    for (int it = 1; it <= nsteps; ++it) {
+        if (lanczos_step(h, it, nsteps + 1, vin, tmp, vout, diag, subdiag, &st, 1e-25)) break;
+        done = it;
+    }
+    free(vin); free(tmp); free(vout);
+    return done;
+}

@@ -86,6 +86,8 @@ def lib():
         L.orc_double_occ.restype = d
         L.orc_double_occ.argtypes = [P, P, i32]
         L.orc_num_threads.restype = i32
+        L.orc_lanczos_steps.restype = i32
+        L.orc_lanczos_steps.argtypes = [P, P, i32, P, P]
         _LIB = L
     return _LIB
 
@@ -222,6 +224,21 @@ def lanczos_e0(h: OracleH, v0=None, nitermax=1000, neigen=1, tolerance=1e-12, de
     it = int(niter[0])
     return dict(E=E[:k].copy(), niter=it, diag=diag[:it].copy(), subdiag=sub[:it].copy(),
                 vecp=vecp[:k * it].reshape(k, it).copy(), conv=conv[:k].copy())
+
+
+def lanczos_steps(h: OracleH, nsteps: int, v0=None):
+    """Runs nsteps plain Lanczos iterations (CPU-baseline sample); returns (alpha, beta)."""
+    if v0 is None:
+        v0 = start_vector(h.dim)
+    v0 = np.ascontiguousarray(v0, np.float64)
+    d = np.zeros(nsteps + 2)
+    s = np.zeros(nsteps + 2)
+    n = lib().orc_lanczos_steps(h.h, _p(v0), nsteps, _p(d), _p(s))
+    return d[:n], s[:n + 1]
+
+
+def num_threads() -> int:
+    return int(lib().orc_num_threads())
 
 
 def lanczos_gs(h: OracleH, coef: np.ndarray, v0=None, cutoff_min=1e-25) -> np.ndarray:

@@ -24,8 +24,15 @@ def _models():
 SECTORS = [(3, 3), (2, 4), (4, 1), (0, 3), (5, 5), (1, 0)]
 
 
+@pytest.fixture(params=[0, 1], ids=["auto-kernel", "generic-kernel"])
+def kpath(request, ctx):
+    ctx.set_kernel_path(request.param)
+    yield request.param
+    ctx.set_kernel_path(0)
+
+
 @pytest.mark.parametrize("mi", [0, 1, 2])
-def test_hmult_fp64_bit_exact(ctx, mi):
+def test_hmult_fp64_bit_exact(ctx, kpath, mi):
     import torch
     m = _models()[mi]
     rng = np.random.default_rng(mi)
@@ -41,7 +48,7 @@ def test_hmult_fp64_bit_exact(ctx, mi):
 
 
 @pytest.mark.parametrize("mi", [0, 1])
-def test_hmult_fp32(ctx, mi):
+def test_hmult_fp32(ctx, kpath, mi):
     import torch
     m = _models()[mi]
     rng = np.random.default_rng(7)
@@ -53,7 +60,7 @@ def test_hmult_fp32(ctx, mi):
         assert np.abs(y - y_ref).max() <= 2e-6 * np.abs(y_ref).max()
 
 
-def test_hmult_large_rows_c3_sector_bit_exact(ctx):
+def test_hmult_large_rows_c3_sector_bit_exact(ctx, kpath):
     """The ns=14 sector (3432 x 3432 rows): staged rows, packed up table, row schedule."""
     import torch
     m = workload("c3").model
@@ -88,3 +95,27 @@ def test_tables_on_device_match_host_builder(ctx):
         p, t, v, d = h.table(spin)
         p2, t2, v2, d2 = edk.build_table(m, spin, 5 if spin == 0 else 4)
         assert np.array_equal(t, t2) and np.array_equal(v, v2) and np.array_equal(d, d2)
+
+
+def test_hmult_misaligned_pointers_take_the_generic_path(ctx):
+    """Vectors offset by one element (not 16-byte aligned) must still be exact."""
+    import torch
+    m = workload("c1").model
+    h = edk.Hamiltonian(ctx, m, 4, 4)
+    x = np.random.default_rng(5).normal(size=h.dim)
+    xb = torch.zeros(h.dim + 1, dtype=torch.float64, device="cuda")
+    xb[1:] = torch.tensor(x, device="cuda")
+    yb = torch.zeros(h.dim + 1, dtype=torch.float64, device="cuda")
+    h.hmult(xb[1:], out=yb[1:])
+    assert np.array_equal(yb[1:].cpu().numpy(), O.OracleH(m, 4, 4).hmult(x))
+
+
+def test_hmult_full_size_ns16_bit_exact(ctx):
+    """The ns=16 half-filled sector (1.66e8 states), FP64, against the oracle."""
+    import torch
+    m = workload("c5").model
+    h = edk.Hamiltonian(ctx, m, 8, 8)
+    x = torch.rand(h.dim, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(1))
+    y = h.hmult(x).cpu().numpy()
+    ho = O.OracleH(m, 8, 8)
+    assert np.array_equal(y, ho.hmult(x.cpu().numpy()))

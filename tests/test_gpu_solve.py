@@ -1,0 +1,65 @@
+"""edk_solve (the driver behind the bench) against the oracle drivers, the
+reference golden output, and mixed precision against FP64."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from ed_solver_b200 import edk
+from ed_solver_b200.model import star_model, workload
+
+pytestmark = pytest.mark.gpu
+
+
+def test_solve_fp64_matches_oracle_driver(ctx):
+    w = workload("c1")
+    m = w.model
+    r = edk.solve(ctx, m, w.sectors, w.beta, 256, dtype="f64", nitergreen=w.nitergreen, spins=(0, 1))
+    gso, e0o, zo = O.ground_states(m, w.sectors, w.beta, w.demax0)
+    assert abs(r["e0"] - e0o) < 1e-11 * abs(e0o)
+    Go_up = O.green_impurity(m, gso, w.beta, 256, w.nitergreen, spin=0)[(0, 0)]
+    Go_dn = O.green_impurity(m, gso, w.beta, 256, w.nitergreen, spin=1)[(0, 0)]
+    assert np.abs(r["G"][0, 0] - Go_up).max() < 1e-8
+    assert np.abs(r["G"][1, 0] - Go_dn).max() < 1e-8
+    assert r["residual"] < 1e-6
+    assert abs(r["docc"][0] - O.OracleH(m, 4, 4).double_occ(gso[0]["psi"])) < 1e-9
+
+
+def test_solve_reference_golden_g_bm(ctx):
+    g = np.loadtxt(os.path.join(os.path.dirname(__file__), "golden", "g_bm_2b.txt"))
+    m = star_model(-5.0, 10.0, [0.0, 0.0], [math.sqrt(0.2), math.sqrt(0.3)], orbital_of_bath=[0, 1], nc=2,
+                   Uprime=2.0, J=0.0, cutoff=1e-8)
+    secs = [(a, b) for a in range(5) for b in range(5)]
+    r = edk.solve(ctx, m, secs, 50.0, len(g), dtype="f64", neigen=40, tolerance=1e-13, demax0=50.0,
+                  nitergreen=400, spins=(0,), pairs=[(0, 0), (1, 1), (0, 1)])
+    assert np.abs(r["G"][0, 0] - (g[:, 1] + 1j * g[:, 2])).max() < 2e-8
+    assert np.abs(r["G"][0, 1] - (g[:, 3] + 1j * g[:, 4])).max() < 2e-8
+    assert np.abs(r["G"][0, 2]).max() < 1e-12
+
+
+@pytest.mark.parametrize("name", ["c1", "c3"])
+def test_mixed_precision_against_fp64(ctx, name):
+    w = workload(name)
+    # both paths converge the eigenvector (Ritz residual) so the comparison
+    # measures the FP32 arithmetic, not an under-converged FP64 ground state
+    kw = dict(nitergreen=w.nitergreen, spins=(0,), tolerance=1e-12, residual_tol=1e-10)
+    r64 = edk.solve(ctx, w.model, w.sectors, w.beta, 512, dtype="f64", **kw)
+    r32 = edk.solve(ctx, w.model, w.sectors, w.beta, 512, dtype="f32", **kw)
+    assert abs(r32["e0"] - r64["e0"]) <= 1e-8 * abs(r64["e0"])
+    assert np.abs(r32["G"] - r64["G"]).max() <= 1e-6
+    assert r32["residual"] < 1e-6
+
+
+def test_solve_two_orbital_kanamori_all_sectors(ctx):
+    """All 121 sectors of the two-orbital Kanamori model (Hund terms active)."""
+    w = workload("c2")
+    r = edk.solve(ctx, w.model, w.sectors, w.beta, 64, dtype="f64", nitergreen=100, spins=(0,),
+                  pairs=[(0, 0), (1, 1), (0, 1)], tolerance=1e-10)
+    secs = sorted(set(r["sectors"]))
+    gso, e0o, zo = O.ground_states(w.model, secs, w.beta, w.demax0, tolerance=1e-10)
+    assert abs(r["e0"] - e0o) < 1e-9 * abs(e0o)
+    Go = O.green_impurity(w.model, gso, w.beta, 64, 100, spin=0, pairs=[(0, 0), (1, 1), (0, 1)])
+    assert np.abs(r["G"][0, 0] - Go[(0, 0)]).max() < 1e-7
+    assert np.abs(r["G"][0, 2] - Go[(0, 1)]).max() < 1e-7
