@@ -184,18 +184,30 @@ __device__ __forceinline__ uint2 ldu2(const uint32_t *p)
     return __ldg(reinterpret_cast<const uint2 *>(p));
 }
 
-// Lanczos coefficients from the three grid sums, written by thread 0 of the
-// last block: alpha_{slot+1} = <w,v>, beta_{slot+2}^2 = |w|^2 - 2 alpha <w,v> + alpha^2 |v|^2.
+// Lanczos coefficients from the grid sums, written by thread 0 of the last
+// block.  The stored vector is s' = w - gamma v' (gamma known before the
+// launch: gamma1 for the first step, alpha_k for step k), so
+//   alpha = <s',v'> + gamma |v'|^2,  delta = alpha - gamma,
+//   beta^2 = |s'|^2 - 2 delta <s',v'> + delta^2 |v'|^2,
+// a difference of numbers of size beta^2 + delta^2 instead of |w|^2.
+__device__ __forceinline__ double step_gamma(const RowArgs &a)
+{
+    return a.mode == kModeFirst ? a.gamma1 : a.tri_diag[a.k - 1];
+}
 __device__ __forceinline__ void lanczos_finalize(const RowArgs &a)
 {
-    const double sww = a.sums_out[0], swv = a.sums_out[1], svv = a.sums_out[2];
-    const double al = swv;
-    const double b2 = sww - 2.0 * al * swv + al * al * svv;
+    const double sss = a.sums_out[0], ssv = a.sums_out[1], svv = a.sums_out[2];
+    const double g = step_gamma(a);
+    const double al = ssv + g * svv;
+    const double de = al - g;
+    const double b2 = sss - 2.0 * de * ssv + de * de * svv;
     const int slot = (a.mode == kModeFirst) ? 0 : a.k;
     double b = b2 > 0.0 ? sqrt(b2) : 0.0;
     const bool finite = isfinite(al) && isfinite(b2);
     if (!finite) { a.flags[1] = 1; b = 0.0; }
-    if (b2 <= 1e-28 * sww) b = 0.0;          // relative breakdown: subtraction at rounding level
+    // relative breakdown: beta at rounding level of |w| = |s' + gamma v'|
+    const double ww = sss + 2.0 * g * ssv + g * g * svv;
+    if (b2 <= 1e-28 * ww) b = 0.0;
     a.tri_diag[slot] = finite ? al : 0.0;
     a.tri_sub[slot + 1] = b;
     if (!(b >= a.cutoff) && a.flags[0] == 0) a.flags[0] = slot + 1;

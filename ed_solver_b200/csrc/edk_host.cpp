@@ -105,6 +105,11 @@ struct edk_ctx {
     int64_t h2d_bytes = 0, d2h_bytes = 0;
     // sector Hamiltonians kept by edk_solve between calls (key: model hash, nup, ndn)
     std::vector<std::pair<std::string, edk_h *>> hcache;
+    // batched chains: device copies of the item list, Hamiltonians, coefficients,
+    // per-block workspace, and the autotuned launch shape per problem class
+    DevBuf b_hams, b_items, b_queue, b_alpha, b_beta, b_done, b_work;
+    struct BatchShape { int block, R, per_sm; };
+    std::vector<std::pair<std::string, BatchShape>> batch_tuned;
     cudaEvent_t get_event() {
         if (!event_pool.empty()) { cudaEvent_t e = event_pool.back(); event_pool.pop_back(); return e; }
         cudaEvent_t e = nullptr;
@@ -351,6 +356,7 @@ struct Krylov {
     const double *psi_coef = nullptr;
     void *psi = nullptr;
     double cutoff = 1e-25;
+    double gamma1 = 0.0;    // shift of the first stored vector (energy scale of the chain)
 };
 
 // v1 = start/|start| into w[1]; tri_sub[0] = |start|; psi = coef[0]*v1 when psi set
@@ -387,6 +393,7 @@ int krylov_step(Krylov &K)
     edk_h *h = K.h;
     RowArgs a = base_args(h);
     a.cutoff = K.cutoff;
+    a.gamma1 = K.gamma1;
     if (K.k == 0) {
         a.mode = kModeFirst;
         a.x = K.w[K.ivk];
@@ -982,6 +989,7 @@ int edk_green_chain(edk_h *t, int dtype, const void *start_dev, int32_t nitergre
     if (rc) return rc;
     Krylov K{t, dtype};
     if ((rc = work_ptrs(t, dtype, K.w))) return rc;
+    K.gamma1 = e0;          // the chain's alphas are energies near the state's
     double nrm = 0.0;
     // the start vector is copied into the workspace and normalised there
     rc = krylov_start(K, start_dev, nullptr, &nrm);
@@ -1087,3 +1095,187 @@ int edk_residual(edk_h *h, const void *psi_dev, double e, double *res_norm, doub
 }
 
 }  // extern "C"
+
+
+// ---------------------------------------------------------------------------
+// batched Green chains (edk_batch.cu)
+// ---------------------------------------------------------------------------
+extern "C" int edk_green_batch(edk_ctx *c, int dtype, int32_t nchain, const edk_chain *ch, int32_t nitergreen,
+                               int32_t nw, const double *wn_host, double cutoff_dynamic, int32_t nout,
+                               double *G_out, int32_t mode, edk_batch_stats *stats)
+{
+    if (!c || nchain < 0 || (nchain > 0 && !ch) || nitergreen < 1 || nw < 1 || !wn_host || nout < 1 || !G_out)
+        return EDK_ERR_INVALID;
+    if (dtype != EDK_F64 && dtype != EDK_F32) return c->fail(EDK_ERR_INVALID, "dtype");
+    std::memset(G_out, 0, sizeof(double) * 2 * (size_t)nout * nw);
+    if (stats) std::memset(stats, 0, sizeof *stats);
+    if (nchain == 0) return EDK_OK;
+    for (int i = 0; i < nchain; ++i)
+        if (!ch[i].target || !ch[i].start_dev || ch[i].out < 0 || ch[i].out >= nout || (ch[i].iph != 1 && ch[i].iph != 2))
+            return c->fail(EDK_ERR_INVALID, "chain %d: bad target/start/out/iph", i);
+    cudaStream_t st = c->stream;
+    int rc;
+    if (mode == 1) {
+        // per-chain launches: one grid per Lanczos step (edk_green_chain)
+        std::vector<double> G(2 * (size_t)nw);
+        int64_t steps = 0;
+        for (int i = 0; i < nchain; ++i) {
+            int32_t nd = 0;
+            if ((rc = edk_green_chain(ch[i].target, dtype, ch[i].start_dev, nitergreen, ch[i].e0, ch[i].iph, nw,
+                                      wn_host, cutoff_dynamic, G.data(), nullptr, nullptr, &nd)))
+                return rc;
+            steps += nd;
+            double *o = G_out + (size_t)ch[i].out * 2 * nw;
+            for (int w = 0; w < 2 * nw; ++w) o[w] += ch[i].weight * G[w];
+        }
+        if (stats) { stats->steps = steps; stats->chains = nchain; }
+        return EDK_OK;
+    }
+    // ---- persistent work queue ----
+    std::vector<const edk_h *> hs;
+    std::vector<HamDev> hd;
+    std::vector<BatchItem> items(nchain);
+    std::vector<int> order(nchain);
+    int64_t maxdim = 0, maxdup = 0;
+    for (int i = 0; i < nchain; ++i) {
+        const edk_h *h = ch[i].target;
+        int idx = -1;
+        for (size_t q = 0; q < hs.size(); ++q)
+            if (hs[q] == h) idx = (int)q;
+        if (idx < 0) { idx = (int)hs.size(); hs.push_back(h); hd.push_back(h->H); }
+        maxdim = std::max(maxdim, h->dim);
+        maxdup = std::max(maxdup, h->dup);
+        order[i] = i;
+    }
+    if (maxdup * (dtype == EDK_F64 ? 8 : 4) > 96 * 1024)
+        return c->fail(EDK_ERR_UNSUPPORTED, "batched chains need rows of at most 96 KB (use mode 1)");
+    // largest chains first (longest-processing-time order)
+    std::sort(order.begin(), order.end(), [&](int a, int b) {
+        const int64_t wa = ch[a].target->dim * std::min<int64_t>(nitergreen, ch[a].target->dim);
+        const int64_t wb = ch[b].target->dim * std::min<int64_t>(nitergreen, ch[b].target->dim);
+        return wa > wb;
+    });
+    const size_t ld = (size_t)nitergreen + 1;
+    if ((rc = c->cuda(c->b_alpha.ensure(sizeof(double) * ld * nchain), "alloc"))) return rc;
+    if ((rc = c->cuda(c->b_beta.ensure(sizeof(double) * ld * nchain), "alloc"))) return rc;
+    if ((rc = c->cuda(c->b_done.ensure(sizeof(int32_t) * nchain), "alloc"))) return rc;
+    for (int q = 0; q < nchain; ++q) {
+        const int i = order[q];
+        const edk_h *h = ch[i].target;
+        int idx = 0;
+        for (size_t z = 0; z < hs.size(); ++z)
+            if (hs[z] == h) idx = (int)z;
+        BatchItem &b = items[q];
+        b.ham = idx;
+        b.niter = (int32_t)std::min<int64_t>(nitergreen, h->dim);
+        b.dim = h->dim;
+        b.start = ch[i].start_dev;
+        b.gamma1 = ch[i].e0;
+        b.cutoff_dynamic = cutoff_dynamic;
+        b.alpha = c->b_alpha.as<double>() + (size_t)q * ld;
+        b.beta = c->b_beta.as<double>() + (size_t)q * ld;
+        b.done = c->b_done.as<int32_t>() + q;
+    }
+    if ((rc = c->cuda(upload(c->b_hams, hd, st), "upload hams"))) return rc;
+    if ((rc = c->cuda(upload(c->b_items, items, st), "upload items"))) return rc;
+    if ((rc = c->cuda(c->b_queue.ensure(sizeof(int)), "alloc"))) return rc;
+    c->h2d_bytes += (int64_t)(hd.size() * sizeof(HamDev) + items.size() * sizeof(BatchItem));
+    const size_t es = dtype == EDK_F64 ? 8 : 4;
+
+    // ---- autotune the launch shape for this problem class ----
+    char key[96];
+    snprintf(key, sizeof key, "%d:%lld:%lld", dtype, (long long)maxdup, (long long)maxdim);
+    edk_ctx::BatchShape shape{0, 0, 0};
+    for (auto &kv : c->batch_tuned)
+        if (kv.first == key) shape = kv.second;
+    auto run = [&](const edk_ctx::BatchShape &s, int nitems, double *ms) -> int {
+        const int grid = c->num_sms * s.per_sm;
+        int r2 = c->cuda(c->b_work.ensure(es * 4 * (size_t)maxdim * grid), "alloc batch workspace");
+        if (r2) return r2;
+        r2 = c->cuda(cudaMemsetAsync(c->b_queue.p, 0, sizeof(int), st), "memset");
+        if (r2) return r2;
+        cudaEvent_t a = c->get_event(), b = c->get_event();
+        cudaEventRecord(a, st);
+        r2 = c->cuda(launch_batch(dtype, s.R, c->b_hams.as<HamDev>(), c->b_items.as<BatchItem>(), nitems,
+                                  c->b_queue.as<int>(), c->b_work.p, maxdim, maxdup, 1e-25, grid, s.block, st),
+                     "batch kernel");
+        c->launches++;
+        cudaEventRecord(b, st);
+        cudaEventSynchronize(b);
+        float t = 0.f;
+        cudaEventElapsedTime(&t, a, b);
+        c->event_pool.push_back(a);
+        c->event_pool.push_back(b);
+        if (ms) *ms = t;
+        return r2;
+    };
+    int tuned = 0;
+    if (shape.block == 0) {
+        // candidates: block size x rows per group x blocks per SM, timed on the
+        // largest items with the chain length cut to 6 steps
+        const int nsample = std::min<int>(nchain, c->num_sms * 2);
+        std::vector<BatchItem> sample(items.begin(), items.begin() + nsample);
+        for (auto &b : sample) b.niter = std::min<int32_t>(b.niter, 6);
+        if ((rc = c->cuda(upload(c->b_items, sample, st), "upload sample"))) return rc;
+        double best = 1e300;
+        for (int block : {128, 256, 512})
+            for (int R : {1, 2, 4}) {
+                if ((int64_t)R * maxdup * (int64_t)es > 96 * 1024) continue;
+                const int occ = batch_max_blocks_per_sm(dtype, R, block, maxdup);
+                for (int per_sm : {1, 2, 4}) {
+                    if (per_sm > occ) continue;
+                    edk_ctx::BatchShape s{block, R, per_sm};
+                    double ms = 0;
+                    if ((rc = run(s, nsample, &ms))) return rc;
+                    ++tuned;
+                    if (ms < best) { best = ms; shape = s; }
+                }
+            }
+        if (shape.block == 0) return c->fail(EDK_ERR_UNSUPPORTED, "no batch launch shape fits");
+        c->batch_tuned.push_back({key, shape});
+        if ((rc = c->cuda(upload(c->b_items, items, st), "upload items"))) return rc;
+    }
+    double ms = 0;
+    if ((rc = run(shape, nchain, &ms))) return rc;
+    // ---- continued fractions for every chain ----
+    std::vector<double> al(ld * nchain), be(ld * nchain);
+    std::vector<int32_t> done(nchain);
+    cudaMemcpyAsync(al.data(), c->b_alpha.p, sizeof(double) * ld * nchain, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(be.data(), c->b_beta.p, sizeof(double) * ld * nchain, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(done.data(), c->b_done.p, sizeof(int32_t) * nchain, cudaMemcpyDeviceToHost, st);
+    if ((rc = c->cuda(cudaStreamSynchronize(st), "sync"))) return rc;
+    c->d2h_bytes += (int64_t)(sizeof(double) * 2 * ld * nchain + sizeof(int32_t) * nchain);
+    std::vector<int32_t> n(nchain);
+    std::vector<double> e(nchain), ph(nchain), scale(nchain);
+    int64_t steps = 0;
+    for (int q = 0; q < nchain; ++q) {
+        const int i = order[q];
+        int m = done[q];
+        for (int k = 1; k < m; ++k)
+            if (!(be[q * ld + k] >= 1e-25)) { m = k; break; }
+        n[q] = m;
+        steps += done[q];
+        e[q] = ch[i].e0;
+        ph[q] = ch[i].iph == 1 ? 1.0 : -1.0;
+        scale[q] = m > 0 ? be[q * ld] * be[q * ld] : 0.0;
+    }
+    std::vector<double> G(2 * (size_t)nchain * nw);
+    if ((rc = edk_cf_eval(c, nchain, (int32_t)ld, n.data(), al.data(), be.data(), e.data(), ph.data(), scale.data(),
+                          nw, wn_host, G.data())))
+        return rc;
+    for (int q = 0; q < nchain; ++q) {
+        const int i = order[q];
+        double *o = G_out + (size_t)ch[i].out * 2 * nw;
+        for (int w = 0; w < 2 * nw; ++w) o[w] += ch[i].weight * G[(size_t)q * 2 * nw + w];
+    }
+    if (stats) {
+        stats->steps = steps;
+        stats->chains = nchain;
+        stats->kernel_ms = ms;
+        stats->block = shape.block;
+        stats->rows = shape.R;
+        stats->blocks_per_sm = shape.per_sm;
+        stats->tuned_shapes = tuned;
+    }
+    return EDK_OK;
+}

@@ -79,6 +79,7 @@ struct RowArgs {
     double *tri_diag = nullptr;    // device alpha array (Dagotto layout, 0-based alpha_{k+1} at [k])
     double *tri_sub = nullptr;     // device beta array (tri_sub[k] = beta_{k+1})
     int k = 0;                     // 1-based step index of v_k
+    double gamma1 = 0.0;           // shift of the first stored vector s_2 = H v_1 - gamma1 v_1
     double eshift = 0.0;           // residual mode: e
     double cutoff = 1e-25;
     double *partials = nullptr;    // gridDim*4 doubles
@@ -95,6 +96,23 @@ struct LaunchCfg {
     bool fast = false;       // use row_fast_kernel (edk_rows_fast.cu)
     int fast_variant = -1;   // -1 = default launch shape of the fast kernel
 };
+
+// One Green chain of a batch (edk_batch.cu).
+struct BatchItem {
+    int32_t ham;             // index into the HamDev array
+    int32_t niter;           // min(nitergreen, dim)
+    int64_t dim;
+    const void *start;       // start vector (batch element type)
+    double gamma1;           // shift of the first stored vector (the state energy)
+    double cutoff_dynamic;
+    double *alpha;           // niter
+    double *beta;            // niter + 1: beta[0] = |start|, beta[k] couples k-1,k
+    int32_t *done;           // steps completed (0 if |start|^2 < cutoff_dynamic)
+};
+cudaError_t launch_batch(int dtype, int R, const HamDev *hams, const BatchItem *items, int nitems, int *queue,
+                         void *work, int64_t maxdim, int64_t maxdup, double cutoff, int grid, int block,
+                         cudaStream_t st);
+int batch_max_blocks_per_sm(int dtype, int R, int block, int64_t maxdup);
 
 // ---- kernel launchers (edk_kernels.cu) ------------------------------------
 LaunchCfg plan_rows(const HamDev &H, int elem_bytes, int num_sms);

@@ -18,16 +18,18 @@
 // multiply and add (no FMA contraction), so the FP64 result equals a
 // sequential FP64 evaluation of HAIMupdo_multr bit for bit.
 //
-// Lanczos step (kModeStep).  With s_{k+1} = w_k = H v_k - beta_k v_{k-1} (not
-// yet orthogonalised against v_k) and alpha_k, beta_{k+1} known from the
-// previous launch's reductions, one pass computes
-//   v_{k+1}   = (s_{k+1} - alpha_k v_k) / beta_{k+1}
-//   H v_{k+1} = (H s_{k+1} - alpha_k s_{k+1} - alpha_k beta_k v_{k-1}) / beta_{k+1}
-//   w_{k+1}   = H v_{k+1} - beta_{k+1} v_k
-// using H v_k = s_{k+1} + beta_k v_{k-1}, and the sums |w|^2, <w,v_{k+1}>,
-// |v_{k+1}|^2 that give alpha_{k+1} = <w,v_{k+1}> and
-// beta_{k+2}^2 = |w|^2 - 2 alpha <w,v> + alpha^2 |v|^2 (lanc_opt,
-// Lanczos_plain.h:66-173, without its separate orthogonalise/normalise passes).
+// Lanczos step (kModeStep).  The previous launch stored s = w_k - gamma_k v_k
+// (w_k = H v_k - beta_k v_{k-1}, gamma_k a shift known before that launch:
+// gamma_1 given, gamma_{k+1} = alpha_k), and its reductions gave alpha_k,
+// beta_{k+1}.  With delta_k = alpha_k - gamma_k one pass computes
+//   v_{k+1}   = (s - delta_k v_k) / beta_{k+1}
+//   H v_{k+1} = (H s - delta_k (s + gamma_k v_k + beta_k v_{k-1})) / beta_{k+1}
+//   w_{k+1}   = H v_{k+1} - beta_{k+1} v_k,   s' = w_{k+1} - alpha_k v_{k+1}
+// using H v_k = s + gamma_k v_k + beta_k v_{k-1}, plus the sums |s'|^2,
+// <s',v_{k+1}>, |v_{k+1}|^2 that give alpha_{k+1} and beta_{k+2}
+// (lanc_opt, Lanczos_plain.h:66-173, without its separate orthogonalise and
+// normalise passes).  The shift keeps |s| near beta, so the rounding of the
+// stored s is not amplified by |alpha|/beta when H s is formed.
 // Reductions are deterministic: per-block partials, summed in block order by
 // the last block to finish.
 #include <cuda_runtime.h>
@@ -112,12 +114,18 @@ __global__ void __launch_bounds__(512, 1) row_kernel(const HamDev H, const RowAr
     const int64_t dup = H.dup, ddn = H.ddn;
     const T *__restrict__ x = static_cast<const T *>(a.x);
 
-    double alpha = 0.0, beta_k = 0.0, beta_k1 = 0.0, inv_b = 0.0, cpsi = 0.0;
+    // step scalars: s = w_k - gamma_k v_k was stored by the previous launch;
+    // delta_k = alpha_k - gamma_k; the new vector is s' = w_{k+1} - gamma_{k+1} v_{k+1}
+    // with gamma_{k+1} = alpha_k
+    double delta = 0.0, gam = 0.0, gam1 = a.gamma1, beta_k = 0.0, beta_k1 = 0.0, inv_b = 0.0, cpsi = 0.0;
     if (a.mode == kModeStep) {
         beta_k1 = a.tri_sub[a.k];
         // the chain already ended (breakdown recorded by an earlier launch)
-        if (!(beta_k1 >= a.cutoff) || a.flags[0] != 0) return;            // breakdown recorded by the previous launch
-        alpha = a.tri_diag[a.k - 1];
+        if (!(beta_k1 >= a.cutoff) || a.flags[0] != 0) return;
+        const double alpha = a.tri_diag[a.k - 1];
+        gam = a.k >= 2 ? a.tri_diag[a.k - 2] : a.gamma1;
+        delta = alpha - gam;
+        gam1 = alpha;
         beta_k = a.k >= 2 ? a.tri_sub[a.k - 1] : 0.0;
         inv_b = 1.0 / beta_k1;
         if (a.psi_coef) cpsi = a.psi_coef[a.k];
@@ -266,17 +274,19 @@ __global__ void __launch_bounds__(512, 1) row_kernel(const HamDev H, const RowAr
                 if (a.mode == kModeHv) {
                     static_cast<T *>(a.y)[i] = acc[r];
                 } else if (a.mode == kModeFirst) {
-                    const double w = (double)acc[r], v = (double)xo[r];
-                    static_cast<T *>(a.y)[i] = acc[r];
-                    s0 += w * w; s1 += w * v; s2 += v * v;
+                    const double v = (double)xo[r];
+                    const T st = (T)((double)acc[r] - gam1 * v);
+                    static_cast<T *>(a.y)[i] = st;
+                    const double sd = (double)st;
+                    s0 += sd * sd; s1 += sd * v; s2 += v * v;
                 } else if (a.mode == kModeStep) {
                     const double sv = (double)xo[r];
                     const double vk = (double)static_cast<const T *>(a.vk)[i];
                     const double vm = a.vkm1 ? (double)static_cast<const T *>(a.vkm1)[i] : 0.0;
-                    const double v1 = (sv - alpha * vk) * inv_b;
-                    const double hv1 = ((double)acc[r] - alpha * sv - (alpha * beta_k) * vm) * inv_b;
+                    const T vt = (T)((sv - delta * vk) * inv_b);
+                    const double hv1 = ((double)acc[r] - delta * (sv + gam * vk + beta_k * vm)) * inv_b;
                     const double w = hv1 - beta_k1 * vk;
-                    const T wt = (T)w, vt = (T)v1;
+                    const T wt = (T)(w - gam1 * (double)vt);
                     static_cast<T *>(a.y)[i] = wt;
                     static_cast<T *>(a.vout)[i] = vt;
                     if (a.psi) {

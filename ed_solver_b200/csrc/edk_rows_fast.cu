@@ -55,12 +55,18 @@ __global__ void __launch_bounds__(512, 1) row_fast_kernel(const HamDev H, const 
     const int64_t ddn = H.ddn;
     const T *__restrict__ x = static_cast<const T *>(a.x);
 
-    double alpha = 0.0, beta_k = 0.0, beta_k1 = 0.0, inv_b = 0.0, cpsi = 0.0;
+    // step scalars: s = w_k - gamma_k v_k was stored by the previous launch;
+    // delta_k = alpha_k - gamma_k; the new vector is s' = w_{k+1} - gamma_{k+1} v_{k+1}
+    // with gamma_{k+1} = alpha_k
+    double delta = 0.0, gam = 0.0, gam1 = a.gamma1, beta_k = 0.0, beta_k1 = 0.0, inv_b = 0.0, cpsi = 0.0;
     if (a.mode == kModeStep) {
         beta_k1 = a.tri_sub[a.k];
         // the chain already ended (breakdown recorded by an earlier launch)
         if (!(beta_k1 >= a.cutoff) || a.flags[0] != 0) return;
-        alpha = a.tri_diag[a.k - 1];
+        const double alpha = a.tri_diag[a.k - 1];
+        gam = a.k >= 2 ? a.tri_diag[a.k - 2] : a.gamma1;
+        delta = alpha - gam;
+        gam1 = alpha;
         beta_k = a.k >= 2 ? a.tri_sub[a.k - 1] : 0.0;
         inv_b = 1.0 / beta_k1;
         if (a.psi_coef) cpsi = a.psi_coef[a.k];
@@ -194,12 +200,15 @@ __global__ void __launch_bounds__(512, 1) row_fast_kernel(const HamDev H, const 
                 if (a.mode == kModeHv) {
                     st2(y, acc[r][0], acc[r][1], stream);
                 } else if (a.mode == kModeFirst) {
-                    st2(y, acc[r][0], acc[r][1], stream);
+                    T st[2];
 #pragma unroll
                     for (int e = 0; e < 2; ++e) {
-                        const double w = (double)acc[r][e], v = (double)xo[e];
-                        s0 += w * w; s1 += w * v; s2 += v * v;
+                        const double v = (double)xo[e];
+                        st[e] = (T)((double)acc[r][e] - gam1 * v);
+                        const double sd = (double)st[e];
+                        s0 += sd * sd; s1 += sd * v; s2 += v * v;
                     }
+                    st2(y, st[0], st[1], stream);
                 } else if (a.mode == kModeStep) {
                     const auto vk2 = ld2(static_cast<const T *>(a.vk) + i, stream);
                     typename V2<T>::t vm2;
@@ -210,11 +219,10 @@ __global__ void __launch_bounds__(512, 1) row_fast_kernel(const HamDev H, const 
 #pragma unroll
                     for (int e = 0; e < 2; ++e) {
                         const double sv = (double)xo[e];
-                        const double v1 = (sv - alpha * vk[e]) * inv_b;
-                        const double hv1 = ((double)acc[r][e] - alpha * sv - (alpha * beta_k) * vm[e]) * inv_b;
+                        vt[e] = (T)((sv - delta * vk[e]) * inv_b);
+                        const double hv1 = ((double)acc[r][e] - delta * (sv + gam * vk[e] + beta_k * vm[e])) * inv_b;
                         const double w = hv1 - beta_k1 * vk[e];
-                        wt[e] = (T)w;
-                        vt[e] = (T)v1;
+                        wt[e] = (T)(w - gam1 * (double)vt[e]);
                         const double wd = (double)wt[e], vd = (double)vt[e];
                         s0 += wd * wd; s1 += wd * vd; s2 += vd * vd;
                     }

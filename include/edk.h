@@ -199,6 +199,34 @@ int edk_double_occ(edk_h *h, int dtype, const void *psi_dev, int site, double *d
 /* |H psi - e psi| and |psi| with the FP64 matvec (psi in FP64). */
 int edk_residual(edk_h *h, const void *psi_dev, double e, double *res_norm, double *psi_norm);
 
+/* ---- batched Green chains ------------------------------------------------
+ * Many compute_dynamic chains (green_class_compute_dynamic.f90:191-334) at
+ * once, as compute_greenAA issues them for every sector, particle/hole part,
+ * eigenstate and orbital combination (green_class_computeAA.f90:105-126).
+ * mode 0: one persistent launch over a work queue (largest chains first, one
+ * thread block per chain, launch shape autotuned once per problem class and
+ * cached on the context); mode 1: one grid per Lanczos step, chain after chain.
+ * G_out[out][w] (interleaved re/im, nout x nw) accumulates weight * dyn. */
+typedef struct edk_chain {
+    edk_h *target;               /* Hamiltonian of the sector start_dev lives in */
+    const void *start_dev;       /* start vector, batch dtype, target dimension */
+    double e0;                   /* energy of the state the vector came from */
+    int32_t iph;                 /* 1 = particle, 2 = hole */
+    double weight;               /* e.g. the Boltzmann weight */
+    int32_t out;                 /* output slot */
+} edk_chain;
+
+typedef struct edk_batch_stats {
+    int64_t steps;               /* Lanczos steps run over all chains */
+    int32_t chains;
+    double kernel_ms;            /* device time of the persistent launch */
+    int32_t block, rows, blocks_per_sm, tuned_shapes;
+} edk_batch_stats;
+
+int edk_green_batch(edk_ctx *ctx, int dtype, int32_t nchain, const edk_chain *chains, int32_t nitergreen,
+                    int32_t nw, const double *wn_host, double cutoff_dynamic, int32_t nout, double *G_out,
+                    int32_t mode, edk_batch_stats *stats);
+
 /* Element-type conversion of a device vector (FP32 <-> FP64, or a copy). */
 int edk_convert(edk_ctx *ctx, int from_dtype, int to_dtype, int64_t n, const void *in_dev, void *out_dev);
 

@@ -119,3 +119,15 @@ def test_hmult_full_size_ns16_bit_exact(ctx):
     y = h.hmult(x).cpu().numpy()
     ho = O.OracleH(m, 8, 8)
     assert np.array_equal(y, ho.hmult(x.cpu().numpy()))
+
+
+@pytest.mark.parametrize("name,sec", [("c3", (7, 7)), ("c3", (8, 7))])
+def test_hmult_fp32_large_sectors(ctx, kpath, name, sec):
+    """FP32 H*v on sectors large enough for multi-row groups (R > 1) in both kernels."""
+    import torch
+    m = workload(name).model
+    h = edk.Hamiltonian(ctx, m, *sec)
+    x = np.random.default_rng(9).normal(size=h.dim)
+    y = h.hmult(torch.tensor(x, dtype=torch.float32, device="cuda")).double().cpu().numpy()
+    y_ref = O.OracleH(m, *sec).hmult(x.astype(np.float32).astype(np.float64))
+    assert np.abs(y - y_ref).max() <= 2e-6 * np.abs(y_ref).max()
