@@ -21,17 +21,17 @@ template <typename T> __device__ __forceinline__ T ldcg(const T *p) { return __l
 template <typename T, int R>
 __device__ void block_rows(const HamDev &H, int mode, const T *x, T *y, const T *vk, const T *vkm1, T *vout,
                            double delta, double gam, double gam1, double beta_k, double beta_k1, double inv_b,
-                           T *xs, const T *pal_s, double &s0, double &s1, double &s2)
+                           T *xs, const double *pal_s, double &s0, double &s1, double &s2)
 {
     const int64_t dup = H.dup, ddn = H.ddn;
     const uint32_t *ell = H.up.ell;
-    const T *ellv = ell_val<T>(H.up);
+    const double *ellv = H.up.ell_val;
     const int K = H.up.ell_k;
-    const T *dnv = tab_val<T>(H.dn);
-    const T *upd = tab_diag<T>(H.up);
-    const T *dnd = tab_diag<T>(H.dn);
-    const T *icoef = int_coef<T>(H);
-    const T *jj = jj_of<T>(H);
+    const double *dnv = H.dn.val;
+    const double *upd = H.up.diag;
+    const double *dnd = H.dn.diag;
+    const double *icoef = H.int_coef;
+    const double *jj = H.jj;
     const int nc = H.nc;
     for (int64_t g0 = 0; g0 < ddn; g0 += R) {
         int row[R];
@@ -45,24 +45,24 @@ __device__ void block_rows(const HamDev &H, int mode, const T *x, T *y, const T 
         __syncthreads();
         for (int64_t c = threadIdx.x; c < dup; c += blockDim.x) {
             const int cu = H.up.imp[c];
-            const T du = upd[c];
+            const double du = upd[c];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 if (row[r] < 0) continue;
                 const T xo = xs[r * dup + c];
                 const int cd = H.dn.imp[row[r]];
                 const int cfg = cu * H.ncfg + cd;
-                T acc = T(0);
-                for (int o = H.int_off[cfg]; o < H.int_off[cfg + 1]; ++o) acc = fadd(acc, fmul(icoef[o], xo));
-                acc = fadd(acc, fmul(fadd(du, dnd[row[r]]), xo));
+                double acc = 0.0;
+                for (int o = H.int_off[cfg]; o < H.int_off[cfg + 1]; ++o) acc = hmadd<T>(acc, icoef[o], xo);
+                acc = hmadd<T>(acc, fadd(du, dnd[row[r]]), xo);
                 for (int k = 0; k < K; ++k) {
                     const uint32_t ent = ell[(int64_t)k * dup + c];
                     const int64_t j = H.up.packed ? (int64_t)(ent & 0xFFFFFFu) : (int64_t)(int32_t)ent;
-                    const T h = H.up.packed ? pal_s[ent >> 24] : ellv[(int64_t)k * dup + c];
-                    acc = fadd(acc, fmul(h, xs[r * dup + j]));
+                    const double h = H.up.packed ? pal_s[ent >> 24] : ellv[(int64_t)k * dup + c];
+                    acc = hmadd<T>(acc, h, xs[r * dup + j]);
                 }
                 for (int f = H.dn.ptr[row[r]]; f < H.dn.ptr[row[r] + 1]; ++f)
-                    acc = fadd(acc, fmul(dnv[f], ldcg(x + (int64_t)H.dn.tgt[f] * dup + c)));
+                    acc = hmadd<T>(acc, dnv[f], ldcg(x + (int64_t)H.dn.tgt[f] * dup + c));
                 if (H.hund) {
                     // Hund spin flip and pair hopping (HAIMupdo.f90:1017-1129), gathers from x
                     for (int s1 = 0; s1 < nc; ++s1) {
@@ -79,7 +79,7 @@ __device__ void block_rows(const HamDev &H, int mode, const T *x, T *y, const T 
                             const int32_t pu = H.up.move[c * H.nmove + mu], pd = H.dn.move[(int64_t)row[r] * H.nmove + md];
                             if (pu == 0 || pd == 0) continue;
                             const int64_t ju = (pu > 0 ? pu : -pu) - 1, jdn = (pd > 0 ? pd : -pd) - 1;
-                            const T t = fmul(ldcg(x + ju + jdn * dup), jj[s1 * nc + s2]);
+                            const double t = fmul((double)ldcg(x + ju + jdn * dup), jj[s1 * nc + s2]);
                             acc = ((pu > 0) == (pd > 0)) ? fadd(acc, t) : fsub(acc, t);
                         }
                     }
@@ -92,7 +92,7 @@ __device__ void block_rows(const HamDev &H, int mode, const T *x, T *y, const T 
                             const int32_t pu = H.up.move[c * H.nmove + mi], pd = H.dn.move[(int64_t)row[r] * H.nmove + mi];
                             if (pu == 0 || pd == 0) continue;
                             const int64_t ju = (pu > 0 ? pu : -pu) - 1, jdn = (pd > 0 ? pd : -pd) - 1;
-                            const T t = fmul(ldcg(x + ju + jdn * dup), jj[s1 * nc + s2]);
+                            const double t = fmul((double)ldcg(x + ju + jdn * dup), jj[s1 * nc + s2]);
                             acc = ((pu > 0) == (pd > 0)) ? fadd(acc, t) : fsub(acc, t);
                         }
                     }
@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(const HamDev *hams, const
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *xs = reinterpret_cast<T *>(smem_raw);
-    __shared__ T pal_s[256];
+    __shared__ double pal_s[256];
     __shared__ double red[3][32];
     __shared__ double bc[4];
     __shared__ int item_id;
@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(const HamDev *hams, const
         const HamDev &H = hams[b.ham];
         const T *start = static_cast<const T *>(b.start);
         if (H.up.packed)
-            for (int i = threadIdx.x; i < H.up.npal; i += blockDim.x) pal_s[i] = pal_of<T>(H.up)[i];
+            for (int i = threadIdx.x; i < H.up.npal; i += blockDim.x) pal_s[i] = H.up.pal[i];
         // |start|^2 and v1 = start / |start|
         double nv[3] = {0.0, 0.0, 0.0};
         for (int64_t i = threadIdx.x; i < b.dim; i += blockDim.x) {

@@ -17,18 +17,18 @@ __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b)
 __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
 
-template <typename T> __device__ __forceinline__ const T *tab_val(const SpinTabDev &t);
-template <> __device__ __forceinline__ const double *tab_val<double>(const SpinTabDev &t) { return t.val; }
-template <> __device__ __forceinline__ const float *tab_val<float>(const SpinTabDev &t) { return t.valf; }
-template <typename T> __device__ __forceinline__ const T *tab_diag(const SpinTabDev &t);
-template <> __device__ __forceinline__ const double *tab_diag<double>(const SpinTabDev &t) { return t.diag; }
-template <> __device__ __forceinline__ const float *tab_diag<float>(const SpinTabDev &t) { return t.diagf; }
-template <typename T> __device__ __forceinline__ const T *int_coef(const HamDev &h);
-template <> __device__ __forceinline__ const double *int_coef<double>(const HamDev &h) { return h.int_coef; }
-template <> __device__ __forceinline__ const float *int_coef<float>(const HamDev &h) { return h.int_coeff; }
-template <typename T> __device__ __forceinline__ const T *jj_of(const HamDev &h);
-template <> __device__ __forceinline__ const double *jj_of<double>(const HamDev &h) { return h.jj; }
-template <> __device__ __forceinline__ const float *jj_of<float>(const HamDev &h) { return h.jjf; }
+// One term of an H*v accumulation.  Coefficients and accumulators are FP64
+// for both vector types.  FP64 vectors: separate multiply and add, so the sum
+// equals a sequential FP64 HAIMupdo_multr bit for bit; FP32 vectors: the
+// element is widened and fused into the FP64 accumulator.  The FP32 path
+// therefore applies exactly the FP64 operator to FP32-stored vectors; only
+// the storage of the Krylov vectors is rounded.
+template <typename T>
+__device__ __forceinline__ double hmadd(double acc, double h, T x)
+{
+    if (sizeof(T) == 8) return fadd(acc, fmul(h, (double)x));
+    return fma(h, (double)x, acc);
+}
 
 // ---------------------------------------------------------------------------
 // deterministic block / grid reductions of NQ doubles
@@ -114,13 +114,6 @@ __device__ __forceinline__ void stage_row(T *dst, const T *src, int64_t n)
     for (int64_t i = head + nv * V + threadIdx.x; i < n; i += blockDim.x) dst[i] = __ldg(src + i);
 }
 
-
-template <typename T> __device__ __forceinline__ const T *ell_val(const SpinTabDev &t);
-template <> __device__ __forceinline__ const double *ell_val<double>(const SpinTabDev &t) { return t.ell_val; }
-template <> __device__ __forceinline__ const float *ell_val<float>(const SpinTabDev &t) { return t.ell_valf; }
-template <typename T> __device__ __forceinline__ const T *pal_of(const SpinTabDev &t);
-template <> __device__ __forceinline__ const double *pal_of<double>(const SpinTabDev &t) { return t.pal; }
-template <> __device__ __forceinline__ const float *pal_of<float>(const SpinTabDev &t) { return t.palf; }
 
 // L2 eviction-priority policies (createpolicy) and loads/stores carrying them.
 __device__ __forceinline__ uint64_t l2_keep()

@@ -203,9 +203,9 @@ struct edk_h {
     int hund = 0;
     // device copies
     struct SpinDev {
-        DevBuf ptr, tgt, val, valf, diag, diagf, imp, move, ell, ell_val, ell_valf, pal, palf;
+        DevBuf ptr, tgt, val, diag, imp, move, ell, ell_val, pal;
     } sd[2];
-    DevBuf int_off_d, int_coef_d, int_coeff_d, jj_d, jjf_d, umask_d, row_order_d;
+    DevBuf int_off_d, int_coef_d, jj_d, umask_d, row_order_d;
     HamDev H;
     // apply_c maps keyed by (spin, dagger, site)
     struct CMap {
@@ -224,29 +224,21 @@ int upload_spin(edk_h *h, int s)
     const SpinTableHost &t = h->tab[s];
     auto &d = h->sd[s];
     cudaStream_t st = c->stream;
-    std::vector<float> valf(t.val.begin(), t.val.end()), diagf(t.diag.begin(), t.diag.end());
-    std::vector<float> ellvf(t.ell_val.begin(), t.ell_val.end()), palf(t.palette.begin(), t.palette.end());
     int rc;
     if ((rc = c->cuda(upload(d.ptr, t.ptr, st), "upload ptr"))) return rc;
     if ((rc = c->cuda(upload(d.tgt, t.tgt, st), "upload tgt"))) return rc;
     if ((rc = c->cuda(upload(d.val, t.val, st), "upload val"))) return rc;
-    if ((rc = c->cuda(upload(d.valf, valf, st), "upload valf"))) return rc;
     if ((rc = c->cuda(upload(d.diag, t.diag, st), "upload diag"))) return rc;
-    if ((rc = c->cuda(upload(d.diagf, diagf, st), "upload diagf"))) return rc;
     if ((rc = c->cuda(upload(d.imp, t.imp, st), "upload imp"))) return rc;
     if ((rc = c->cuda(upload(d.move, t.move, st), "upload move"))) return rc;
     if ((rc = c->cuda(upload(d.ell, t.ell, st), "upload ell"))) return rc;
     if ((rc = c->cuda(upload(d.ell_val, t.ell_val, st), "upload ell_val"))) return rc;
-    if ((rc = c->cuda(upload(d.ell_valf, ellvf, st), "upload ell_valf"))) return rc;
     if ((rc = c->cuda(upload(d.pal, t.palette, st), "upload pal"))) return rc;
-    if ((rc = c->cuda(upload(d.palf, palf, st), "upload palf"))) return rc;
     SpinTabDev &o = (s == 0) ? h->H.up : h->H.dn;
     o.ptr = d.ptr.as<int32_t>();
     o.tgt = d.tgt.as<int32_t>();
     o.val = d.val.as<double>();
-    o.valf = d.valf.as<float>();
     o.diag = d.diag.as<double>();
-    o.diagf = d.diagf.as<float>();
     o.imp = d.imp.as<uint8_t>();
     o.move = d.move.as<int32_t>();
     o.ell_k = t.ell_k;
@@ -254,9 +246,7 @@ int upload_spin(edk_h *h, int s)
     o.npal = (int)t.palette.size();
     o.ell = d.ell.as<uint32_t>();
     o.ell_val = d.ell_val.as<double>();
-    o.ell_valf = d.ell_valf.as<float>();
     o.pal = d.pal.as<double>();
-    o.palf = d.palf.as<float>();
     return EDK_OK;
 }
 
@@ -668,15 +658,12 @@ int edk_h_create(edk_ctx *ctx, const edk_model *m, int nup, int ndn, edk_h **out
     if ((rc = upload_spin(h.get(), 0))) return rc;
     if ((rc = upload_spin(h.get(), 1))) return rc;
     cudaStream_t st = ctx->stream;
-    std::vector<float> icf(h->int_coef.begin(), h->int_coef.end()), jjf(mh.jj.begin(), mh.jj.end());
     std::vector<uint8_t> umask(mh.nc * mh.nc);
     for (int i = 0; i < mh.nc * mh.nc; ++i) umask[i] = mh.u[i] != 0.0;
     auto order = row_schedule(h->tab[1].states, mh.nc, mh.nb);
     if ((rc = ctx->cuda(upload(h->int_off_d, h->int_off, st), "upload"))) return rc;
     if ((rc = ctx->cuda(upload(h->int_coef_d, h->int_coef, st), "upload"))) return rc;
-    if ((rc = ctx->cuda(upload(h->int_coeff_d, icf, st), "upload"))) return rc;
     if ((rc = ctx->cuda(upload(h->jj_d, mh.jj, st), "upload"))) return rc;
-    if ((rc = ctx->cuda(upload(h->jjf_d, jjf, st), "upload"))) return rc;
     if ((rc = ctx->cuda(upload(h->umask_d, umask, st), "upload"))) return rc;
     if ((rc = ctx->cuda(upload(h->row_order_d, order, st), "upload"))) return rc;
     HamDev &H = h->H;
@@ -690,9 +677,7 @@ int edk_h_create(edk_ctx *ctx, const edk_model *m, int nup, int ndn, edk_h **out
         H.dn_kmax = std::max<int>(H.dn_kmax, h->tab[1].ptr[r + 1] - h->tab[1].ptr[r]);
     H.int_off = h->int_off_d.as<int32_t>();
     H.int_coef = h->int_coef_d.as<double>();
-    H.int_coeff = h->int_coeff_d.as<float>();
     H.jj = h->jj_d.as<double>();
-    H.jjf = h->jjf_d.as<float>();
     H.umask = h->umask_d.as<uint8_t>();
     H.row_order = h->row_order_d.as<int32_t>();
     {

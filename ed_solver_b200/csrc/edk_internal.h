@@ -21,9 +21,7 @@ struct SpinTabDev {
     const int32_t *ptr = nullptr;    // dim+1 CSR offsets
     const int32_t *tgt = nullptr;    // nnz, 0-based target rank
     const double *val = nullptr;     // nnz
-    const float *valf = nullptr;
     const double *diag = nullptr;    // dim
-    const float *diagf = nullptr;
     const uint8_t *imp = nullptr;    // dim: occupation bits of the impurity sites
     const int32_t *move = nullptr;   // dim * nmove: (rank+1)*sign of moving one
                                      // electron between impurity sites, 0 if none
@@ -37,9 +35,7 @@ struct SpinTabDev {
     int npal = 0;
     const uint32_t *ell = nullptr;
     const double *ell_val = nullptr;
-    const float *ell_valf = nullptr;
     const double *pal = nullptr;      // npal <= 256
-    const float *palf = nullptr;
 };
 
 // Everything a row kernel needs to evaluate (H x) for an element.
@@ -52,9 +48,7 @@ struct HamDev {
     SpinTabDev up, dn;
     const int32_t *int_off = nullptr;  // ncfg*ncfg+1 offsets into the coefficient lists
     const double *int_coef = nullptr;  // per (cfg_up, cfg_dn): the ordered density terms
-    const float *int_coeff = nullptr;
     const double *jj = nullptr;        // nc*nc (device)
-    const float *jjf = nullptr;
     const uint8_t *umask = nullptr;    // nc*nc
     const int32_t *row_order = nullptr;  // ddn: schedule of rows for L2 reuse
 };

@@ -48,11 +48,11 @@ __device__ __forceinline__ int move_index(int a, int b, int nc)
 
 // Hund spin flip and pair hopping for element (iup, ido) (HAIMupdo.f90:1017-1129).
 template <typename T>
-__device__ __forceinline__ T hund_terms(const HamDev &H, const T *x, int64_t iup, int64_t ido,
-                                        int cu, int cd, T acc)
+__device__ __forceinline__ double hund_terms(const HamDev &H, const T *x, int64_t iup, int64_t ido,
+                                             int cu, int cd, double acc)
 {
     const int nc = H.nc;
-    const T *jj = jj_of<T>(H);
+    const double *jj = H.jj;
     // spin flip, sites s1 < s2 singly occupied with opposite spins
     for (int s1 = 0; s1 < nc; ++s1) {
         const int b1u = (cu >> s1) & 1, b1d = (cd >> s1) & 1;
@@ -69,7 +69,7 @@ __device__ __forceinline__ T hund_terms(const HamDev &H, const T *x, int64_t iup
             const int32_t pd = H.dn.move[ido * H.nmove + md];
             if (pu == 0 || pd == 0) continue;
             const int64_t ju = (pu > 0 ? pu : -pu) - 1, jd = (pd > 0 ? pd : -pd) - 1;
-            const T t = fmul(__ldg(x + ju + jd * H.dup), jj[s1 * nc + s2]);
+            const double t = fmul((double)__ldg(x + ju + jd * H.dup), jj[s1 * nc + s2]);
             acc = ((pu > 0) == (pd > 0)) ? fadd(acc, t) : fsub(acc, t);
         }
     }
@@ -84,7 +84,7 @@ __device__ __forceinline__ T hund_terms(const HamDev &H, const T *x, int64_t iup
             const int32_t pd = H.dn.move[ido * H.nmove + m];
             if (pu == 0 || pd == 0) continue;
             const int64_t ju = (pu > 0 ? pu : -pu) - 1, jd = (pd > 0 ? pd : -pd) - 1;
-            const T t = fmul(__ldg(x + ju + jd * H.dup), jj[s1 * nc + s2]);
+            const double t = fmul((double)__ldg(x + ju + jd * H.dup), jj[s1 * nc + s2]);
             acc = ((pu > 0) == (pd > 0)) ? fadd(acc, t) : fsub(acc, t);
         }
     }
@@ -106,10 +106,10 @@ __global__ void __launch_bounds__(512, 1) row_kernel(const HamDev H, const RowAr
 {
     constexpr int KB = KM > 0 ? KM : 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ T pal_s[256];
+    __shared__ double pal_s[256];
     __shared__ int s_nd[R];
     __shared__ int s_jd[R][KB];
-    __shared__ T s_hd[R][KB];
+    __shared__ double s_hd[R][KB];
     T *xs = reinterpret_cast<T *>(smem_raw);
     const int64_t dup = H.dup, ddn = H.ddn;
     const T *__restrict__ x = static_cast<const T *>(a.x);
@@ -131,29 +131,28 @@ __global__ void __launch_bounds__(512, 1) row_kernel(const HamDev H, const RowAr
         if (a.psi_coef) cpsi = a.psi_coef[a.k];
     }
     if (PACKED) {
-        const T *p = pal_of<T>(H.up);
-        for (int i = threadIdx.x; i < H.up.npal; i += blockDim.x) pal_s[i] = p[i];
+        for (int i = threadIdx.x; i < H.up.npal; i += blockDim.x) pal_s[i] = H.up.pal[i];
     }
 
     const uint32_t *__restrict__ ell = H.up.ell;
-    const T *__restrict__ ellv = ell_val<T>(H.up);
+    const double *__restrict__ ellv = H.up.ell_val;
     const int K = H.up.ell_k;
-    const T *__restrict__ dnv = tab_val<T>(H.dn);
-    const T *__restrict__ upd = tab_diag<T>(H.up);
-    const T *__restrict__ dnd = tab_diag<T>(H.dn);
-    const T *__restrict__ icoef = int_coef<T>(H);
+    const double *__restrict__ dnv = H.dn.val;
+    const double *__restrict__ upd = H.up.diag;
+    const double *__restrict__ dnd = H.dn.diag;
+    const double *__restrict__ icoef = H.int_coef;
 
     double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
     const int64_t ngroups = (ddn + R - 1) / R;
     for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
         int row[R];
-        T dd[R];
+        double dd[R];
         int cd[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int64_t q = g * R + r;
             row[r] = q < ddn ? H.row_order[q] : -1;
-            dd[r] = row[r] >= 0 ? dnd[row[r]] : T(0);
+            dd[r] = row[r] >= 0 ? dnd[row[r]] : 0.0;
             cd[r] = row[r] >= 0 ? (int)H.dn.imp[row[r]] : 0;
         }
         __syncthreads();                                 // previous group done with shared data
@@ -161,7 +160,7 @@ __global__ void __launch_bounds__(512, 1) row_kernel(const HamDev H, const RowAr
             for (int t = threadIdx.x; t < R * KM; t += blockDim.x) {
                 const int r = t / KM, f = t % KM;
                 int nd = 0, jd = 0;
-                T hd = T(0);
+                double hd = 0.0;
                 if (row[r] >= 0) {
                     const int f0 = H.dn.ptr[row[r]];
                     nd = H.dn.ptr[row[r] + 1] - f0;
@@ -180,12 +179,13 @@ __global__ void __launch_bounds__(512, 1) row_kernel(const HamDev H, const RowAr
         __syncthreads();
         for (int64_t c = threadIdx.x; c < dup; c += blockDim.x) {
             const int cu = H.up.imp[c];
-            const T du = upd[c];
-            T acc[R], xo[R];
+            const double du = upd[c];
+            double acc[R];
+            T xo[R];
             if (KM > 0) {
                 // ---- issue every load of this column first ----
                 uint32_t ent[KB];
-                T hv[KB];
+                double hv[KB];
 #pragma unroll
                 for (int k = 0; k < KB; ++k) {
                     if (k < K) {
@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(512, 1) row_kernel(const HamDev H, const RowAr
                         if (!PACKED) hv[k] = __ldg(ellv + (int64_t)k * dup + c);
                     } else {
                         ent[k] = (uint32_t)c;
-                        if (!PACKED) hv[k] = T(0);
+                        if (!PACKED) hv[k] = 0.0;
                     }
                 }
                 T xd[R][KB];
@@ -210,49 +210,49 @@ __global__ void __launch_bounds__(512, 1) row_kernel(const HamDev H, const RowAr
                 for (int r = 0; r < R; ++r) {
                     const int cfg = cu * H.ncfg + cd[r];
                     const int o0 = H.int_off[cfg], o1 = H.int_off[cfg + 1];
-                    T ac = T(0);
-                    for (int o = o0; o < o1; ++o) ac = fadd(ac, fmul(icoef[o], xo[r]));
-                    acc[r] = fadd(ac, fmul(fadd(du, dd[r]), xo[r]));
+                    double ac = 0.0;
+                    for (int o = o0; o < o1; ++o) ac = hmadd<T>(ac, icoef[o], xo[r]);
+                    acc[r] = hmadd<T>(ac, fadd(du, dd[r]), xo[r]);
                 }
 #pragma unroll
                 for (int k = 0; k < KB; ++k) {
                     if (k >= K) break;
                     const int64_t j = PACKED ? (int64_t)(ent[k] & 0xFFFFFFu) : (int64_t)(int32_t)ent[k];
-                    const T h = PACKED ? pal_s[ent[k] >> 24] : hv[k];
+                    const double h = PACKED ? pal_s[ent[k] >> 24] : hv[k];
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         const T xj = STAGE ? xs[(size_t)r * dup + j] : __ldg(x + (int64_t)row[r] * dup + j);
-                        acc[r] = fadd(acc[r], fmul(h, xj));
+                        acc[r] = hmadd<T>(acc[r], h, xj);
                     }
                 }
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
 #pragma unroll
                     for (int f = 0; f < KB; ++f)
-                        if (f < s_nd[r]) acc[r] = fadd(acc[r], fmul(s_hd[r][f], xd[r][f]));
+                        if (f < s_nd[r]) acc[r] = hmadd<T>(acc[r], s_hd[r][f], xd[r][f]);
                     if (H.hund && row[r] >= 0) acc[r] = hund_terms<T>(H, x, c, row[r], cu, cd[r], acc[r]);
                 }
             } else {
                 // ---- generic tables: dynamic loops ----
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    if (row[r] < 0) { acc[r] = T(0); xo[r] = T(0); continue; }
+                    if (row[r] < 0) { acc[r] = 0.0; xo[r] = T(0); continue; }
                     xo[r] = STAGE ? xs[(size_t)r * dup + c] : __ldg(x + (int64_t)row[r] * dup + c);
                     const int cfg = cu * H.ncfg + cd[r];
                     const int o0 = H.int_off[cfg], o1 = H.int_off[cfg + 1];
-                    T ac = T(0);
-                    for (int o = o0; o < o1; ++o) ac = fadd(ac, fmul(icoef[o], xo[r]));
-                    acc[r] = fadd(ac, fmul(fadd(du, dd[r]), xo[r]));
+                    double ac = 0.0;
+                    for (int o = o0; o < o1; ++o) ac = hmadd<T>(ac, icoef[o], xo[r]);
+                    acc[r] = hmadd<T>(ac, fadd(du, dd[r]), xo[r]);
                 }
                 for (int k = 0; k < K; ++k) {
                     const uint32_t ent = __ldg(ell + (int64_t)k * dup + c);
                     const int64_t j = PACKED ? (int64_t)(ent & 0xFFFFFFu) : (int64_t)(int32_t)ent;
-                    const T h = PACKED ? pal_s[ent >> 24] : __ldg(ellv + (int64_t)k * dup + c);
+                    const double h = PACKED ? pal_s[ent >> 24] : __ldg(ellv + (int64_t)k * dup + c);
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         if (row[r] < 0) continue;
                         const T xj = STAGE ? xs[(size_t)r * dup + j] : __ldg(x + (int64_t)row[r] * dup + j);
-                        acc[r] = fadd(acc[r], fmul(h, xj));
+                        acc[r] = hmadd<T>(acc[r], h, xj);
                     }
                 }
 #pragma unroll
@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(512, 1) row_kernel(const HamDev H, const RowAr
                     const int f0 = H.dn.ptr[row[r]], f1 = H.dn.ptr[row[r] + 1];
                     for (int f = f0; f < f1; ++f) {
                         const int64_t jd = H.dn.tgt[f];
-                        acc[r] = fadd(acc[r], fmul(dnv[f], __ldg(x + jd * dup + c)));
+                        acc[r] = hmadd<T>(acc[r], dnv[f], __ldg(x + jd * dup + c));
                     }
                     if (H.hund) acc[r] = hund_terms<T>(H, x, c, row[r], cu, cd[r], acc[r]);
                 }
@@ -272,7 +272,7 @@ __global__ void __launch_bounds__(512, 1) row_kernel(const HamDev H, const RowAr
                 if (row[r] < 0) continue;
                 const int64_t i = (int64_t)row[r] * dup + c;
                 if (a.mode == kModeHv) {
-                    static_cast<T *>(a.y)[i] = acc[r];
+                    static_cast<T *>(a.y)[i] = (T)acc[r];
                 } else if (a.mode == kModeFirst) {
                     const double v = (double)xo[r];
                     const T st = (T)((double)acc[r] - gam1 * v);

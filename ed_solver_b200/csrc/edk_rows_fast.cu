@@ -10,8 +10,10 @@
 //     before the ordered accumulation;
 //   * x is read with an L2 evict_last policy, the streamed vectors and all
 //     outputs with evict_first, so the neighbour rows stay resident longer;
-//   * FP32 uses fused multiply-add; FP64 keeps separate multiply and add so
-//     the result stays bit-identical to a sequential HAIMupdo_multr.
+//   * coefficients and accumulators are FP64 for both vector types (hmadd):
+//     FP32 vectors are widened and fused into FP64 accumulators; FP64 keeps
+//     separate multiply and add so the result stays bit-identical to a
+//     sequential HAIMupdo_multr.
 #include "edk_device.cuh"
 
 namespace edk {
@@ -19,13 +21,6 @@ namespace edk {
 template <typename T> struct V2;
 template <> struct V2<float> { using t = float2; };
 template <> struct V2<double> { using t = double2; };
-
-template <typename T, bool EXACT>
-__device__ __forceinline__ T madd(T acc, T h, T x)
-{
-    if (EXACT) return fadd(acc, fmul(h, x));
-    return fma(h, x, acc);
-}
 
 // The R staged rows are interleaved element by element in shared memory
 // (xs[j*R + r]), so the R values a gather needs at target j are one aligned
@@ -43,13 +38,12 @@ __device__ __forceinline__ RowVec<T, R> lds_rows(const T *xs, uint32_t j)
 template <typename T, int R, int KM>
 __global__ void __launch_bounds__(512, 1) row_fast_kernel(const HamDev H, const RowArgs a)
 {
-    constexpr bool EXACT = sizeof(T) == 8;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ T pal_s[256];
+    __shared__ double pal_s[256];
     __shared__ int s_ioff[17];
-    __shared__ T s_icoef[96];
+    __shared__ double s_icoef[96];
     __shared__ int s_nofs[R][KM];
-    __shared__ T s_hd[R][KM];
+    __shared__ double s_hd[R][KM];
     T *xs = reinterpret_cast<T *>(smem_raw);
     const int dup = (int)H.dup;
     const int64_t ddn = H.ddn;
@@ -72,27 +66,25 @@ __global__ void __launch_bounds__(512, 1) row_fast_kernel(const HamDev H, const 
         if (a.psi_coef) cpsi = a.psi_coef[a.k];
     }
     {
-        const T *p = pal_of<T>(H.up);
-        for (int i = threadIdx.x; i < H.up.npal; i += blockDim.x) pal_s[i] = p[i];
+        for (int i = threadIdx.x; i < H.up.npal; i += blockDim.x) pal_s[i] = H.up.pal[i];
         const int nio = H.ncfg * H.ncfg + 1;
         for (int i = threadIdx.x; i < nio; i += blockDim.x) s_ioff[i] = H.int_off[i];
-        const T *ic = int_coef<T>(H);
         const int ncoef = H.int_off[nio - 1];
-        for (int i = threadIdx.x; i < ncoef; i += blockDim.x) s_icoef[i] = ic[i];
+        for (int i = threadIdx.x; i < ncoef; i += blockDim.x) s_icoef[i] = H.int_coef[i];
     }
     const uint64_t keep = l2_keep(), stream = l2_stream();
     const uint32_t *__restrict__ ell = H.up.ell;
     const int K = H.up.ell_k;
-    const T *__restrict__ dnv = tab_val<T>(H.dn);
-    const T *__restrict__ upd = tab_diag<T>(H.up);
-    const T *__restrict__ dnd = tab_diag<T>(H.dn);
+    const double *__restrict__ dnv = H.dn.val;
+    const double *__restrict__ upd = H.up.diag;
+    const double *__restrict__ dnd = H.dn.diag;
     const int ncfg = H.ncfg;
 
     double s0 = 0.0, s1 = 0.0, s2 = 0.0;
     const int64_t ngroups = (ddn + R - 1) / R;
     for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
         int row[R], cd[R];
-        T dd[R];
+        double dd[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int64_t q = g * R + r;
@@ -110,7 +102,7 @@ __global__ void __launch_bounds__(512, 1) row_fast_kernel(const HamDev H, const 
             const int f0 = H.dn.ptr[rr], nd = H.dn.ptr[rr + 1] - f0;
             const bool ok = f < nd;
             s_nofs[r][f] = (ok ? H.dn.tgt[f0 + f] : rr) * dup;
-            s_hd[r][f] = ok ? dnv[f0 + f] : T(0);
+            s_hd[r][f] = ok ? dnv[f0 + f] : 0.0;
         }
         // stage the R rows interleaved: xs[c*R + r]
         {
@@ -155,18 +147,18 @@ __global__ void __launch_bounds__(512, 1) row_fast_kernel(const HamDev H, const 
                     for (int f = 0; f < KM; ++f) prefetch_l2(x + s_nofs[r][f] + c + 2 * blockDim.x);
             }
             const int cu0 = H.up.imp[c], cu1 = H.up.imp[c + 1];
-            const T du0 = upd[c], du1 = upd[c + 1];
+            const double du0 = upd[c], du1 = upd[c + 1];
             const RowVec<T, R> o0 = lds_rows<T, R>(xs, c), o1 = lds_rows<T, R>(xs, c + 1);
-            T acc[R][2];
+            double acc[R][2];
             // ---- ordered accumulation: density terms, diagonal ----
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                T a0 = T(0), a1 = T(0);
+                double a0 = 0.0, a1 = 0.0;
                 const int g0 = cu0 * ncfg + cd[r], g1 = cu1 * ncfg + cd[r];
-                for (int o2 = s_ioff[g0]; o2 < s_ioff[g0 + 1]; ++o2) a0 = fadd(a0, fmul(s_icoef[o2], o0.v[r]));
-                for (int o2 = s_ioff[g1]; o2 < s_ioff[g1 + 1]; ++o2) a1 = fadd(a1, fmul(s_icoef[o2], o1.v[r]));
-                acc[r][0] = fadd(a0, fmul(fadd(du0, dd[r]), o0.v[r]));
-                acc[r][1] = fadd(a1, fmul(fadd(du1, dd[r]), o1.v[r]));
+                for (int o2 = s_ioff[g0]; o2 < s_ioff[g0 + 1]; ++o2) a0 = hmadd<T>(a0, s_icoef[o2], o0.v[r]);
+                for (int o2 = s_ioff[g1]; o2 < s_ioff[g1 + 1]; ++o2) a1 = hmadd<T>(a1, s_icoef[o2], o1.v[r]);
+                acc[r][0] = hmadd<T>(a0, fadd(du0, dd[r]), o0.v[r]);
+                acc[r][1] = hmadd<T>(a1, fadd(du1, dd[r]), o1.v[r]);
             }
             // ---- up-spin hops: one vector load serves the R rows ----
 #pragma unroll
@@ -174,11 +166,11 @@ __global__ void __launch_bounds__(512, 1) row_fast_kernel(const HamDev H, const 
                 if (k >= K) break;
                 const RowVec<T, R> g0 = lds_rows<T, R>(xs, ent[k].x & 0xFFFFFFu);
                 const RowVec<T, R> g1 = lds_rows<T, R>(xs, ent[k].y & 0xFFFFFFu);
-                const T h0 = pal_s[ent[k].x >> 24], h1 = pal_s[ent[k].y >> 24];
+                const double h0 = pal_s[ent[k].x >> 24], h1 = pal_s[ent[k].y >> 24];
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    acc[r][0] = madd<T, EXACT>(acc[r][0], h0, g0.v[r]);
-                    acc[r][1] = madd<T, EXACT>(acc[r][1], h1, g1.v[r]);
+                    acc[r][0] = hmadd<T>(acc[r][0], h0, g0.v[r]);
+                    acc[r][1] = hmadd<T>(acc[r][1], h1, g1.v[r]);
                 }
             }
             // ---- down-spin hops ----
@@ -186,9 +178,9 @@ __global__ void __launch_bounds__(512, 1) row_fast_kernel(const HamDev H, const 
             for (int r = 0; r < R; ++r)
 #pragma unroll
                 for (int f = 0; f < KM; ++f) {
-                    const T h = s_hd[r][f];
-                    acc[r][0] = madd<T, EXACT>(acc[r][0], h, xd[r][f].x);
-                    acc[r][1] = madd<T, EXACT>(acc[r][1], h, xd[r][f].y);
+                    const double h = s_hd[r][f];
+                    acc[r][0] = hmadd<T>(acc[r][0], h, xd[r][f].x);
+                    acc[r][1] = hmadd<T>(acc[r][1], h, xd[r][f].y);
                 }
             // ---- epilogue ----
 #pragma unroll
@@ -198,7 +190,7 @@ __global__ void __launch_bounds__(512, 1) row_fast_kernel(const HamDev H, const 
                 T *y = static_cast<T *>(a.y) + i;
                 const T xo[2] = {o0.v[r], o1.v[r]};
                 if (a.mode == kModeHv) {
-                    st2(y, acc[r][0], acc[r][1], stream);
+                    st2(y, (T)acc[r][0], (T)acc[r][1], stream);
                 } else if (a.mode == kModeFirst) {
                     T st[2];
 #pragma unroll

@@ -13,9 +13,12 @@
 //     fractions on the Matsubara axis, and the off-diagonal reshuffle
 //     G_ij = (G_{i+j} - G_ii - G_jj)/2 (green_class_compute_symmetric_combination_AA.h:10-60);
 //   the double occupancy of each impurity orbital (correlations_write.h:93-95).
-// Mixed precision (dtype EDK_F32): both Lanczos passes and the Green chains
-// run on FP32 vectors; every ground state is checked with the FP64 matvec and
-// refined once by an FP64 Lanczos restart from the FP32 vector.
+// Mixed precision (dtype EDK_F32): in every sector of at least kLowprecMinDim
+// states both Lanczos passes and the Green chains run on FP32 vectors (FP64
+// coefficients and accumulation); every such ground state is refined once by
+// an FP64 Lanczos restart from the FP32 vector and checked with the FP64
+// matvec.  Smaller sectors stay in FP64: their kernels are bound by launch
+// latency, so FP32 storage would add rounding without saving time.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -38,9 +41,13 @@ struct DBuf {
     ~DBuf() { if (p) cudaFree(p); }
 };
 
+// Sectors with fewer states than this run in FP64 even in mixed precision.
+constexpr int64_t kLowprecMinDim = (int64_t)1 << 20;
+
 struct State {
     int nup, ndn;
     double E;
+    double E_pass1;            // energy of the first (possibly FP32) pass
     int dtype;                 // element type of psi
     DBuf psi;
     double boltz = 0.0;
@@ -75,8 +82,10 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
     const int ns = m->nc + m->nb;
     cudaStream_t st = edk_internal_stream(ctx);
     const double demax = o->demax0 / o->beta;
-    const size_t ebytes = o->dtype == EDK_F64 ? 8 : 4;
     int rc;
+    auto sector_dtype = [&](int64_t dim) {
+        return (o->dtype == EDK_F32 && dim >= kLowprecMinDim) ? EDK_F32 : EDK_F64;
+    };
 
     // sector Hamiltonians are kept on the context, keyed by the model's bytes and the sector
     std::string mkey;
@@ -138,7 +147,7 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
             for (int k = 0; k < j; ++k) {
                 if (k > 0 && !(w[k] <= w[0] + demax)) break;
                 auto stt = std::make_unique<State>();
-                stt->nup = nu; stt->ndn = nd; stt->E = w[k]; stt->dtype = EDK_F64;
+                stt->nup = nu; stt->ndn = nd; stt->E = w[k]; stt->E_pass1 = w[k]; stt->dtype = EDK_F64;
                 stt->psi = DBuf((size_t)dim * 8);
                 std::vector<double> col(dim);
                 for (int64_t q = 0; q < dim; ++q) col[q] = V[(size_t)q * dim + k];
@@ -146,16 +155,18 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
                 found.push_back(std::move(stt));
             }
         } else {
+            const int sdt = sector_dtype(dim);
+            const size_t ebytes = sdt == EDK_F64 ? 8 : 4;
             edk_lanczos_opts lo{};
             lo.nitermax = o->nitermax;
             lo.neigen = std::max(1, o->neigen);
-            lo.tolerance = o->dtype == EDK_F32 ? std::max(o->tolerance, o->tolerance_lowprec) : o->tolerance;
+            lo.tolerance = sdt == EDK_F32 ? std::max(o->tolerance, o->tolerance_lowprec) : o->tolerance;
             lo.demax = demax;
             lo.cutoff_min_lanczos_vec = 1e-25;
-            lo.dtype = o->dtype;
+            lo.dtype = sdt;
             lo.check_every = o->check_every > 0 ? o->check_every : 8;
             lo.ran_tab = o->ran_tab;
-            lo.residual_tol = o->dtype == EDK_F64 ? o->residual_tol : 0.0;
+            lo.residual_tol = sdt == EDK_F64 ? o->residual_tol : 0.0;
             edk_lanczos_result lr{};
             lr.diag = diag.data();
             lr.subdiag = sub.data();
@@ -164,14 +175,13 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
             lanczos_steps += lr.niter;
             for (int k = 0; k < lr.nkept; ++k) {
                 auto stt = std::make_unique<State>();
-                stt->nup = nu; stt->ndn = nd; stt->E = lr.E[k]; stt->dtype = o->dtype;
+                stt->nup = nu; stt->ndn = nd; stt->E = lr.E[k]; stt->E_pass1 = lr.E[k]; stt->dtype = sdt;
                 stt->psi = DBuf((size_t)dim * ebytes);
                 if (!stt->psi.p) return edk_internal_fail(ctx, EDK_ERR_NOMEM, "state vector");
                 if ((rc = edk_lanczos_gs(h, &lo, lr.niter, lr.vecp + (size_t)k * lr.niter, stt->psi.p))) return rc;
                 lanczos_steps += lr.niter;
-                if (o->dtype == EDK_F32) {
+                if (sdt == EDK_F32) {
                     // FP64 refinement restart from the FP32 eigenvector
-                    e0_low = std::min(e0_low, stt->E);
                     DBuf p64((size_t)dim * 8);
                     if ((rc = edk_convert(ctx, EDK_F32, EDK_F64, dim, stt->psi.p, p64.p))) return rc;
                     edk_lanczos_opts ro = lo;
@@ -211,6 +221,7 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
     if (states.empty()) return edk_internal_fail(ctx, EDK_ERR_INVALID, "no eigenstate found");
     double e0 = 1e300;
     for (auto &s : states) e0 = std::min(e0, s->E);
+    for (auto &s : states) e0_low = std::min(e0_low, s->E_pass1);
     std::vector<std::unique_ptr<State>> gs;
     for (auto &s : states)
         if (s->E <= e0 + demax) gs.push_back(std::move(s));
@@ -219,7 +230,7 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
     for (auto &s : gs) s->boltz = std::exp(-o->beta * (s->E - e0)) / z;
     r->e0 = e0;
     r->z = z;
-    r->e0_lowprec = o->dtype == EDK_F32 ? e0_low : e0;
+    r->e0_lowprec = e0_low;
     r->nstates = (int)gs.size();
     for (size_t k = 0; k < gs.size() && k < 64; ++k) {
         if (r->energies) r->energies[k] = gs[k]->E;
@@ -278,7 +289,6 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
         }
         std::vector<double> raw((size_t)combos.size() * nw * 2);
         std::vector<double> Gc((size_t)2 * nw);
-        const int gdt = o->dtype;
         for (int spin = 0; spin < 2; ++spin) {
             if (!((o->spin_mask >> spin) & 1)) continue;
             std::fill(raw.begin(), raw.end(), 0.0);
@@ -287,14 +297,19 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
                 if ((rc = getH(s->nup, s->ndn, &hs_src))) return rc;
                 int64_t sdim = 0;
                 edk_h_dims(hs_src, &sdim, nullptr, nullptr);
-                // the state in the chain precision
-                DBuf conv;
-                const void *psi = s->psi.p;
-                if (s->dtype != gdt) {
-                    conv = DBuf((size_t)sdim * (gdt == EDK_F64 ? 8 : 4));
-                    if ((rc = edk_convert(ctx, s->dtype, gdt, sdim, s->psi.p, conv.p))) return rc;
-                    psi = conv.p;
-                }
+                // the state in the precision of each target sector's chains
+                DBuf conv[2];
+                auto psi_in = [&](int dt, const void **out) -> int {
+                    if (s->dtype == dt) { *out = s->psi.p; return EDK_OK; }
+                    if (!conv[dt].p) {
+                        conv[dt] = DBuf((size_t)sdim * (dt == EDK_F64 ? 8 : 4));
+                        if (!conv[dt].p) return edk_internal_fail(ctx, EDK_ERR_NOMEM, "state copy");
+                        int rc2 = edk_convert(ctx, s->dtype, dt, sdim, s->psi.p, conv[dt].p);
+                        if (rc2) return rc2;
+                    }
+                    *out = conv[dt].p;
+                    return EDK_OK;
+                };
                 for (int iph = 1; iph <= 2; ++iph) {
                     const int d = iph == 1 ? 1 : -1;
                     const int tnu = s->nup + (spin == 0 ? d : 0), tnd = s->ndn + (spin == 1 ? d : 0);
@@ -304,6 +319,9 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
                     int64_t tdim = 0;
                     edk_h_dims(ht, &tdim, nullptr, nullptr);
                     if (tdim == 0) continue;
+                    const int gdt = sector_dtype(tdim);
+                    const void *psi = nullptr;
+                    if ((rc = psi_in(gdt, &psi))) return rc;
                     DBuf phi((size_t)tdim * (gdt == EDK_F64 ? 8 : 4));
                     for (size_t q = 0; q < combos.size(); ++q) {
                         const int i = combos[q].first, j = combos[q].second;

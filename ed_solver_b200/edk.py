@@ -72,6 +72,16 @@ class _SolveResult(C.Structure):
                 ("G", C.c_void_p), ("docc", C.c_void_p), ("energies", C.c_void_p), ("state_sectors", C.c_void_p)]
 
 
+class _Chain(C.Structure):
+    _fields_ = [("target", C.c_void_p), ("start_dev", C.c_void_p), ("e0", C.c_double), ("iph", C.c_int32),
+                ("weight", C.c_double), ("out", C.c_int32)]
+
+
+class _BatchStats(C.Structure):
+    _fields_ = [("steps", C.c_int64), ("chains", C.c_int32), ("kernel_ms", C.c_double), ("block", C.c_int32),
+                ("rows", C.c_int32), ("blocks_per_sm", C.c_int32), ("tuned_shapes", C.c_int32)]
+
+
 _LIB = None
 
 
@@ -116,6 +126,7 @@ def lib():
         "edk_residual": (C.c_int, [P, P, D, P, P]),
         "edk_convert": (C.c_int, [P, C.c_int, C.c_int, I64, P, P]),
         "edk_solve": (C.c_int, [P, P, P, P]),
+        "edk_green_batch": (C.c_int, [P, C.c_int, I32, P, I32, I32, P, D, I32, P, I32, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -430,6 +441,26 @@ def cf_eval(ctx: Context, chains, wn, ld=None):
                                 e.ctypes.data, ph.ctypes.data, sc.ctypes.data, len(wn), wn.ctypes.data,
                                 G.ctypes.data), "edk_cf_eval")
     return G[..., 0] + 1j * G[..., 1]
+
+
+def green_batch(ctx: Context, chains, nitergreen: int, wn, nout: int, mode: int = 0, dtype="f64",
+                cutoff_dynamic=1e-8):
+    """Many compute_dynamic chains at once (edk_green_batch).
+
+    chains: list of dict(h=Hamiltonian of the start vector's sector, start=device tensor, e0, iph (1 particle,
+    2 hole), weight, out).  Returns (G (nout, nw) complex, stats dict)."""
+    wn = np.ascontiguousarray(wn, np.float64)
+    arr = (_Chain * max(len(chains), 1))()
+    for i, c in enumerate(chains):
+        arr[i] = _Chain(c["h"].h, _ptr(c["start"]), float(c["e0"]), int(c["iph"]), float(c.get("weight", 1.0)),
+                        int(c.get("out", 0)))
+    G = np.zeros((nout, len(wn), 2))
+    st = _BatchStats()
+    ctx.check(lib().edk_green_batch(ctx.h, _dtype_code(dtype), len(chains), C.cast(arr, C.c_void_p),
+                                    int(nitergreen), len(wn), wn.ctypes.data, float(cutoff_dynamic), int(nout),
+                                    G.ctypes.data, int(mode), C.byref(st)), "edk_green_batch")
+    stats = {f: getattr(st, f) for f, _ in _BatchStats._fields_}
+    return G[..., 0] + 1j * G[..., 1], stats
 
 
 def solve(ctx: Context, model: AIMModel, sectors, beta: float, nw: int, dtype="f64", neigen=1,

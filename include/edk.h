@@ -41,7 +41,7 @@ extern "C" {
 
 /* ---- element types ----------------------------------------------------- */
 #define EDK_F64 0   /* FP64 vectors and arithmetic (the reference's REAL(DBL) path) */
-#define EDK_F32 1   /* FP32 vectors and H*v, FP64 accumulation of norms and alpha/beta */
+#define EDK_F32 1   /* FP32 vectors; H*v coefficients, accumulation, norms, alpha/beta in FP64 */
 
 typedef struct edk_ctx edk_ctx;   /* device, stream, workspaces */
 typedef struct edk_h edk_h;       /* one (N_up, N_dn) sector Hamiltonian on the device */
@@ -237,9 +237,11 @@ int edk_convert(edk_ctx *ctx, int from_dtype, int to_dtype, int64_t n, const voi
  * (correlations_write.h:93-95) and the (c, c+) Green functions of
  * compute_greenAA (green_class_computeAA.f90:40-185) for the requested
  * impurity orbital pairs and spins.  All inputs and outputs are host buffers;
- * vectors live on the device only.  dtype EDK_F32 = mixed precision: FP32
- * Krylov vectors and H*v with FP64 alpha/beta, FP32 passes refined by one FP64
- * Lanczos restart per state, FP64 residual check, FP64 continued fractions. */
+ * vectors live on the device only.  dtype EDK_F32 = mixed precision: in
+ * sectors of at least 2^20 states, FP32 Krylov vectors (H*v, alpha and beta
+ * still computed in FP64), FP32 passes refined by one FP64 Lanczos restart per
+ * state, FP64 residual check, FP64 continued fractions; smaller sectors, whose
+ * kernels are latency-bound, run in FP64. */
 typedef struct edk_solve_opts {
     int32_t dtype;
     int32_t nsectors;

@@ -8,7 +8,7 @@ import pytest
 
 import oracle as O
 from ed_solver_b200 import edk
-from ed_solver_b200.model import star_model, workload
+from ed_solver_b200.model import matsubara, star_model, workload
 
 pytestmark = pytest.mark.gpu
 
@@ -39,17 +39,50 @@ def test_solve_reference_golden_g_bm(ctx):
     assert np.abs(r["G"][0, 2]).max() < 1e-12
 
 
-@pytest.mark.parametrize("name", ["c1", "c3"])
-def test_mixed_precision_against_fp64(ctx, name):
-    w = workload(name)
+def test_mixed_precision_against_fp64(ctx):
+    """ns=14, (7,7): every sector of the solve has more than 2^20 states, so the
+    mixed path runs FP32 vectors throughout.  Bounds: |dE0/E0| <= 1e-8,
+    max|dG| <= 1e-6 against the FP64 solve."""
+    w = workload("c3")
     # both paths converge the eigenvector (Ritz residual) so the comparison
-    # measures the FP32 arithmetic, not an under-converged FP64 ground state
-    kw = dict(nitergreen=w.nitergreen, spins=(0,), tolerance=1e-12, residual_tol=1e-10)
+    # measures the FP32 storage, not an under-converged FP64 ground state
+    kw = dict(nitergreen=w.nitergreen, spins=(0, 1), tolerance=1e-12, residual_tol=1e-10)
     r64 = edk.solve(ctx, w.model, w.sectors, w.beta, 512, dtype="f64", **kw)
     r32 = edk.solve(ctx, w.model, w.sectors, w.beta, 512, dtype="f32", **kw)
     assert abs(r32["e0"] - r64["e0"]) <= 1e-8 * abs(r64["e0"])
     assert np.abs(r32["G"] - r64["G"]).max() <= 1e-6
     assert r32["residual"] < 1e-6
+    assert r32["e0_lowprec"] != r32["e0"]          # the FP32 pass ran and was refined
+
+
+def test_mixed_precision_keeps_small_sectors_fp64(ctx):
+    """Sectors below 2^20 states run in FP64 in a mixed-precision solve: the
+    result equals the FP64 solve exactly."""
+    w = workload("c1")
+    kw = dict(nitergreen=w.nitergreen, spins=(0, 1), tolerance=1e-12)
+    r64 = edk.solve(ctx, w.model, w.sectors, w.beta, 256, dtype="f64", **kw)
+    r32 = edk.solve(ctx, w.model, w.sectors, w.beta, 256, dtype="f32", **kw)
+    assert r32["e0"] == r64["e0"] and r32["e0_lowprec"] == r32["e0"]
+    assert np.array_equal(r32["G"], r64["G"])
+
+
+def test_fp32_green_chain_small_sector(ctx):
+    """FP32 chain storage on a small sector (FP64 arithmetic): the hole chain
+    of ns=8 has a pole 0.06 from the Fermi level (|G| = 2 at the first
+    Matsubara frequency), the worst conditioning among the workloads.
+    Bound: max|dG| <= 2e-6 against the FP64 chain from the same state."""
+    import torch
+    w = workload("c1")
+    h = edk.Hamiltonian(ctx, w.model, 4, 4)
+    r = h.lanczos_e0("f64", tolerance=1e-12, residual_tol=1e-10)
+    psi = h.lanczos_gs(r["vecp"][0])
+    wn = matsubara(w.beta, 256)
+    for dag, iph in ((True, 1), (False, 2)):
+        phi, ts = h.apply_c(psi, 0, 0, dag)
+        ht = edk.Hamiltonian(ctx, w.model, *ts)
+        G64, *_ = ht.green_chain(phi, w.nitergreen, r["E"][0], iph, wn)
+        G32, *_ = ht.green_chain(phi.to(torch.float32), w.nitergreen, r["E"][0], iph, wn)
+        assert np.abs(G32 - G64).max() <= 2e-6
 
 
 def test_solve_two_orbital_kanamori_all_sectors(ctx):
