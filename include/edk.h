@@ -192,6 +192,25 @@ int edk_cf_eval(edk_ctx *ctx, int32_t nchain, int32_t ld, const int32_t *n_host,
                 const double *ph_host, const double *scale_host, int32_t nw,
                 const double *wn_host, double *G_host);
 
+/* The continued fractions of edk_cf_eval (same arguments, same results and
+ * status codes) without any device allocation; it has no counterpart in the
+ * reference.  For callers that cannot allocate device memory at that point:
+ * code whose device memory is held by another allocator (a framework's caching
+ * allocator, or Krylov workspaces sized to fill HBM), where cudaMalloc would
+ * fail or cudaFree would stall the device.  Its device memory is one static
+ * array of EDK_NOALLOC_SCRATCH_BYTES per device, cut per call into 256-byte
+ * aligned regions (flag, n, diag, subdiag, e, ph, scale, wn, G); a call whose
+ * regions exceed it returns EDK_ERR_INVALID with the byte counts in the error
+ * text.  The first call on a device resolves the array's address
+ * (cudaGetSymbolAddress, that device current); make it before any stream
+ * capture.  All calls on a device share the array and clear its flag first:
+ * calls whose GPU work overlaps race.  The context's device must be current. */
+#define EDK_NOALLOC_SCRATCH_BYTES 4194304
+int edk_cf_eval_noalloc(edk_ctx *ctx, int32_t nchain, int32_t ld, const int32_t *n_host,
+                        const double *diag_host, const double *subdiag_host, const double *e_host,
+                        const double *ph_host, const double *scale_host, int32_t nw,
+                        const double *wn_host, double *G_host);
+
 /* ---- observables --------------------------------------------------------
  * <psi| n_{site,up} n_{site,dn} |psi> (the double occupancy of
  * correlations_write.h:93-95) and |psi|^2 in one pass. */
