@@ -36,7 +36,7 @@ WORKLOAD = dict(name="ns16_halffilled_E0_G512", nc=1, nb=15, sector=(8, 8), beta
 # H*v applications of one plain FP64 solve of this workload (eigen part + Green part),
 # measured on B200 with the library's start-vector table; used to convert a
 # per-step CPU time into solves/s for the reference arm.
-FP64_STEPS_PER_SOLVE = None
+FP64_STEPS_PER_SOLVE = 1418
 PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "row_fast_kernel_step_ns16_f32.txt")
 
 
@@ -299,6 +299,20 @@ def run_ours(args):
         print(json.dumps(out), flush=True)
 
 
+def run_kernel_case(args):
+    """Six FP32 Lanczos steps of the ns=16 (8,8) sector and nothing else: the
+    small case (3.3 GB of vectors) for per-kernel ncu captures."""
+    import torch
+    from ed_solver_b200 import edk
+    ctx = edk.Context(0)
+    h = edk.Hamiltonian(ctx, _model(), *WORKLOAD["sector"])
+    r = h.lanczos_e0(dtype="f32", nitermax=6, tolerance=0.0, check_every=6)
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel_case": "ns16 (8,8) FP32 Lanczos", "dim": h.dim, "niter": r["niter"]}), flush=True)
+    h.close()
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -306,7 +320,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--kernel-case", action="store_true",
+                    help="run only six FP32 Lanczos steps of the (8,8) sector (profiling case)")
     args = ap.parse_args()
+    if args.kernel_case:
+        run_kernel_case(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -92,7 +92,7 @@ struct edk_ctx {
     size_t tri_cap = 0;
     int reduce_grid = 0;
     int kernel_path = 0;     // 0 = fastest applicable row kernel, 1 = generic row kernel only,
-                             // 2/3 = fast kernel launch shape 0/1 when applicable
+                             // 2/3 = the fast kernel where applicable
     // optional event timing of row-kernel launches: (class, start, stop)
     bool timing = false;
     struct Timed { int cls; cudaEvent_t a, b; double elems; };
@@ -214,6 +214,9 @@ struct edk_h {
         DevBuf src, sg;
     };
     std::vector<std::unique_ptr<CMap>> cmaps;
+    // fast-kernel launch shape per element type, chosen by timing on first use
+    FastShape fast_shape[2];
+    bool fast_tuned[2] = {false, false};
 };
 
 namespace {
@@ -301,6 +304,54 @@ RowArgs base_args(edk_h *h)
     return a;
 }
 
+// The fast kernel's launch shape for this sector and element type.  On the
+// first call with an output vector, every feasible shape is timed (two H*v
+// launches each, the first as warm-up) writing into that vector, which the
+// real launch then overwrites; the fastest is kept on the Hamiltonian.
+int fast_shape_for(edk_h *h, int dtype, const RowArgs &a, FastShape &out)
+{
+    edk_ctx *c = h->ctx;
+    const int eb = dtype == EDK_F64 ? 8 : 4;
+    FastShape cand[8];
+    if (c->kernel_path >= 16) {
+        // a fixed candidate, for measurements
+        const int n = fast_shapes(h->H, eb, c->num_sms, cand, 8);
+        if (n == 0) return c->fail(EDK_ERR_INVALID, "fast row kernel: no launch shape");
+        out = cand[(c->kernel_path - 16) % n];
+        return EDK_OK;
+    }
+    if (h->fast_tuned[dtype]) { out = h->fast_shape[dtype]; return EDK_OK; }
+    const int n = fast_shapes(h->H, eb, c->num_sms, cand, 8);
+    if (n == 0) return c->fail(EDK_ERR_INVALID, "fast row kernel: no launch shape");
+    out = cand[0];
+    if (c->kernel_path != 0 || n == 1 || !a.x || !a.y) {
+        if (n == 1 || c->kernel_path != 0) { h->fast_shape[dtype] = out; h->fast_tuned[dtype] = true; }
+        return EDK_OK;
+    }
+    RowArgs t = a;
+    t.mode = kModeHv;
+    cudaEvent_t ea = c->get_event(), eb_ = c->get_event();
+    float best = 3.0e38f;
+    for (int i = 0; i < n; ++i)
+        for (int rep = 0; rep < 2; ++rep) {
+            cudaEventRecord(ea, c->stream);
+            cudaError_t e = launch_rows_fast(h->H, dtype, t, c->num_sms, cand[i], c->stream);
+            cudaEventRecord(eb_, c->stream);
+            c->launches++;
+            if (e != cudaSuccess) { (void)cudaGetLastError(); break; }
+            float ms = 0.f;
+            if (cudaEventSynchronize(eb_) != cudaSuccess || cudaEventElapsedTime(&ms, ea, eb_) != cudaSuccess) break;
+            if (rep == 1 && ms < best) { best = ms; out = cand[i]; }
+        }
+    c->event_pool.push_back(ea);
+    c->event_pool.push_back(eb_);
+    int rc = c->cuda(cudaGetLastError(), "fast row kernel autotune");
+    if (rc) return rc;
+    h->fast_shape[dtype] = out;
+    h->fast_tuned[dtype] = true;
+    return EDK_OK;
+}
+
 int rows(edk_h *h, int dtype, const RowArgs &a)
 {
     edk_ctx *c = h->ctx;
@@ -311,7 +362,10 @@ int rows(edk_h *h, int dtype, const RowArgs &a)
     auto al = [&](const void *p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) % (2 * eb)) == 0; };
     const bool aligned = al(a.x) && al(a.y) && al(a.vk) && al(a.vkm1) && al(a.vout) && al(a.psi);
     cfg.fast = c->kernel_path != 1 && aligned && fast_rows_ok(h->H, eb);
-    cfg.fast_variant = c->kernel_path >= 2 ? c->kernel_path - 2 : -1;
+    if (cfg.fast) {
+        int rc = fast_shape_for(h, dtype, a, cfg.fast_shape);
+        if (rc) return rc;
+    }
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;
     if (c->timing) {
         ev_a = c->get_event();
@@ -548,7 +602,7 @@ int edk_internal_fail(edk_ctx *ctx, int code, const char *msg) { return ctx->fai
 
 int edk_ctx_set_kernel_path(edk_ctx *ctx, int path)
 {
-    if (!ctx || path < 0 || path > 3) return EDK_ERR_INVALID;
+    if (!ctx || path < 0 || (path > 3 && path < 16) || path > 23) return EDK_ERR_INVALID;
     ctx->kernel_path = path;
     return EDK_OK;
 }

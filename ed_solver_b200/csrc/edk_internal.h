@@ -82,14 +82,22 @@ struct RowArgs {
     int *flags = nullptr;          // [0] breakdown step (0 = none), [1] non-finite
 };
 
+// Launch shape of the fast row kernel: rows per group, up/down table-width
+// bounds, and block shape (variant 0: 512 threads, one block per SM;
+// variant 1: 256 threads, two blocks per SM).
+struct FastShape {
+    int r = 0, kmu = 0, kmd = 0, variant = 0;
+};
+
 struct LaunchCfg {
     int grid = 0, block = 0, rows = 1, km = 0, num_sms = 1;
     int64_t groups = 0;
     size_t smem = 0;
     bool stage = true;
-    bool fast = false;       // use row_fast_kernel (edk_rows_fast.cu)
-    int fast_variant = -1;   // -1 = default launch shape of the fast kernel
+    bool fast = false;       // use row_fast_kernel (edk_rows_fast.cuh)
+    FastShape fast_shape;    // its launch shape
 };
+
 
 // One Green chain of a batch (edk_batch.cu).
 struct BatchItem {
@@ -113,7 +121,9 @@ LaunchCfg plan_rows(const HamDev &H, int elem_bytes, int num_sms);
 cudaError_t launch_rows(const HamDev &H, int dtype, const RowArgs &a, const LaunchCfg &cfg,
                         cudaStream_t st);
 bool fast_rows_ok(const HamDev &H, int elem_bytes);
-cudaError_t launch_rows_fast(const HamDev &H, int dtype, const RowArgs &a, int num_sms, int variant,
+// The feasible launch shapes of the fast kernel for H (the first is the default).
+int fast_shapes(const HamDev &H, int elem_bytes, int num_sms, FastShape *out, int cap);
+cudaError_t launch_rows_fast(const HamDev &H, int dtype, const RowArgs &a, int num_sms, const FastShape &s,
                              cudaStream_t st);
 cudaError_t launch_start_vector(int dtype, int64_t n, const double *ran_tab_dev,
                                 const void *user_start, void *v, double *partials,

@@ -558,7 +558,7 @@ static cudaError_t launch_rows_r(const HamDev &H, const RowArgs &a, const Launch
 
 cudaError_t launch_rows(const HamDev &H, int dtype, const RowArgs &a, const LaunchCfg &cfg, cudaStream_t st)
 {
-    if (cfg.fast) return launch_rows_fast(H, dtype, a, cfg.num_sms, cfg.fast_variant, st);
+    if (cfg.fast) return launch_rows_fast(H, dtype, a, cfg.num_sms, cfg.fast_shape, st);
     return dtype == EDK_F64 ? launch_rows_r<double>(H, a, cfg, st) : launch_rows_r<float>(H, a, cfg, st);
 }
 

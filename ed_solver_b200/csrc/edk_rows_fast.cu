@@ -1,311 +1,81 @@
-// Fast row kernel for the common sector shape: impurity of at most 2 sites
-// without Hund spin-flip/pair-hop terms, even dim_up (16-byte aligned column
-// pairs), table widths of at most 16, fewer than 2^31 elements.  Same
-// mathematics and, in FP64, the same per-element order of additions as the
-// generic row kernel (edk_kernels.cu); what differs is instruction economy:
-//   * each thread owns two adjacent columns (8- or 16-byte loads and stores);
-//   * the down-spin neighbour rows of the R staged rows (offsets and values)
-//     sit in registers for the whole group, padded to KM entries of value 0;
-//   * all table entries and neighbour elements of a column pair are loaded
-//     before the ordered accumulation;
-//   * x is read with an L2 evict_last policy, the streamed vectors and all
-//     outputs with evict_first, so the neighbour rows stay resident longer;
-//   * coefficients and accumulators are FP64 for both vector types (hmadd):
-//     FP32 vectors are widened and fused into FP64 accumulators; FP64 keeps
-//     separate multiply and add so the result stays bit-identical to a
-//     sequential HAIMupdo_multr.
-#include "edk_device.cuh"
+// Fast row kernel: FP32 instances, launch-shape enumeration and dispatch.
+// The kernel itself is in edk_rows_fast.cuh.
+#include "edk_rows_fast.cuh"
 
 namespace edk {
 
-template <typename T> struct V2;
-template <> struct V2<float> { using t = float2; };
-template <> struct V2<double> { using t = double2; };
+namespace {
 
-// The R staged rows are interleaved element by element in shared memory
-// (xs[j*R + r]), so the R values a gather needs at target j are one aligned
-// vector load; RowVec<T,R> is that vector.
-template <typename T, int R> struct alignas(sizeof(T) * R <= 16 ? sizeof(T) * R : 16) RowVec { T v[R]; };
-
-template <typename T, int R>
-__device__ __forceinline__ RowVec<T, R> lds_rows(const T *xs, uint32_t j)
+// Rows per group allowed for (element bytes, down-table bound): the R*KMD
+// neighbour pairs and the up-table entries stay in registers.
+int rows_allowed(int eb, int kmd, int *out)
 {
-    return *reinterpret_cast<const RowVec<T, R> *>(xs + (size_t)j * R);
+    if (eb == 4) {
+        if (kmd == 4) { out[0] = 4; out[1] = 2; out[2] = 1; return 3; }
+        if (kmd == 8 || kmd == 12) { out[0] = 2; out[1] = 1; return 2; }
+        out[0] = 1;
+        return 1;
+    }
+    if (kmd == 4) { out[0] = 2; out[1] = 1; return 2; }
+    out[0] = 1;
+    return 1;
 }
 
-// T: element type; R: staged rows per group; KM: padded table width.  Each
-// thread owns two adjacent columns; one block of up to 512 threads per SM.
-template <typename T, int R, int KM>
-__global__ void __launch_bounds__(512, 1) row_fast_kernel(const HamDev H, const RowArgs a)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double pal_s[256];
-    __shared__ int s_ioff[17];
-    __shared__ double s_icoef[96];
-    __shared__ int s_nofs[R][KM];
-    __shared__ double s_hd[R][KM];
-    T *xs = reinterpret_cast<T *>(smem_raw);
-    const int dup = (int)H.dup;
-    const int64_t ddn = H.ddn;
-    const T *__restrict__ x = static_cast<const T *>(a.x);
-
-    // step scalars: s = w_k - gamma_k v_k was stored by the previous launch;
-    // delta_k = alpha_k - gamma_k; the new vector is s' = w_{k+1} - gamma_{k+1} v_{k+1}
-    // with gamma_{k+1} = alpha_k
-    double delta = 0.0, gam = 0.0, gam1 = a.gamma1, beta_k = 0.0, beta_k1 = 0.0, inv_b = 0.0, cpsi = 0.0;
-    if (a.mode == kModeStep) {
-        beta_k1 = a.tri_sub[a.k];
-        // the chain already ended (breakdown recorded by an earlier launch)
-        if (!(beta_k1 >= a.cutoff) || a.flags[0] != 0) return;
-        const double alpha = a.tri_diag[a.k - 1];
-        gam = a.k >= 2 ? a.tri_diag[a.k - 2] : a.gamma1;
-        delta = alpha - gam;
-        gam1 = alpha;
-        beta_k = a.k >= 2 ? a.tri_sub[a.k - 1] : 0.0;
-        inv_b = 1.0 / beta_k1;
-        if (a.psi_coef) cpsi = a.psi_coef[a.k];
-    }
-    {
-        for (int i = threadIdx.x; i < H.up.npal; i += blockDim.x) pal_s[i] = H.up.pal[i];
-        const int nio = H.ncfg * H.ncfg + 1;
-        for (int i = threadIdx.x; i < nio; i += blockDim.x) s_ioff[i] = H.int_off[i];
-        const int ncoef = H.int_off[nio - 1];
-        for (int i = threadIdx.x; i < ncoef; i += blockDim.x) s_icoef[i] = H.int_coef[i];
-    }
-    const uint64_t keep = l2_keep(), stream = l2_stream();
-    const uint32_t *__restrict__ ell = H.up.ell;
-    const int K = H.up.ell_k;
-    const double *__restrict__ dnv = H.dn.val;
-    const double *__restrict__ upd = H.up.diag;
-    const double *__restrict__ dnd = H.dn.diag;
-    const int ncfg = H.ncfg;
-
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-    const int64_t ngroups = (ddn + R - 1) / R;
-    for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
-        int row[R], cd[R];
-        double dd[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const int64_t q = g * R + r;
-            row[r] = q < ddn ? H.row_order[q] : -1;
-            const int rr = row[r] >= 0 ? row[r] : 0;
-            dd[r] = dnd[rr];
-            cd[r] = (int)H.dn.imp[rr];
-        }
-        __syncthreads();
-        // neighbour rows (offsets, values) of the group, padded with value 0 on the own row
-        for (int t = threadIdx.x; t < R * KM; t += blockDim.x) {
-            const int r = t / KM, f = t % KM;
-            const int64_t q = g * R + r;
-            const int rr = q < ddn ? H.row_order[q] : 0;
-            const int f0 = H.dn.ptr[rr], nd = H.dn.ptr[rr + 1] - f0;
-            const bool ok = f < nd;
-            s_nofs[r][f] = (ok ? H.dn.tgt[f0 + f] : rr) * dup;
-            s_hd[r][f] = ok ? dnv[f0 + f] : 0.0;
-        }
-        // stage the R rows interleaved: xs[c*R + r]
-        {
-            constexpr int V = 16 / sizeof(T);
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const T *src = x + (int64_t)(row[r] >= 0 ? row[r] : 0) * dup;
-                const uintptr_t addr = reinterpret_cast<uintptr_t>(src);
-                int head = (int)(((16u - (addr & 15u)) & 15u) / sizeof(T));
-                if (head > dup) head = dup;
-                for (int i = threadIdx.x; i < head; i += blockDim.x) xs[i * R + r] = __ldg(src + i);
-                const int nv = (dup - head) / V;
-                const int4 *sv = reinterpret_cast<const int4 *>(src + head);
-                for (int i = threadIdx.x; i < nv; i += blockDim.x) {
-                    const int4 q = __ldg(sv + i);
-                    T tmp[V];
-                    memcpy(tmp, &q, 16);
-#pragma unroll
-                    for (int v = 0; v < V; ++v) xs[(head + i * V + v) * R + r] = tmp[v];
-                }
-                for (int i = head + nv * V + threadIdx.x; i < dup; i += blockDim.x) xs[i * R + r] = __ldg(src + i);
-            }
-        }
-        __syncthreads();
-
-        for (int c = 2 * threadIdx.x; c < dup; c += 2 * blockDim.x) {
-            // ---- loads ----
-            uint2 ent[KM];
-#pragma unroll
-            for (int k = 0; k < KM; ++k)
-                ent[k] = k < K ? ldu2(ell + (size_t)k * dup + c) : make_uint2((uint32_t)c, (uint32_t)(c + 1));
-            typename V2<T>::t xd[R][KM];
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-#pragma unroll
-                for (int f = 0; f < KM; ++f) xd[r][f] = ld2(x + s_nofs[r][f] + c, keep);
-            // bring the next iteration's neighbour elements towards L2 while this one computes
-            if (c + 2 * (int)blockDim.x < dup) {
-#pragma unroll
-                for (int r = 0; r < R; ++r)
-#pragma unroll
-                    for (int f = 0; f < KM; ++f) prefetch_l2(x + s_nofs[r][f] + c + 2 * blockDim.x);
-            }
-            const int cu0 = H.up.imp[c], cu1 = H.up.imp[c + 1];
-            const double du0 = upd[c], du1 = upd[c + 1];
-            const RowVec<T, R> o0 = lds_rows<T, R>(xs, c), o1 = lds_rows<T, R>(xs, c + 1);
-            double acc[R][2];
-            // ---- ordered accumulation: density terms, diagonal ----
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                double a0 = 0.0, a1 = 0.0;
-                const int g0 = cu0 * ncfg + cd[r], g1 = cu1 * ncfg + cd[r];
-                for (int o2 = s_ioff[g0]; o2 < s_ioff[g0 + 1]; ++o2) a0 = hmadd<T>(a0, s_icoef[o2], o0.v[r]);
-                for (int o2 = s_ioff[g1]; o2 < s_ioff[g1 + 1]; ++o2) a1 = hmadd<T>(a1, s_icoef[o2], o1.v[r]);
-                acc[r][0] = hmadd<T>(a0, fadd(du0, dd[r]), o0.v[r]);
-                acc[r][1] = hmadd<T>(a1, fadd(du1, dd[r]), o1.v[r]);
-            }
-            // ---- up-spin hops: one vector load serves the R rows ----
-#pragma unroll
-            for (int k = 0; k < KM; ++k) {
-                if (k >= K) break;
-                const RowVec<T, R> g0 = lds_rows<T, R>(xs, ent[k].x & 0xFFFFFFu);
-                const RowVec<T, R> g1 = lds_rows<T, R>(xs, ent[k].y & 0xFFFFFFu);
-                const double h0 = pal_s[ent[k].x >> 24], h1 = pal_s[ent[k].y >> 24];
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    acc[r][0] = hmadd<T>(acc[r][0], h0, g0.v[r]);
-                    acc[r][1] = hmadd<T>(acc[r][1], h1, g1.v[r]);
-                }
-            }
-            // ---- down-spin hops ----
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-#pragma unroll
-                for (int f = 0; f < KM; ++f) {
-                    const double h = s_hd[r][f];
-                    acc[r][0] = hmadd<T>(acc[r][0], h, xd[r][f].x);
-                    acc[r][1] = hmadd<T>(acc[r][1], h, xd[r][f].y);
-                }
-            // ---- epilogue ----
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                if (row[r] < 0) continue;
-                const size_t i = (size_t)row[r] * dup + c;
-                T *y = static_cast<T *>(a.y) + i;
-                const T xo[2] = {o0.v[r], o1.v[r]};
-                if (a.mode == kModeHv) {
-                    st2(y, (T)acc[r][0], (T)acc[r][1], stream);
-                } else if (a.mode == kModeFirst) {
-                    T st[2];
-#pragma unroll
-                    for (int e = 0; e < 2; ++e) {
-                        const double v = (double)xo[e];
-                        st[e] = (T)((double)acc[r][e] - gam1 * v);
-                        const double sd = (double)st[e];
-                        s0 += sd * sd; s1 += sd * v; s2 += v * v;
-                    }
-                    st2(y, st[0], st[1], stream);
-                } else if (a.mode == kModeStep) {
-                    const auto vk2 = ld2(static_cast<const T *>(a.vk) + i, stream);
-                    typename V2<T>::t vm2;
-                    if (a.vkm1) vm2 = ld2(static_cast<const T *>(a.vkm1) + i, stream);
-                    else { vm2.x = T(0); vm2.y = T(0); }
-                    const double vk[2] = {(double)vk2.x, (double)vk2.y}, vm[2] = {(double)vm2.x, (double)vm2.y};
-                    T wt[2], vt[2];
-#pragma unroll
-                    for (int e = 0; e < 2; ++e) {
-                        const double sv = (double)xo[e];
-                        vt[e] = (T)((sv - delta * vk[e]) * inv_b);
-                        const double hv1 = ((double)acc[r][e] - delta * (sv + gam * vk[e] + beta_k * vm[e])) * inv_b;
-                        const double w = hv1 - beta_k1 * vk[e];
-                        wt[e] = (T)(w - gam1 * (double)vt[e]);
-                        const double wd = (double)wt[e], vd = (double)vt[e];
-                        s0 += wd * wd; s1 += wd * vd; s2 += vd * vd;
-                    }
-                    st2(y, wt[0], wt[1], stream);
-                    st2(static_cast<T *>(a.vout) + i, vt[0], vt[1], stream);
-                    if (a.psi) {
-                        T *p = static_cast<T *>(a.psi) + i;
-                        const auto pv = ld2(p, stream);
-                        st2(p, (T)((double)pv.x + cpsi * (double)vt[0]), (T)((double)pv.y + cpsi * (double)vt[1]),
-                            stream);
-                    }
-                } else {
-#pragma unroll
-                    for (int e = 0; e < 2; ++e) {
-                        const double rr = (double)acc[r][e] - a.eshift * (double)xo[e];
-                        s0 += rr * rr; s2 += (double)xo[e] * (double)xo[e];
-                    }
-                }
-            }
-        }
-    }
-    if (a.mode == kModeHv) return;
-    double v[4] = {s0, s1, s2, 0.0};
-    if (grid_sum<4>(v, a.partials, a.counter, a.sums_out))
-        if (a.mode == kModeFirst || a.mode == kModeStep) lanczos_finalize(a);
-}
-
-// ---------------------------------------------------------------------------
+}  // namespace
 
 bool fast_rows_ok(const HamDev &H, int elem_bytes)
 {
     const int kmax = H.up.ell_k > H.dn_kmax ? H.up.ell_k : H.dn_kmax;
     const int64_t rowbytes = H.dup * (int64_t)elem_bytes;
     return !H.hund && H.nc <= 2 && (H.dup % 2) == 0 && kmax <= 16 && rowbytes <= kMaxSmemBytes &&
-           H.up.packed &&
-           H.dup * H.ddn < (int64_t)1 << 31 && H.up.ell_k >= 0;
+           H.up.packed && H.dup * H.ddn < (int64_t)1 << 31 && H.up.ell_k >= 0;
 }
 
-template <typename T, int R, int KM>
-static cudaError_t launch_fast_k(const HamDev &H, const RowArgs &a, int num_sms, size_t smem, cudaStream_t st)
+int fast_shapes(const HamDev &H, int elem_bytes, int num_sms, FastShape *out, int cap)
 {
-    auto k = row_fast_kernel<T, R, KM>;
-    if (smem > 0) {
-        // static + dynamic shared memory may exceed the 48 KB default
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
+    if (!fast_rows_ok(H, elem_bytes)) return 0;
+    const int kmu = H.up.ell_k <= 8 ? 8 : 16;
+    const int kmd = H.dn_kmax <= 4 ? 4 : H.dn_kmax <= 8 ? 8 : H.dn_kmax <= 12 ? 12 : 16;
+    const int64_t rowbytes = H.dup * (int64_t)elem_bytes;
+    int rs[3];
+    const int nr = rows_allowed(elem_bytes, kmd, rs);
+    int n = 0;
+    for (int variant = 0; variant < 2; ++variant) {
+        const int64_t smem_cap = variant == 0 ? kMaxSmemBytes : kMaxSmemBytes / 2;
+        for (int i = 0; i < nr && n < cap; ++i) {
+            const int r = rs[i];
+            if ((int64_t)r * rowbytes > smem_cap) continue;
+            // keep every SM busy: no multi-row groups when there are too few rows
+            if (r > 1 && (H.ddn + r - 1) / r < num_sms) continue;
+            out[n++] = FastShape{r, kmu, kmd, variant};
+        }
     }
-    const int cols = (int)((H.dup + 1) / 2);
-    int block = 512;
-    if (cols < block) block = ((cols + 31) / 32) * 32;
-    if (block < 32) block = 32;
-    int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block, smem);
-    if (e != cudaSuccess) return e;
-    if (per_sm < 1) per_sm = 1;
-    const int64_t groups = (H.ddn + R - 1) / R;
-    int64_t grid = (int64_t)num_sms * per_sm;
-    if (grid > groups) grid = groups;
-    if (grid < 1) grid = 1;
-    k<<<(int)grid, block, smem, st>>>(H, a);
-    return cudaGetLastError();
+    return n;
 }
 
-cudaError_t launch_rows_fast(const HamDev &H, int dtype, const RowArgs &a, int num_sms, int want_variant,
+cudaError_t launch_rows_fast(const HamDev &H, int dtype, const RowArgs &a, int num_sms, const FastShape &s,
                              cudaStream_t st)
 {
-    (void)want_variant;
-    const int eb = dtype == EDK_F64 ? 8 : 4;
-    const int kmax = H.up.ell_k > H.dn_kmax ? H.up.ell_k : H.dn_kmax;
-    const int KM = kmax <= 4 ? 4 : kmax <= 8 ? 8 : 16;
-    const int64_t rowbytes = H.dup * (int64_t)eb;
-    // rows per group: shared memory, and registers for R*KM neighbour pairs
-    int R = (int)(kMaxSmemBytes / rowbytes);
-    const int rreg = eb == 4 ? (KM == 4 ? 4 : KM == 8 ? 2 : 1) : (KM == 4 ? 2 : 1);
-    if (R > rreg) R = rreg;
-    R = R >= 4 ? 4 : R >= 2 ? 2 : 1;
-    while (R > 1 && (H.ddn + R - 1) / R < num_sms) R >>= 1;
-    const size_t smem = (size_t)R * (size_t)rowbytes;
-#define EDK_FAST(TT, KK)                                                       \
-    if (R == 4) return launch_fast_k<TT, 4, KK>(H, a, num_sms, smem, st);       \
-    if (R == 2) return launch_fast_k<TT, 2, KK>(H, a, num_sms, smem, st);       \
-    return launch_fast_k<TT, 1, KK>(H, a, num_sms, smem, st);
-    if (eb == 8) {
-        if (KM == 4) { EDK_FAST(double, 4) }
-        if (KM == 8) { EDK_FAST(double, 8) }
-        EDK_FAST(double, 16)
-    }
-    if (KM == 4) { EDK_FAST(float, 4) }
-    if (KM == 8) { EDK_FAST(float, 8) }
-    EDK_FAST(float, 16)
-#undef EDK_FAST
+    return dtype == EDK_F64 ? launch_fast_f64(H, a, num_sms, s, st) : launch_fast_f32(H, a, num_sms, s, st);
+}
+
+#define EDK_FAST_V(T, R, KMU, KMD)                                                                \
+    if (s.r == R && s.kmu == KMU && s.kmd == KMD)                                                 \
+        return s.variant == 0 ? launch_fast_t<T, R, KMU, KMD, 512, 1>(H, a, num_sms, st)          \
+                              : launch_fast_t<T, R, KMU, KMD, 256, 2>(H, a, num_sms, st);
+#define EDK_FAST_KMU(T, R, KMD) EDK_FAST_V(T, R, 8, KMD) EDK_FAST_V(T, R, 16, KMD)
+
+cudaError_t launch_fast_f32(const HamDev &H, const RowArgs &a, int num_sms, const FastShape &s, cudaStream_t st)
+{
+    EDK_FAST_KMU(float, 4, 4)
+    EDK_FAST_KMU(float, 2, 4)
+    EDK_FAST_KMU(float, 1, 4)
+    EDK_FAST_KMU(float, 2, 8)
+    EDK_FAST_KMU(float, 1, 8)
+    EDK_FAST_KMU(float, 2, 12)
+    EDK_FAST_KMU(float, 1, 12)
+    EDK_FAST_KMU(float, 1, 16)
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace edk

@@ -76,9 +76,11 @@ int64_t edk_ctx_launch_count(const edk_ctx *ctx);
  * FP32), the number of launches and their summed device time in ms. */
 int edk_ctx_timing(edk_ctx *ctx, int enable);
 /* Row-kernel selection: 0 = the fastest kernel whose preconditions hold
- * (default), 1 = always the generic kernel (for A/B checks), 2/3 = the fast
- * kernel with launch shape 0 (two columns per thread, one block per SM) or 1
- * (one column per thread, two blocks per SM) when its preconditions hold. */
+ * (default; the fast kernel's launch shape is timed once per sector and
+ * element type), 1 = always the generic kernel (for A/B checks), 2 or 3 = the
+ * fast kernel where its preconditions hold with its default launch shape,
+ * 16+i (i < 8) = the fast kernel with its i-th feasible launch shape (modulo
+ * their number), for measurements. */
 int edk_ctx_set_kernel_path(edk_ctx *ctx, int path);
 int edk_ctx_timing_report(edk_ctx *ctx, int which, int64_t *launches, double *total_ms);
 /* Sum over the timed launches of class `which` of the sector dimension each

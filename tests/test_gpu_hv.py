@@ -24,7 +24,7 @@ def _models():
 SECTORS = [(3, 3), (2, 4), (4, 1), (0, 3), (5, 5), (1, 0)]
 
 
-@pytest.fixture(params=[0, 1], ids=["auto-kernel", "generic-kernel"])
+@pytest.fixture(params=[0, 1, 2], ids=["auto-kernel", "generic-kernel", "fast-kernel"])
 def kpath(request, ctx):
     ctx.set_kernel_path(request.param)
     yield request.param
@@ -57,7 +57,8 @@ def test_hmult_fp32(ctx, kpath, mi):
         x = rng.normal(size=h.dim)
         y = h.hmult(torch.tensor(x, dtype=torch.float32, device="cuda")).double().cpu().numpy()
         y_ref = O.OracleH(m, nu, nd).hmult(x.astype(np.float32).astype(np.float64))
-        assert np.abs(y - y_ref).max() <= 2e-6 * np.abs(y_ref).max()
+        # FP64 arithmetic on FP32-stored vectors: only the output rounding remains
+        assert np.abs(y - y_ref).max() <= 1.2e-7 * np.abs(y_ref).max()
 
 
 def test_hmult_large_rows_c3_sector_bit_exact(ctx, kpath):
@@ -130,4 +131,4 @@ def test_hmult_fp32_large_sectors(ctx, kpath, name, sec):
     x = np.random.default_rng(9).normal(size=h.dim)
     y = h.hmult(torch.tensor(x, dtype=torch.float32, device="cuda")).double().cpu().numpy()
     y_ref = O.OracleH(m, *sec).hmult(x.astype(np.float32).astype(np.float64))
-    assert np.abs(y - y_ref).max() <= 2e-6 * np.abs(y_ref).max()
+    assert np.abs(y - y_ref).max() <= 1.2e-7 * np.abs(y_ref).max()

@@ -151,3 +151,34 @@ def test_reference_golden_through_the_device(ctx):
     G = solver.green_impurity(hc, gs, 50.0, len(g), 400, pairs=[(0, 0), (1, 1)])
     assert np.abs(G[(0, 0)] - (g[:, 1] + 1j * g[:, 2])).max() < 2e-8
     assert np.abs(G[(1, 1)] - (g[:, 3] + 1j * g[:, 4])).max() < 2e-8
+
+
+def test_pipelined_kernel_krylov_ns14_against_oracle(ctx):
+    """The ns=14 (7,7) sector (1.18e7 states) runs on the pipelined row kernel:
+    Lanczos coefficients, the pass-2 vector (accumulated inside the fused step),
+    the c+ map and a Green chain in FP64 against the oracle (1e-9); the FP32
+    chain against the FP64 one (1e-5)."""
+    import torch
+    w = workload("c3")
+    m = w.model
+    nst = 40
+    h = edk.Hamiltonian(ctx, m, 7, 7)
+    ho = O.OracleH(m, 7, 7)
+    r = h.lanczos_e0(nitermax=nst, tolerance=0.0, check_every=nst)
+    ro = O.lanczos_e0(ho, nitermax=nst, tolerance=0.0)
+    n = min(r["niter"], ro["niter"])
+    assert n >= nst - 1
+    assert np.allclose(r["diag"][:n], ro["diag"][:n], rtol=1e-9, atol=1e-10)
+    assert np.allclose(r["subdiag"][1:n], ro["subdiag"][1:n], rtol=1e-9, atol=1e-10)
+    psi = h.lanczos_gs(r["vecp"][0])
+    psio = O.lanczos_gs(ho, r["vecp"][0])
+    assert np.abs(psi.cpu().numpy() - psio).max() < 1e-8
+    e0 = r["E"][0]
+    phi, ts = h.apply_c(psi, 0, 0, True)
+    wn = matsubara(w.beta, 128)
+    ht = edk.Hamiltonian(ctx, m, *ts)
+    G, _, _, _ = ht.green_chain(phi, nst, e0, 1, wn)
+    Go, _, _ = O.green_chain(O.OracleH(m, *ts), phi.cpu().numpy(), nst, e0, 1, wn)
+    assert np.abs(G - Go).max() < 1e-9
+    G32, _, _, _ = ht.green_chain(phi.to(torch.float32), nst, e0, 1, wn)
+    assert np.abs(G32 - G).max() < 1e-5
