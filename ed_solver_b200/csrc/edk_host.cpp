@@ -600,6 +600,30 @@ cudaStream_t edk_internal_stream(edk_ctx *ctx) { return ctx->stream; }
 
 int edk_internal_fail(edk_ctx *ctx, int code, const char *msg) { return ctx->fail(code, "%s", msg); }
 
+edk_ctx *edk_internal_h_ctx(edk_h *h) { return h->ctx; }
+
+void edk_internal_h_info(const edk_h *h, int *nc, int *nb, int *nup, int *ndn)
+{
+    *nc = h->model.nc;
+    *nb = h->model.nb;
+    *nup = h->nup;
+    *ndn = h->ndn;
+}
+
+void edk_internal_add_launches(edk_ctx *ctx, int64_t n) { ctx->launches += n; }
+
+// A Hamiltonian of another (nup, ndn) sector of the same model.
+int edk_internal_h_sibling(edk_h *h, int nup, int ndn, edk_h **out)
+{
+    const ModelHost &mh = h->model;
+    edk_model m{mh.nc, mh.nb, mh.ec.data(), mh.eb.data(), mh.vbc.data(), mh.u.data(), mh.jj.data(),
+                mh.jhund, mh.cutoff};
+    return edk_h_create(h->ctx, &m, nup, ndn, out);
+}
+
+// The basis states of one spin species of the sector (increasing order).
+const uint64_t *edk_internal_h_states(const edk_h *h, int spin) { return h->tab[spin].states.data(); }
+
 int edk_ctx_set_kernel_path(edk_ctx *ctx, int path)
 {
     if (!ctx || path < 0 || (path > 3 && path < 16) || path > 23) return EDK_ERR_INVALID;

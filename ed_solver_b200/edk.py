@@ -82,6 +82,63 @@ class _BatchStats(C.Structure):
                 ("rows", C.c_int32), ("blocks_per_sm", C.c_int32), ("tuned_shapes", C.c_int32)]
 
 
+class _Param(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("i", C.c_int32), ("j", C.c_int32), ("spin", C.c_int32)]
+
+
+class _GreenSpec(C.Structure):
+    _fields_ = [("site", C.c_int32), ("spin", C.c_int32), ("dagger", C.c_int32), ("site2", C.c_int32),
+                ("sign2", C.c_int32)]
+
+
+class _GradStats(C.Structure):
+    _fields_ = [("forward_steps", C.c_int64), ("replay_steps", C.c_int64), ("reverse_steps", C.c_int64),
+                ("cg_iterations", C.c_int32), ("cg_residual", C.c_double), ("stored_vectors", C.c_int32)]
+
+
+PARAM_EC, PARAM_EB, PARAM_VBC, PARAM_U = 0, 1, 2, 3
+
+
+def star_params(model: AIMModel, spin: int = 2):
+    """The parameters of a star model: every bath level Eb(k,k), every nonzero
+    hybridisation Vbc(k,c), the impurity levels Ec(c,c) and the on-site U(c,c);
+    spin-symmetric (spin=2) by default.  List of (kind, i, j, spin)."""
+    p = [(PARAM_EB, k, k, spin) for k in range(model.nb)]
+    p += [(PARAM_VBC, k, c, spin) for k in range(model.nb) for c in range(model.nc)
+          if np.any(model.vbc[:, k, c] != 0)]
+    p += [(PARAM_EC, c, c, spin) for c in range(model.nc)]
+    p += [(PARAM_U, c, c, 0) for c in range(model.nc)]
+    return p
+
+
+def perturb(model: AIMModel, param, h: float) -> AIMModel:
+    """A copy of the model with one parameter (kind, i, j, spin) moved by h;
+    symmetric pairs (i, j), (j, i) move together, as the derivative operators
+    assume."""
+    import dataclasses
+    kind, i, j, spin = param
+    m = dataclasses.replace(model, ec=model.ec.copy(), eb=model.eb.copy(), vbc=model.vbc.copy(), u=model.u.copy())
+    spins = (0, 1) if spin == 2 else (spin,)
+    if kind == PARAM_U:
+        m.u[i, j] += h
+        if i != j:
+            m.u[j, i] += h
+        return m
+    arr = {PARAM_EC: m.ec, PARAM_EB: m.eb, PARAM_VBC: m.vbc}[kind]
+    for s in spins:
+        arr[s, i, j] += h
+        if kind != PARAM_VBC and i != j:
+            arr[s, j, i] += h
+    return m
+
+
+def _params_arr(params):
+    arr = (_Param * len(params))()
+    for q, (k, i, j, s) in enumerate(params):
+        arr[q] = _Param(int(k), int(i), int(j), int(s))
+    return arr
+
+
 _LIB = None
 
 
@@ -127,6 +184,9 @@ def lib():
         "edk_convert": (C.c_int, [P, C.c_int, C.c_int, I64, P, P]),
         "edk_solve": (C.c_int, [P, P, P, P]),
         "edk_green_batch": (C.c_int, [P, C.c_int, I32, P, I32, I32, P, D, I32, P, I32, P]),
+        "edk_dh_bilinear": (C.c_int, [P, P, P, I32, P, P]),
+        "edk_grad_e0": (C.c_int, [P, P, I32, P, P]),
+        "edk_grad_green": (C.c_int, [P, P, D, I32, P, I32, I32, P, P, D, I32, P, D, P, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -404,6 +464,52 @@ class Hamiltonian:
         self.ctx.check(lib().edk_apply_c(self.h, _dtype_code(vec.dtype), site, spin, int(bool(dagger)),
                                          site2, sign2, _ptr(vec), _ptr(out), C.byref(od)), "edk_apply_c")
         return out, (tnup, tndn)
+
+    # ---- parameter gradients -----------------------------------------------
+    def dh_bilinear(self, a, b, params):
+        """<a| dH/dtheta_q |b> for every parameter (FP64 device vectors)."""
+        arr = _params_arr(params)
+        out = np.zeros(len(params))
+        self.ctx.check(lib().edk_dh_bilinear(self.h, _ptr(a.contiguous()), _ptr(b.contiguous()), len(params),
+                                             C.cast(arr, C.c_void_p), out.ctypes.data), "edk_dh_bilinear")
+        return out
+
+    def grad_e0(self, psi, params):
+        """Hellmann-Feynman dE/dtheta_q of the state psi (FP64 device vector)."""
+        arr = _params_arr(params)
+        out = np.zeros(len(params))
+        self.ctx.check(lib().edk_grad_e0(self.h, _ptr(psi.contiguous()), len(params), C.cast(arr, C.c_void_p),
+                                         out.ctypes.data), "edk_grad_e0")
+        return out
+
+    def grad_green(self, psi, e0, chains, nitergreen, wn, gbar, params, e0bar=0.0, cg_tol=1e-10):
+        """VJP of the Green functions of the eigenstate psi (and of E0).
+
+        chains: list of (site, spin, dagger) or (site, spin, dagger, site2, sign2);
+        gbar: complex array (nchain, nw) of dL/dRe G + i dL/dIm G.
+        Returns (grad (np,), G (nchain, nw) complex, stats dict)."""
+        wn = np.ascontiguousarray(wn, np.float64)
+        nch = len(chains)
+        spec = (_GreenSpec * max(nch, 1))()
+        for c, ch in enumerate(chains):
+            site, spin, dag = ch[:3]
+            site2, sign2 = (ch[3], ch[4]) if len(ch) > 3 else (-1, 1)
+            spec[c] = _GreenSpec(int(site), int(spin), int(bool(dag)), int(site2), int(sign2))
+        gb = np.zeros((max(nch, 1), len(wn), 2))
+        if nch:
+            g = np.asarray(gbar, np.complex128).reshape(nch, len(wn))
+            gb[:nch, :, 0] = g.real
+            gb[:nch, :, 1] = g.imag
+        G = np.zeros((max(nch, 1), len(wn), 2))
+        arr = _params_arr(params)
+        out = np.zeros(len(params))
+        st = _GradStats()
+        self.ctx.check(lib().edk_grad_green(self.h, _ptr(psi.contiguous()), float(e0), nch, C.cast(spec, C.c_void_p),
+                                            int(nitergreen), len(wn), wn.ctypes.data, gb.ctypes.data, float(e0bar),
+                                            len(params), C.cast(arr, C.c_void_p), float(cg_tol), out.ctypes.data,
+                                            G.ctypes.data, C.byref(st)), "edk_grad_green")
+        stats = {f: getattr(st, f) for f, _ in _GradStats._fields_}
+        return out, (G[:nch, :, 0] + 1j * G[:nch, :, 1]), stats
 
     # ---- dynamic correlation ----------------------------------------------
     def green_chain(self, start, nitergreen, e0, iph, wn, cutoff_dynamic=1e-8):

@@ -251,6 +251,60 @@ int edk_green_batch(edk_ctx *ctx, int dtype, int32_t nchain, const edk_chain *ch
 /* Element-type conversion of a device vector (FP32 <-> FP64, or a copy). */
 int edk_convert(edk_ctx *ctx, int from_dtype, int to_dtype, int64_t n, const void *in_dev, void *out_dev);
 
+/* ---- adjoint: parameter gradients ------------------------------------------
+ * The reference has no derivatives; these entry points differentiate its
+ * quantities with respect to the model parameters of edk_model.  H is linear
+ * in every parameter, so dH/dtheta is a fixed operator:
+ *   EDK_PARAM_EC  (i,j): Ec(i,j) and Ec(j,i) together -- n_c (i=j) or the
+ *                 impurity hop c+_i c_j + c+_j c_i (HAIM_offdiag_arrays.f90:419-464)
+ *   EDK_PARAM_EB  (i,j): the same for Eb (bath levels and bath-bath hops, :469-486)
+ *   EDK_PARAM_VBC (k,c): Vbc(k,c), both hop directions bath k <-> impurity c (:497-524)
+ *   EDK_PARAM_U   (i,j): U(i,i): n_i,up n_i,dn; U(i,j), i<j: n_i n_j (HAIMupdo.f90:784-829)
+ * spin: 0 = the up-spin entry only, 1 = down only, 2 = both spins' entries
+ * (a spin-symmetric parameter); ignored for EDK_PARAM_U.  At most 64
+ * parameters per call.  All vectors are FP64 device vectors of h's sector. */
+#define EDK_PARAM_EC   0
+#define EDK_PARAM_EB   1
+#define EDK_PARAM_VBC  2
+#define EDK_PARAM_U    3
+typedef struct edk_param {
+    int32_t kind, i, j, spin;
+} edk_param;
+
+/* out_host[q] = <a| dH/dtheta_q |b> for every parameter, one pass. */
+int edk_dh_bilinear(edk_h *h, const void *a_dev, const void *b_dev, int32_t np, const edk_param *params,
+                    double *out_host);
+/* Hellmann-Feynman: dE/dtheta_q = <psi| dH/dtheta_q |psi> / <psi|psi>. */
+int edk_grad_e0(edk_h *h, const void *psi_dev, int32_t np, const edk_param *params, double *grad_host);
+
+/* One Green-function channel of an eigenstate: the compute_dynamic chain of
+ * (c[+]_{site,spin} + sign2 c[+]_{site2,spin})|psi> (site2 < 0: single
+ * operator), dagger = 1 particle part (iph = 1), 0 hole part (iph = 2). */
+typedef struct edk_green_spec {
+    int32_t site, spin, dagger, site2, sign2;
+} edk_green_spec;
+typedef struct edk_grad_stats {
+    int64_t forward_steps, replay_steps, reverse_steps;
+    int32_t cg_iterations;
+    double cg_residual;
+    int32_t stored_vectors;      /* FP64 vectors of the largest chain's checkpoints + segment */
+} edk_grad_stats;
+/* Vector-Jacobian product of the Green functions G_c(i wn) (the dyn of
+ * edk_green_chain, nitergreen steps from |psi> normalised) and of E0 for the
+ * eigenstate psi (FP64, energy e0) of h's sector:
+ *   grad_q = sum_c sum_w Re(conj(gbar[c][w]) dG_c(i wn_w)/dtheta_q) + e0bar dE0/dtheta_q.
+ * gbar_host: nchain x nw interleaved re/im (torch's complex-gradient
+ * convention: dL/dRe G + i dL/dIm G).  The chain part is reverse mode through
+ * the Lanczos recurrence with checkpointed replay; the eigenvector part solves
+ * (H - E0) lambda = (1 - |psi><psi|) psibar by conjugate gradients to relative
+ * residual cg_tol (psi must be a converged, non-degenerate ground state).
+ * G_host (optional, nchain x nw interleaved) receives the forward G; stats may
+ * be NULL.  Everything is FP64. */
+int edk_grad_green(edk_h *h, const void *psi_dev, double e0, int32_t nchain, const edk_green_spec *chains,
+                   int32_t nitergreen, int32_t nw, const double *wn_host, const double *gbar_host, double e0bar,
+                   int32_t np, const edk_param *params, double cg_tol, double *grad_host, double *G_host,
+                   edk_grad_stats *stats);
+
 /* ---- solver driver -------------------------------------------------------
  * One solve of the impurity problem for the (N_up, N_dn) basis: the sector
  * scan and ground states of get_eigen_energies/get_GS (solver.h:11-237), the
