@@ -314,6 +314,69 @@ def run_kernel_case(args):
     ctx.close()
 
 
+def run_grad(args):
+    """Gradients of E0 + G(i w_n) of the (8,8) ground state with respect to
+    the 32 star-model parameters (15 bath levels, 15 hybridisations, impurity
+    level, U): one edk_grad_green call (four 300-step chains, 512 frequencies,
+    FP64), timed, then central differences (h = 1e-5, FP64 solves) for the
+    first args.grad_fd parameters."""
+    import numpy as np
+    import torch
+    from ed_solver_b200 import edk
+    from ed_solver_b200.model import matsubara
+    w = WORKLOAD
+    ctx = edk.Context(0)
+    model = _model()
+    params = edk.star_params(model)
+    chains = [(0, 0, True), (0, 0, False), (0, 1, True), (0, 1, False)]
+    wn = matsubara(w["beta"], w["nw"])
+    rng = np.random.default_rng(11)
+    gbar = rng.normal(size=(4, w["nw"])) + 1j * rng.normal(size=(4, w["nw"]))
+    e0bar = 1.0
+
+    def ground(m):
+        h = edk.Hamiltonian(ctx, m, *w["sector"])
+        r = h.lanczos_e0("f64", tolerance=1e-14, residual_tol=1e-11, nitermax=w["nitermax"])
+        return h, h.lanczos_gs(r["vecp"][0]), float(r["E"][0])
+
+    def loss(m):
+        h, psi, e0 = ground(m)
+        val = e0bar * e0
+        for c, (site, spin, dag) in enumerate(chains):
+            phi, ts = h.apply_c(psi, site, spin, dag)
+            ht = edk.Hamiltonian(ctx, m, *ts)
+            G, _, _, _ = ht.green_chain(phi, w["nitergreen"], e0, 1 if dag else 2, wn, cutoff_dynamic=0.0)
+            val += float(np.sum((np.conj(gbar[c]) * G).real))
+            ht.close()
+            del phi
+        h.close()
+        return val
+
+    h, psi, e0 = ground(model)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    grad, _, st = h.grad_green(psi, e0, chains, w["nitergreen"], wn, gbar, params, e0bar=e0bar, cg_tol=1e-11)
+    torch.cuda.synchronize()
+    t_grad = time.perf_counter() - t0
+    h.close()
+    del psi
+    ctx.clear_cache()
+    nfd = min(args.grad_fd, len(params))
+    fd = []
+    for p in params[:nfd]:
+        fd.append((loss(edk.perturb(model, p, 1e-5)) - loss(edk.perturb(model, p, -1e-5))) / 2e-5)
+    fd = np.array(fd)
+    err = np.abs(grad[:nfd] - fd)
+    out = {"grad": "E0 + G(iw_n) VJP, ns=16 (8,8), 4 chains x 300 steps, 512 frequencies, FP64",
+           "n_params": len(params), "grad_s": t_grad, "stats": st,
+           "fd_checked": nfd, "fd_h": 1e-5,
+           "max_abs_err": float(err.max()) if nfd else None,
+           "max_rel_err_vs_largest": float(err.max() / np.abs(fd).max()) if nfd else None,
+           "grad": [float(g) for g in grad], "fd": [float(f) for f in fd]}
+    print(json.dumps(out), flush=True)
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -323,7 +386,13 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--kernel-case", action="store_true",
                     help="run only six FP32 Lanczos steps of the (8,8) sector (profiling case)")
+    ap.add_argument("--grad", action="store_true",
+                    help="time the 32 parameter gradients of E0 + G and check them by central differences")
+    ap.add_argument("--grad-fd", type=int, default=4, help="parameters checked by central differences (--grad)")
     args = ap.parse_args()
+    if args.grad:
+        run_grad(args)
+        return
     if args.kernel_case:
         run_kernel_case(args)
         return
