@@ -29,6 +29,24 @@ module edk_fortran
     real(c_double) :: target, residual_tol
   end type
 
+  ! parameter of the adjoint: kind EDK_PARAM_EC=0, EB=1, VBC=2, U=3 (0-based i, j);
+  ! spin 0 up, 1 down, 2 both
+  type, bind(C) :: edk_param
+    integer(c_int32_t) :: kind, i, j, spin
+  end type
+
+  ! one Green channel of an eigenstate (0-based site; site2 < 0: single operator)
+  type, bind(C) :: edk_green_spec
+    integer(c_int32_t) :: site, spin, dagger, site2, sign2
+  end type
+
+  type, bind(C) :: edk_grad_stats
+    integer(c_int64_t) :: forward_steps, replay_steps, reverse_steps
+    integer(c_int32_t) :: cg_iterations
+    real(c_double) :: cg_residual
+    integer(c_int32_t) :: stored_vectors
+  end type
+
   type, bind(C) :: edk_lanczos_result
     integer(c_int32_t) :: nkept, niter, status
     real(c_double) :: E(64)
@@ -111,6 +129,38 @@ module edk_fortran
       real(c_double), intent(in) :: wn(*)
       real(c_double), intent(out) :: G(*), diag(*), subdiag(*)
       integer(c_int32_t) :: niter_done
+    end function
+
+    ! <a| dH/dtheta_q |b> for every parameter (FP64 device vectors a, b)
+    integer(c_int) function edk_dh_bilinear(h, a, b, np, params, out) bind(C, name="edk_dh_bilinear")
+      import :: c_int, c_ptr, c_int32_t, c_double, edk_param
+      type(c_ptr), value :: h, a, b
+      integer(c_int32_t), value :: np
+      type(edk_param), intent(in) :: params(*)
+      real(c_double), intent(out) :: out(*)
+    end function
+
+    ! Hellmann-Feynman dE/dtheta_q of the state psi (FP64 device vector)
+    integer(c_int) function edk_grad_e0(h, psi, np, params, grad) bind(C, name="edk_grad_e0")
+      import :: c_int, c_ptr, c_int32_t, c_double, edk_param
+      type(c_ptr), value :: h, psi
+      integer(c_int32_t), value :: np
+      type(edk_param), intent(in) :: params(*)
+      real(c_double), intent(out) :: grad(*)
+    end function
+
+    ! vector-Jacobian product of the Green functions and of E0 of the eigenstate psi
+    integer(c_int) function edk_grad_green(h, psi, e0, nchain, chains, nitergreen, nw, wn, gbar, e0bar, &
+        np, params, cg_tol, grad, G, stats) bind(C, name="edk_grad_green")
+      import :: c_int, c_ptr, c_int32_t, c_double, edk_param, edk_green_spec, edk_grad_stats
+      type(c_ptr), value :: h, psi
+      real(c_double), value :: e0, e0bar, cg_tol
+      integer(c_int32_t), value :: nchain, nitergreen, nw, np
+      type(edk_green_spec), intent(in) :: chains(*)
+      real(c_double), intent(in) :: wn(*), gbar(*)
+      type(edk_param), intent(in) :: params(*)
+      real(c_double), intent(out) :: grad(*), G(*)
+      type(edk_grad_stats), intent(out) :: stats
     end function
   end interface
 
