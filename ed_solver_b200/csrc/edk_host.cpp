@@ -312,16 +312,16 @@ int fast_shape_for(edk_h *h, int dtype, const RowArgs &a, FastShape &out)
 {
     edk_ctx *c = h->ctx;
     const int eb = dtype == EDK_F64 ? 8 : 4;
-    FastShape cand[8];
+    FastShape cand[12];
     if (c->kernel_path >= 16) {
         // a fixed candidate, for measurements
-        const int n = fast_shapes(h->H, eb, c->num_sms, cand, 8);
+        const int n = fast_shapes(h->H, eb, c->num_sms, cand, 12);
         if (n == 0) return c->fail(EDK_ERR_INVALID, "fast row kernel: no launch shape");
         out = cand[(c->kernel_path - 16) % n];
         return EDK_OK;
     }
     if (h->fast_tuned[dtype]) { out = h->fast_shape[dtype]; return EDK_OK; }
-    const int n = fast_shapes(h->H, eb, c->num_sms, cand, 8);
+    const int n = fast_shapes(h->H, eb, c->num_sms, cand, 12);
     if (n == 0) return c->fail(EDK_ERR_INVALID, "fast row kernel: no launch shape");
     out = cand[0];
     if (c->kernel_path != 0 || n == 1 || !a.x || !a.y) {
@@ -626,7 +626,7 @@ const uint64_t *edk_internal_h_states(const edk_h *h, int spin) { return h->tab[
 
 int edk_ctx_set_kernel_path(edk_ctx *ctx, int path)
 {
-    if (!ctx || path < 0 || (path > 3 && path < 16) || path > 23) return EDK_ERR_INVALID;
+    if (!ctx || path < 0 || (path > 3 && path < 16) || path > 27) return EDK_ERR_INVALID;
     ctx->kernel_path = path;
     return EDK_OK;
 }

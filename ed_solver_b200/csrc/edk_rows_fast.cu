@@ -61,8 +61,8 @@ cudaError_t launch_rows_fast(const HamDev &H, int dtype, const RowArgs &a, int n
 
 #define EDK_FAST_V(T, R, KMU, KMD)                                                                \
     if (s.r == R && s.kmu == KMU && s.kmd == KMD)                                                 \
-        return s.variant == 0 ? launch_fast_t<T, R, KMU, KMD, 512, 1>(H, a, num_sms, st)          \
-                              : launch_fast_t<T, R, KMU, KMD, 256, 2>(H, a, num_sms, st);
+        return s.variant == 0 ? launch_fast_t<T, R, KMU, KMD, 512, 1, 2>(H, a, num_sms, st)       \
+                              : launch_fast_t<T, R, KMU, KMD, 256, 2, 2>(H, a, num_sms, st);
 #define EDK_FAST_KMU(T, R, KMD) EDK_FAST_V(T, R, 8, KMD) EDK_FAST_V(T, R, 16, KMD)
 
 cudaError_t launch_fast_f32(const HamDev &H, const RowArgs &a, int num_sms, const FastShape &s, cudaStream_t st)

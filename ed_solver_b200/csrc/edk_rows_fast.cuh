@@ -3,7 +3,8 @@
 // table widths of at most 16, fewer than 2^31 elements.  Same mathematics
 // and, in FP64, the same per-element order of additions as the generic row
 // kernel (edk_kernels.cu); what differs is instruction economy:
-//   * each thread owns two adjacent columns (8- or 16-byte loads and stores);
+//   * each thread owns CPT adjacent columns (CPT = 2: 8- or 16-byte loads and
+//     stores; CPT = 1: half the registers, so twice the resident warps);
 //   * the down-spin neighbour rows of the R staged rows (offsets and values)
 //     sit in shared memory for the whole group, padded to KMD entries of
 //     value 0 on the own row; the up-table entries are padded to KMU with the
@@ -13,9 +14,10 @@
 //   * x is read with an L2 evict_last policy, the streamed vectors and all
 //     outputs with evict_first, so the neighbour rows stay resident longer;
 //   * coefficients and accumulators are FP64 for both vector types (hmadd):
-//     FP32 vectors are widened and fused into FP64 accumulators; FP64 keeps
-//     separate multiply and add so the result stays bit-identical to a
-//     sequential HAIMupdo_multr.
+//     FP32 vectors are widened and fused into FP64 accumulators, with the
+//     down-spin hops in a second accumulator (two independent FMA chains);
+//     FP64 keeps one chain with separate multiply and add so the result stays
+//     bit-identical to a sequential HAIMupdo_multr.
 // The launch shape (threads per block and blocks per SM, rows per group) is
 // a template choice; the host times the feasible shapes once per sector
 // Hamiltonian and element type and keeps the fastest.
@@ -39,12 +41,26 @@ __device__ __forceinline__ RowVec<T, R> lds_rows(const T *xs, uint32_t j)
     return *reinterpret_cast<const RowVec<T, R> *>(xs + (size_t)j * R);
 }
 
+template <typename T> __device__ __forceinline__ void ld_cols(const T *p, uint64_t pol, T (&v)[2])
+{
+    const auto t = ld2(p, pol);
+    v[0] = t.x;
+    v[1] = t.y;
+}
+template <typename T> __device__ __forceinline__ void ld_cols(const T *p, uint64_t pol, T (&v)[1]) { v[0] = ld1(p, pol); }
+template <typename T> __device__ __forceinline__ void st_cols(T *p, const T (&v)[2], uint64_t pol)
+{
+    st2(p, v[0], v[1], pol);
+}
+template <typename T> __device__ __forceinline__ void st_cols(T *p, const T (&v)[1], uint64_t pol) { st1(p, v[0], pol); }
+
 // T: element type; R: staged rows per group; KMU: bound on the up-table width;
 // KMD: bound on the down-table row length; NTHR threads per block, at least
-// MINB blocks per SM.
-template <typename T, int R, int KMU, int KMD, int NTHR, int MINB>
+// MINB blocks per SM; CPT columns per thread.
+template <typename T, int R, int KMU, int KMD, int NTHR, int MINB, int CPT = 2>
 __global__ void __launch_bounds__(NTHR, MINB) row_fast_kernel(const HamDev H, const RowArgs a)
 {
+    constexpr bool EXACT = sizeof(T) == 8;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double pal_s[256];
     __shared__ int s_ioff[17];
@@ -135,107 +151,137 @@ __global__ void __launch_bounds__(NTHR, MINB) row_fast_kernel(const HamDev H, co
         }
         __syncthreads();
 
-        for (int c = 2 * threadIdx.x; c < dup; c += 2 * blockDim.x) {
+        for (int c = CPT * threadIdx.x; c < dup; c += CPT * blockDim.x) {
             // ---- loads ----
-            uint2 ent[KMU];
+            uint32_t ent[KMU][CPT];
 #pragma unroll
-            for (int k = 0; k < KMU; ++k)
-                ent[k] = k < K ? ldu2(ell + (size_t)k * dup + c) : make_uint2((uint32_t)c, (uint32_t)(c + 1));
-            typename V2<T>::t xd[R][KMD];
+            for (int k = 0; k < KMU; ++k) {
+                if (CPT == 2) {
+                    const uint2 e2 = k < K ? ldu2(ell + (size_t)k * dup + c) : make_uint2((uint32_t)c, (uint32_t)(c + 1));
+                    ent[k][0] = e2.x;
+                    ent[k][CPT - 1] = e2.y;
+                } else {
+                    ent[k][0] = k < K ? __ldg(ell + (size_t)k * dup + c) : (uint32_t)c;
+                }
+            }
+            T xd[R][KMD][CPT];
 #pragma unroll
             for (int r = 0; r < R; ++r)
 #pragma unroll
-                for (int f = 0; f < KMD; ++f) xd[r][f] = ld2(x + s_nofs[r][f] + c, keep);
+                for (int f = 0; f < KMD; ++f) ld_cols(x + s_nofs[r][f] + c, keep, xd[r][f]);
             // bring the next iteration's neighbour elements towards L2 while this one computes
-            if (c + 2 * (int)blockDim.x < dup) {
+            if (c + CPT * (int)blockDim.x < dup) {
 #pragma unroll
                 for (int r = 0; r < R; ++r)
 #pragma unroll
-                    for (int f = 0; f < KMD; ++f) prefetch_l2(x + s_nofs[r][f] + c + 2 * blockDim.x);
+                    for (int f = 0; f < KMD; ++f) prefetch_l2(x + s_nofs[r][f] + c + CPT * blockDim.x);
             }
-            const int cu0 = H.up.imp[c], cu1 = H.up.imp[c + 1];
-            const double du0 = upd[c], du1 = upd[c + 1];
-            const RowVec<T, R> o0 = lds_rows<T, R>(xs, c), o1 = lds_rows<T, R>(xs, c + 1);
-            double acc[R][2];
+            int cu[CPT];
+            double du[CPT];
+            RowVec<T, R> o[CPT];
+#pragma unroll
+            for (int e = 0; e < CPT; ++e) {
+                cu[e] = H.up.imp[c + e];
+                du[e] = upd[c + e];
+                o[e] = lds_rows<T, R>(xs, c + e);
+            }
+            double acc[R][CPT], accd[R][CPT];
             // ---- ordered accumulation: density terms, diagonal ----
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                double a0 = 0.0, a1 = 0.0;
-                const int g0 = cu0 * ncfg + cd[r], g1 = cu1 * ncfg + cd[r];
-                for (int o2 = s_ioff[g0]; o2 < s_ioff[g0 + 1]; ++o2) a0 = hmadd<T>(a0, s_icoef[o2], o0.v[r]);
-                for (int o2 = s_ioff[g1]; o2 < s_ioff[g1 + 1]; ++o2) a1 = hmadd<T>(a1, s_icoef[o2], o1.v[r]);
-                acc[r][0] = hmadd<T>(a0, fadd(du0, dd[r]), o0.v[r]);
-                acc[r][1] = hmadd<T>(a1, fadd(du1, dd[r]), o1.v[r]);
-            }
+            for (int r = 0; r < R; ++r)
+#pragma unroll
+                for (int e = 0; e < CPT; ++e) {
+                    double a0 = 0.0;
+                    const int g0 = cu[e] * ncfg + cd[r];
+                    for (int o2 = s_ioff[g0]; o2 < s_ioff[g0 + 1]; ++o2) a0 = hmadd<T>(a0, s_icoef[o2], o[e].v[r]);
+                    acc[r][e] = hmadd<T>(a0, fadd(du[e], dd[r]), o[e].v[r]);
+                    accd[r][e] = 0.0;
+                }
             // ---- up-spin hops: one vector load serves the R rows ----
 #pragma unroll
             for (int k = 0; k < KMU; ++k) {
                 if (k >= K) break;
-                const RowVec<T, R> g0 = lds_rows<T, R>(xs, ent[k].x & 0xFFFFFFu);
-                const RowVec<T, R> g1 = lds_rows<T, R>(xs, ent[k].y & 0xFFFFFFu);
-                const double h0 = pal_s[ent[k].x >> 24], h1 = pal_s[ent[k].y >> 24];
 #pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    acc[r][0] = hmadd<T>(acc[r][0], h0, g0.v[r]);
-                    acc[r][1] = hmadd<T>(acc[r][1], h1, g1.v[r]);
+                for (int e = 0; e < CPT; ++e) {
+                    const RowVec<T, R> g = lds_rows<T, R>(xs, ent[k][e] & 0xFFFFFFu);
+                    const double h = pal_s[ent[k][e] >> 24];
+#pragma unroll
+                    for (int r = 0; r < R; ++r) acc[r][e] = hmadd<T>(acc[r][e], h, g.v[r]);
                 }
             }
-            // ---- down-spin hops ----
+            // ---- down-spin hops (FP32 vectors: second accumulator) ----
 #pragma unroll
             for (int r = 0; r < R; ++r)
 #pragma unroll
                 for (int f = 0; f < KMD; ++f) {
                     const double h = s_hd[r][f];
-                    acc[r][0] = hmadd<T>(acc[r][0], h, xd[r][f].x);
-                    acc[r][1] = hmadd<T>(acc[r][1], h, xd[r][f].y);
+#pragma unroll
+                    for (int e = 0; e < CPT; ++e) {
+                        if (EXACT) acc[r][e] = hmadd<T>(acc[r][e], h, xd[r][f][e]);
+                        else accd[r][e] = hmadd<T>(accd[r][e], h, xd[r][f][e]);
+                    }
                 }
+            if (!EXACT) {
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+#pragma unroll
+                    for (int e = 0; e < CPT; ++e) acc[r][e] += accd[r][e];
+            }
             // ---- epilogue ----
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 if (row[r] < 0) continue;
                 const size_t i = (size_t)row[r] * dup + c;
                 T *y = static_cast<T *>(a.y) + i;
-                const T xo[2] = {o0.v[r], o1.v[r]};
-                if (a.mode == kModeHv) {
-                    st2(y, (T)acc[r][0], (T)acc[r][1], stream);
-                } else if (a.mode == kModeFirst) {
-                    T st[2];
+                T xo[CPT];
 #pragma unroll
-                    for (int e = 0; e < 2; ++e) {
+                for (int e = 0; e < CPT; ++e) xo[e] = o[e].v[r];
+                if (a.mode == kModeHv) {
+                    T out[CPT];
+#pragma unroll
+                    for (int e = 0; e < CPT; ++e) out[e] = (T)acc[r][e];
+                    st_cols(y, out, stream);
+                } else if (a.mode == kModeFirst) {
+                    T st[CPT];
+#pragma unroll
+                    for (int e = 0; e < CPT; ++e) {
                         const double v = (double)xo[e];
                         st[e] = (T)(acc[r][e] - gam1 * v);
                         const double sd = (double)st[e];
                         s0 += sd * sd; s1 += sd * v; s2 += v * v;
                     }
-                    st2(y, st[0], st[1], stream);
+                    st_cols(y, st, stream);
                 } else if (a.mode == kModeStep) {
-                    const auto vk2 = ld2(static_cast<const T *>(a.vk) + i, stream);
-                    typename V2<T>::t vm2;
-                    if (a.vkm1) vm2 = ld2(static_cast<const T *>(a.vkm1) + i, stream);
-                    else { vm2.x = T(0); vm2.y = T(0); }
-                    const double vk[2] = {(double)vk2.x, (double)vk2.y}, vm[2] = {(double)vm2.x, (double)vm2.y};
-                    T wt[2], vt[2];
+                    T vkt[CPT], vmt[CPT];
+                    ld_cols(static_cast<const T *>(a.vk) + i, stream, vkt);
+                    if (a.vkm1) ld_cols(static_cast<const T *>(a.vkm1) + i, stream, vmt);
+                    else
 #pragma unroll
-                    for (int e = 0; e < 2; ++e) {
-                        const double sv = (double)xo[e];
-                        vt[e] = (T)((sv - delta * vk[e]) * inv_b);
-                        const double hv1 = (acc[r][e] - delta * (sv + gam * vk[e] + beta_k * vm[e])) * inv_b;
-                        const double w = hv1 - beta_k1 * vk[e];
+                        for (int e = 0; e < CPT; ++e) vmt[e] = T(0);
+                    T wt[CPT], vt[CPT];
+#pragma unroll
+                    for (int e = 0; e < CPT; ++e) {
+                        const double sv = (double)xo[e], vk = (double)vkt[e], vm = (double)vmt[e];
+                        vt[e] = (T)((sv - delta * vk) * inv_b);
+                        const double hv1 = (acc[r][e] - delta * (sv + gam * vk + beta_k * vm)) * inv_b;
+                        const double w = hv1 - beta_k1 * vk;
                         wt[e] = (T)(w - gam1 * (double)vt[e]);
                         const double wd = (double)wt[e], vd = (double)vt[e];
                         s0 += wd * wd; s1 += wd * vd; s2 += vd * vd;
                     }
-                    st2(y, wt[0], wt[1], stream);
-                    st2(static_cast<T *>(a.vout) + i, vt[0], vt[1], stream);
+                    st_cols(y, wt, stream);
+                    st_cols(static_cast<T *>(a.vout) + i, vt, stream);
                     if (a.psi) {
                         T *p = static_cast<T *>(a.psi) + i;
-                        const auto pv = ld2(p, stream);
-                        st2(p, (T)((double)pv.x + cpsi * (double)vt[0]), (T)((double)pv.y + cpsi * (double)vt[1]),
-                            stream);
+                        T pv[CPT];
+                        ld_cols(p, stream, pv);
+#pragma unroll
+                        for (int e = 0; e < CPT; ++e) pv[e] = (T)((double)pv[e] + cpsi * (double)vt[e]);
+                        st_cols(p, pv, stream);
                     }
                 } else {
 #pragma unroll
-                    for (int e = 0; e < 2; ++e) {
+                    for (int e = 0; e < CPT; ++e) {
                         const double rr = acc[r][e] - a.eshift * (double)xo[e];
                         s0 += rr * rr; s2 += (double)xo[e] * (double)xo[e];
                     }
@@ -251,15 +297,15 @@ __global__ void __launch_bounds__(NTHR, MINB) row_fast_kernel(const HamDev H, co
 
 // Launch of one instance: grid = SMs x resident blocks, at most one block per
 // row group; blocks narrower than NTHR when dim_up is small.
-template <typename T, int R, int KMU, int KMD, int NTHR, int MINB>
+template <typename T, int R, int KMU, int KMD, int NTHR, int MINB, int CPT = 2>
 cudaError_t launch_fast_t(const HamDev &H, const RowArgs &a, int num_sms, cudaStream_t st)
 {
-    auto k = row_fast_kernel<T, R, KMU, KMD, NTHR, MINB>;
+    auto k = row_fast_kernel<T, R, KMU, KMD, NTHR, MINB, CPT>;
     const size_t smem = (size_t)R * (size_t)H.dup * sizeof(T);
     // static + dynamic shared memory may exceed the 48 KB default
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    const int cols = (int)((H.dup + 1) / 2);
+    const int cols = (int)((H.dup + CPT - 1) / CPT);
     int block = NTHR;
     if (cols < block) block = ((cols + 31) / 32) * 32;
     if (block < 32) block = 32;

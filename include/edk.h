@@ -79,7 +79,7 @@ int edk_ctx_timing(edk_ctx *ctx, int enable);
  * (default; the fast kernel's launch shape is timed once per sector and
  * element type), 1 = always the generic kernel (for A/B checks), 2 or 3 = the
  * fast kernel where its preconditions hold with its default launch shape,
- * 16+i (i < 8) = the fast kernel with its i-th feasible launch shape (modulo
+ * 16+i (i < 12) = the fast kernel with its i-th feasible launch shape (modulo
  * their number), for measurements. */
 int edk_ctx_set_kernel_path(edk_ctx *ctx, int path);
 int edk_ctx_timing_report(edk_ctx *ctx, int which, int64_t *launches, double *total_ms);

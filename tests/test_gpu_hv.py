@@ -132,3 +132,28 @@ def test_hmult_fp32_large_sectors(ctx, kpath, name, sec):
     y = h.hmult(torch.tensor(x, dtype=torch.float32, device="cuda")).double().cpu().numpy()
     y_ref = O.OracleH(m, *sec).hmult(x.astype(np.float32).astype(np.float64))
     assert np.abs(y - y_ref).max() <= 1.2e-7 * np.abs(y_ref).max()
+
+
+def test_every_fast_kernel_launch_shape_is_exact(ctx):
+    """Each feasible launch shape of the fast row kernel (rows per group, block
+    shape, columns per thread) on the ns=14 (7,7) and (8,7) sectors: FP64
+    bit-exact, FP32 within the output rounding."""
+    import torch
+    m = workload("c3").model
+    rng = np.random.default_rng(13)
+    for sec in [(7, 7), (8, 7)]:
+        h = edk.Hamiltonian(ctx, m, *sec)
+        ho = O.OracleH(m, *sec)
+        x = rng.normal(size=h.dim)
+        y64 = ho.hmult(x)
+        y32 = ho.hmult(x.astype(np.float32).astype(np.float64))
+        xd = torch.tensor(x, device="cuda")
+        xf = xd.to(torch.float32)
+        try:
+            for i in range(12):
+                ctx.set_kernel_path(16 + i)
+                assert np.array_equal(h.hmult(xd).cpu().numpy(), y64), (sec, i)
+                yf = h.hmult(xf).double().cpu().numpy()
+                assert np.abs(yf - y32).max() <= 1.2e-7 * np.abs(y32).max(), (sec, i)
+        finally:
+            ctx.set_kernel_path(0)
