@@ -377,6 +377,36 @@ def run_grad(args):
     ctx.close()
 
 
+def run_c4(args):
+    """The many-small-sectors workload: two-orbital Kanamori model, ns = 12
+    (169 sectors, dims up to 924^2), 3 lowest states per sector inside the
+    exp(-beta (E - E0)) >= 1e-8 window, 8 Green start vectors per state
+    (2 spins x particle/hole x 2 orbitals), 200-step chains, 512 Matsubara
+    points, FP64.  Times one solve with the chains batched into one persistent
+    launch per spin against one launch per chain step."""
+    import torch
+    from ed_solver_b200 import edk
+    from ed_solver_b200.model import workload
+    w = workload("c4")
+    ctx = edk.Context(0)
+    out = {"workload": "c4_ns12_kanamori_all_sectors", "sectors": len(w.sectors)}
+    for mode in (1, 0, 1, 0):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = edk.solve(ctx, w.model, w.sectors, w.beta, 512, dtype="f64", neigen=3, nitergreen=200,
+                      demax0=w.demax0, spins=(0, 1), pairs=[(0, 0), (1, 1)], tolerance=1e-10, green_mode=mode)
+        torch.cuda.synchronize()
+        key = "batched" if mode == 0 else "per_chain"
+        out[key] = {"solve_s": time.perf_counter() - t0, "nstates": r["nstates"],
+                    "green_steps": r["green_steps"], "lanczos_steps": r["lanczos_steps"]}
+        out.setdefault("G_" + key, r["G"])
+    import numpy as np
+    out["max_abs_dG_batched_vs_per_chain"] = float(np.abs(out.pop("G_batched") - out.pop("G_per_chain")).max())
+    out["speedup_batched"] = out["per_chain"]["solve_s"] / out["batched"]["solve_s"]
+    print(json.dumps(out), flush=True)
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -389,7 +419,11 @@ def main():
     ap.add_argument("--grad", action="store_true",
                     help="time the 32 parameter gradients of E0 + G and check them by central differences")
     ap.add_argument("--grad-fd", type=int, default=4, help="parameters checked by central differences (--grad)")
+    ap.add_argument("--c4", action="store_true", help="time the many-small-sectors solve, batched vs per chain")
     args = ap.parse_args()
+    if args.c4:
+        run_c4(args)
+        return
     if args.grad:
         run_grad(args)
         return

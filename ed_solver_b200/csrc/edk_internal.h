@@ -84,7 +84,9 @@ struct RowArgs {
 
 // Launch shape of the fast row kernel: rows per group, up/down table-width
 // bounds, and block shape (variant 0: 512 threads, one block per SM;
-// variant 1: 256 threads, two blocks per SM; two columns per thread in both).
+// variant 1: 256 threads, two blocks per SM; variant 2: 128 threads, four
+// blocks per SM, offered for rows of at most 4096 states; two columns per
+// thread in all).
 // One column per thread (24 resident warps instead of 16) was measured at
 // ns=16 and never beat these two, so it is not instantiated.
 struct FastShape {

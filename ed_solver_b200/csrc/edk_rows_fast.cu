@@ -40,8 +40,11 @@ int fast_shapes(const HamDev &H, int elem_bytes, int num_sms, FastShape *out, in
     int rs[3];
     const int nr = rows_allowed(elem_bytes, kmd, rs);
     int n = 0;
-    for (int variant = 0; variant < 2; ++variant) {
-        const int64_t smem_cap = variant == 0 ? kMaxSmemBytes : kMaxSmemBytes / 2;
+    for (int variant = 0; variant < 3; ++variant) {
+        // shared memory per block when 1, 2 or 4 blocks share an SM
+        const int64_t smem_cap = kMaxSmemBytes / (variant == 0 ? 1 : variant == 1 ? 2 : 4);
+        // 128-thread blocks only pay off for short rows
+        if (variant == 2 && H.dup > 4096) continue;
         for (int i = 0; i < nr && n < cap; ++i) {
             const int r = rs[i];
             if ((int64_t)r * rowbytes > smem_cap) continue;
@@ -61,8 +64,9 @@ cudaError_t launch_rows_fast(const HamDev &H, int dtype, const RowArgs &a, int n
 
 #define EDK_FAST_V(T, R, KMU, KMD)                                                                \
     if (s.r == R && s.kmu == KMU && s.kmd == KMD)                                                 \
-        return s.variant == 0 ? launch_fast_t<T, R, KMU, KMD, 512, 1, 2>(H, a, num_sms, st)       \
-                              : launch_fast_t<T, R, KMU, KMD, 256, 2, 2>(H, a, num_sms, st);
+        return s.variant == 0   ? launch_fast_t<T, R, KMU, KMD, 512, 1, 2>(H, a, num_sms, st)     \
+               : s.variant == 1 ? launch_fast_t<T, R, KMU, KMD, 256, 2, 2>(H, a, num_sms, st)     \
+                                : launch_fast_t<T, R, KMU, KMD, 128, 4, 2>(H, a, num_sms, st);
 #define EDK_FAST_KMU(T, R, KMD) EDK_FAST_V(T, R, 8, KMD) EDK_FAST_V(T, R, 16, KMD)
 
 cudaError_t launch_fast_f32(const HamDev &H, const RowArgs &a, int num_sms, const FastShape &s, cudaStream_t st)

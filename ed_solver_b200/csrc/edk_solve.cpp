@@ -41,8 +41,11 @@ struct DBuf {
     ~DBuf() { if (p) cudaFree(p); }
 };
 
-// Sectors with fewer states than this run in FP64 even in mixed precision.
+// Sectors with fewer states than this run in FP64 even in mixed precision,
+// and their Green chains run batched (one persistent launch for all of them).
 constexpr int64_t kLowprecMinDim = (int64_t)1 << 20;
+// Longest row the batched kernel stages in shared memory (FP64 elements).
+constexpr int64_t kBatchMaxDup = 96 * 1024 / 8;
 
 struct State {
     int nup, ndn;
@@ -292,6 +295,9 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
         for (int spin = 0; spin < 2; ++spin) {
             if (!((o->spin_mask >> spin) & 1)) continue;
             std::fill(raw.begin(), raw.end(), 0.0);
+            // chains of small target sectors, run together after the state loop
+            std::vector<edk_chain> batch;
+            std::vector<DBuf> batch_phi;
             for (auto &s : gs) {
                 edk_h *hs_src = nullptr;
                 if ((rc = getH(s->nup, s->ndn, &hs_src))) return rc;
@@ -322,6 +328,21 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
                     const int gdt = sector_dtype(tdim);
                     const void *psi = nullptr;
                     if ((rc = psi_in(gdt, &psi))) return rc;
+                    int64_t tdup = 0;
+                    edk_h_dims(ht, nullptr, &tdup, nullptr);
+                    if (o->green_mode == 0 && gdt == EDK_F64 && tdim < kLowprecMinDim && tdup <= kBatchMaxDup) {
+                        for (size_t q = 0; q < combos.size(); ++q) {
+                            const int i = combos[q].first, j = combos[q].second;
+                            batch_phi.emplace_back((size_t)tdim * 8);
+                            if (!batch_phi.back().p) return edk_internal_fail(ctx, EDK_ERR_NOMEM, "chain start");
+                            int64_t od = 0;
+                            if ((rc = edk_apply_c(hs_src, gdt, i, spin, iph == 1, i == j ? -1 : j, 1, psi,
+                                                  batch_phi.back().p, &od)))
+                                return rc;
+                            batch.push_back(edk_chain{ht, batch_phi.back().p, s->E, iph, s->boltz, (int32_t)q});
+                        }
+                        continue;
+                    }
                     DBuf phi((size_t)tdim * (gdt == EDK_F64 ? 8 : 4));
                     for (size_t q = 0; q < combos.size(); ++q) {
                         const int i = combos[q].first, j = combos[q].second;
@@ -336,6 +357,15 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
                         for (int w = 0; w < 2 * nw; ++w) raw[q * 2 * nw + w] += s->boltz * Gc[w];
                     }
                 }
+            }
+            if (!batch.empty()) {
+                std::vector<double> Gb((size_t)combos.size() * 2 * nw);
+                edk_batch_stats bst{};
+                if ((rc = edk_green_batch(ctx, EDK_F64, (int32_t)batch.size(), batch.data(), o->nitergreen, nw,
+                                          wn.data(), o->cutoff_dynamic, (int32_t)combos.size(), Gb.data(), 0, &bst)))
+                    return rc;
+                green_steps += bst.steps;
+                for (size_t t = 0; t < Gb.size(); ++t) raw[t] += Gb[t];
             }
             auto idx = [&](int i, int j) {
                 return (size_t)(std::find(combos.begin(), combos.end(), std::make_pair(i, j)) - combos.begin());

@@ -63,7 +63,7 @@ class _SolveOpts(C.Structure):
                 ("check_every", C.c_int32), ("beta", C.c_double), ("demax0", C.c_double),
                 ("nitergreen", C.c_int32), ("nw", C.c_int32), ("spin_mask", C.c_int32), ("npairs", C.c_int32),
                 ("pairs", C.c_void_p), ("cutoff_dynamic", C.c_double), ("ran_tab", C.c_void_p),
-                ("residual_tol", C.c_double)]
+                ("residual_tol", C.c_double), ("green_mode", C.c_int32)]
 
 
 class _SolveResult(C.Structure):
@@ -571,7 +571,8 @@ def green_batch(ctx: Context, chains, nitergreen: int, wn, nout: int, mode: int 
 
 def solve(ctx: Context, model: AIMModel, sectors, beta: float, nw: int, dtype="f64", neigen=1,
           nitermax=1000, tolerance=1e-12, tolerance_lowprec=1e-6, demax0=5.0, nitergreen=200,
-          spins=(0, 1), pairs=None, cutoff_dynamic=1e-8, check_every=8, ran_tab=None, residual_tol=0.0):
+          spins=(0, 1), pairs=None, cutoff_dynamic=1e-8, check_every=8, ran_tab=None, residual_tol=0.0,
+          green_mode=0):
     """One impurity solve through the C-ABI (edk_solve): host inputs, host outputs.
 
     Returns dict(e0, z, residual, nstates, lanczos_steps, green_steps, G (2, npairs, nw) complex,
@@ -586,7 +587,7 @@ def solve(ctx: Context, model: AIMModel, sectors, beta: float, nw: int, dtype="f
     o = _SolveOpts(_dtype_code(dtype), len(sec) // 2, sec.ctypes.data, int(neigen), int(nitermax), float(tolerance),
                    float(tolerance_lowprec), int(check_every), float(beta), float(demax0), int(nitergreen),
                    int(nw), int(mask), len(pr) // 2, pr.ctypes.data, float(cutoff_dynamic),
-                   None if tab is None else tab.ctypes.data, float(residual_tol))
+                   None if tab is None else tab.ctypes.data, float(residual_tol), int(green_mode))
     G = np.zeros((2, len(pr) // 2, nw, 2))
     docc = np.zeros(model.nc)
     en = np.zeros(64)

@@ -337,6 +337,9 @@ typedef struct edk_solve_opts {
     const double *ran_tab;       /* start-vector table, NULL = library table */
     double residual_tol;         /* > 0: eigenvector criterion of the FP64 passes (see
                                     edk_lanczos_opts); mixed precision always refines to it */
+    int32_t green_mode;          /* 0: the chains of target sectors below 2^20 states (FP64)
+                                    run together in one persistent edk_green_batch launch per
+                                    spin; 1: every chain on its own (edk_green_chain) */
 } edk_solve_opts;
 
 typedef struct edk_solve_result {

@@ -96,3 +96,18 @@ def test_solve_two_orbital_kanamori_all_sectors(ctx):
     Go = O.green_impurity(w.model, gso, w.beta, 64, 100, spin=0, pairs=[(0, 0), (1, 1), (0, 1)])
     assert np.abs(r["G"][0, 0] - Go[(0, 0)]).max() < 1e-7
     assert np.abs(r["G"][0, 2] - Go[(0, 1)]).max() < 1e-7
+
+
+def test_batched_chains_in_the_solve_equal_per_chain_runs(ctx):
+    """ns=12 two-orbital Kanamori model, sectors (6,6), (5,6), (6,5) with three
+    states each: the Green chains of these small sectors run in one persistent
+    launch per spin (green_mode 0) or one by one (green_mode 1); G agrees to 1e-9."""
+    w = workload("c4")
+    kw = dict(dtype="f64", neigen=3, nitergreen=120, spins=(0, 1), pairs=[(0, 0), (1, 1), (0, 1)],
+              tolerance=1e-11, demax0=w.demax0)
+    secs = [(6, 6), (5, 6), (6, 5)]
+    r0 = edk.solve(ctx, w.model, secs, w.beta, 128, green_mode=0, **kw)
+    r1 = edk.solve(ctx, w.model, secs, w.beta, 128, green_mode=1, **kw)
+    assert r0["nstates"] == r1["nstates"] and r0["e0"] == r1["e0"]
+    assert r0["green_steps"] == r1["green_steps"]
+    assert np.abs(r0["G"] - r1["G"]).max() < 1e-9 * max(1.0, np.abs(r1["G"]).max())
