@@ -28,6 +28,7 @@ cudaError_t launch_lincomb(int64_t n, double *out, bool accumulate, const double
 cudaError_t launch_dots(int64_t n, const double *x0, const double *y0, const double *x1, const double *y1,
                         const double *x2, const double *y2, const double *x3, const double *y3, double *partials,
                         unsigned *counter, double *out, int grid, cudaStream_t st);
+cudaError_t launch_fill_periodic(int64_t n, const double *tab, int64_t offset, double *out, int grid, cudaStream_t st);
 cudaError_t launch_bilinear(int64_t dup, int64_t ddn, const double *a, const double *b, const uint32_t *st_up,
                             const uint32_t *st_dn, int np, const ParamDev *P, double *partials, unsigned *counter,
                             double *out, int grid, cudaStream_t st);

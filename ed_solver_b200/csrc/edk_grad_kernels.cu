@@ -139,7 +139,21 @@ __global__ void __launch_bounds__(512, 1) bilinear_kernel(int dup, int ddn, cons
     if (threadIdx.x == 0) *counter = 0u;
 }
 
+// out[i] = tab[(i + offset) % 10000 + 1] (the reference's periodic start
+// vector, rcvector_class.f90:43-60, shifted by `offset` for a block column)
+__global__ void fill_periodic_kernel(int64_t n, const double *tab, int64_t offset, double *out)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = tab[(i + offset) % 10000 + 1];
+}
+
 }  // namespace
+
+cudaError_t launch_fill_periodic(int64_t n, const double *tab, int64_t offset, double *out, int grid, cudaStream_t st)
+{
+    fill_periodic_kernel<<<grid, 256, 0, st>>>(n, tab, offset, out);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_lincomb(int64_t n, double *out, bool accumulate, const double *x0, double c0,
                            const double *x1, double c1, const double *x2, double c2, const double *x3,

@@ -170,4 +170,63 @@ void dense_eigh(int n, std::vector<double> A, std::vector<double> &w, std::vecto
     V.swap(V2);
 }
 
+void dense_lowest(int n, std::vector<double> A, int m, std::vector<double> &w, std::vector<double> &V)
+{
+    // A = Q T Q^T with Q = H_0 H_1 ... H_{n-3}, H_k = 1 - 2 v_k v_k^T acting on indices k+1..n-1
+    std::vector<std::vector<double>> refl(n > 2 ? n - 2 : 0);
+    std::vector<double> p(n), q(n);
+    auto a = [&](int i, int j) -> double & { return A[(size_t)i * n + j]; };
+    for (int k = 0; k + 2 < n; ++k) {
+        const int len = n - k - 1;
+        double nrm = 0.0;
+        for (int i = 0; i < len; ++i) nrm += a(k + 1 + i, k) * a(k + 1 + i, k);
+        nrm = std::sqrt(nrm);
+        std::vector<double> &v = refl[k];
+        v.assign(len, 0.0);
+        if (nrm == 0.0) continue;
+        const double x0 = a(k + 1, k);
+        const double alpha = x0 >= 0 ? -nrm : nrm;
+        for (int i = 0; i < len; ++i) v[i] = a(k + 1 + i, k);
+        v[0] -= alpha;
+        double vn = 0.0;
+        for (int i = 0; i < len; ++i) vn += v[i] * v[i];
+        vn = std::sqrt(vn);
+        if (vn == 0.0) { v.assign(len, 0.0); continue; }
+        for (int i = 0; i < len; ++i) v[i] /= vn;
+        // trailing block: A22 <- A22 - v q^T - q v^T, q = 2 (A22 v) - 2 (v^T A22 v) v
+        double c = 0.0;
+        for (int i = 0; i < len; ++i) {
+            double t = 0.0;
+            for (int j = 0; j < len; ++j) t += a(k + 1 + i, k + 1 + j) * v[j];
+            p[i] = t;
+            c += v[i] * t;
+        }
+        for (int i = 0; i < len; ++i) q[i] = 2.0 * p[i] - 2.0 * c * v[i];
+        for (int i = 0; i < len; ++i)
+            for (int j = 0; j < len; ++j) a(k + 1 + i, k + 1 + j) -= v[i] * q[j] + q[i] * v[j];
+        a(k + 1, k) = a(k, k + 1) = alpha;
+        for (int i = 1; i < len; ++i) a(k + 1 + i, k) = a(k, k + 1 + i) = 0.0;
+    }
+    std::vector<double> d(n), e(n > 1 ? n - 1 : 1);
+    for (int i = 0; i < n; ++i) d[i] = a(i, i);
+    for (int i = 0; i + 1 < n; ++i) e[i] = a(i + 1, i);
+    m = std::min(m, n);
+    w.assign(m, 0.0);
+    tridiag_lowest(n, d.data(), e.data(), m, w.data());
+    V.assign((size_t)n * m, 0.0);
+    std::vector<double> prev((size_t)n * m), y(n);
+    for (int j = 0; j < m; ++j) {
+        tridiag_vector(n, d.data(), e.data(), w[j], prev.data(), j, y.data());
+        std::copy(y.begin(), y.end(), prev.begin() + (size_t)j * n);
+        for (int k = n - 3; k >= 0; --k) {
+            const std::vector<double> &v = refl[k];
+            if (v.empty()) continue;
+            double t = 0.0;
+            for (size_t i = 0; i < v.size(); ++i) t += v[i] * y[k + 1 + i];
+            for (size_t i = 0; i < v.size(); ++i) y[k + 1 + i] -= 2.0 * t * v[i];
+        }
+        for (int i = 0; i < n; ++i) V[(size_t)i * m + j] = y[i];
+    }
+}
+
 }  // namespace edk

@@ -96,6 +96,11 @@ class _GradStats(C.Structure):
                 ("cg_iterations", C.c_int32), ("cg_residual", C.c_double), ("stored_vectors", C.c_int32)]
 
 
+class _BlockOpts(C.Structure):
+    _fields_ = [("block", C.c_int32), ("nitermax", C.c_int32), ("neigen", C.c_int32), ("tolerance", C.c_double),
+                ("check_every", C.c_int32), ("ran_tab", C.c_void_p)]
+
+
 PARAM_EC, PARAM_EB, PARAM_VBC, PARAM_U = 0, 1, 2, 3
 
 
@@ -185,6 +190,7 @@ def lib():
         "edk_solve": (C.c_int, [P, P, P, P]),
         "edk_green_batch": (C.c_int, [P, C.c_int, I32, P, I32, I32, P, D, I32, P, I32, P]),
         "edk_dh_bilinear": (C.c_int, [P, P, P, I32, P, P]),
+        "edk_block_lanczos": (C.c_int, [P, P, P, P, P, P]),
         "edk_grad_e0": (C.c_int, [P, P, I32, P, P]),
         "edk_grad_green": (C.c_int, [P, P, D, I32, P, I32, I32, P, P, D, I32, P, D, P, P, P]),
     }
@@ -464,6 +470,21 @@ class Hamiltonian:
         self.ctx.check(lib().edk_apply_c(self.h, _dtype_code(vec.dtype), site, spin, int(bool(dagger)),
                                          site2, sign2, _ptr(vec), _ptr(out), C.byref(od)), "edk_apply_c")
         return out, (tnup, tndn)
+
+    def block_lanczos(self, block=2, neigen=4, nitermax=300, tolerance=1e-12, check_every=4, vectors=True,
+                      ran_tab=None):
+        """Block_Lanczos_diagonalize: lowest eigenvalues (and FP64 eigenvectors
+        as a (neigen, dim) device tensor when vectors) by block Lanczos."""
+        import torch
+        tab = None if ran_tab is None else np.ascontiguousarray(ran_tab, np.float64)
+        o = _BlockOpts(int(block), int(nitermax), int(neigen), float(tolerance), int(check_every),
+                       None if tab is None else tab.ctypes.data)
+        E = np.zeros(neigen)
+        V = torch.zeros((neigen, self.dim), dtype=torch.float64, device=f"cuda:{self.ctx.device}") if vectors else None
+        it, conv = C.c_int32(), C.c_int32()
+        self.ctx.check(lib().edk_block_lanczos(self.h, C.byref(o), E.ctypes.data, _ptr(V), C.byref(it), C.byref(conv)),
+                       "edk_block_lanczos")
+        return E, V, it.value, bool(conv.value)
 
     # ---- parameter gradients -----------------------------------------------
     def dh_bilinear(self, a, b, params):

@@ -220,6 +220,28 @@ int edk_double_occ(edk_h *h, int dtype, const void *psi_dev, int site, double *d
 /* |H psi - e psi| and |psi| with the FP64 matvec (psi in FP64). */
 int edk_residual(edk_h *h, const void *psi_dev, double e, double *res_norm, double *psi_norm);
 
+/* ---- block Lanczos (Block_Lanczos_diagonalize, Block_Lanczos.f90:37-355) ----
+ * The reference drives BLZPACK (not part of its sources) with H applied to a
+ * block of NVOPU vectors (Block_Lanczos.f90:222-246).  This is a plain block
+ * Lanczos of block size p: V_1 = QR of p periodic start vectors
+ * (tab[(i + 977 c) % 10000 + 1] for column c), then
+ *   W = H V_j - V_{j-1} B_j^T - V_j A_j  (A_j = V_j^T H V_j, orthogonalised twice),
+ *   W = V_{j+1} B_{j+1} (modified Gram-Schmidt),
+ * with the lowest eigenvalues of the block tridiagonal checked every
+ * check_every block steps until each of the neigen lowest changes by less
+ * than tolerance.  Eigenvectors, when vecs_dev is given (neigen x dim FP64,
+ * vector e at e*dim), come from a second pass of the same recurrence.  FP64. */
+typedef struct edk_block_opts {
+    int32_t block;               /* block size p, 1..4 */
+    int32_t nitermax;            /* block steps */
+    int32_t neigen;              /* lowest eigenpairs (<= 64) */
+    double tolerance;            /* eigenvalue change for convergence */
+    int32_t check_every;         /* block steps between checks */
+    const double *ran_tab;       /* 10001-entry start table (host), NULL = library table */
+} edk_block_opts;
+int edk_block_lanczos(edk_h *h, const edk_block_opts *opts, double *E_host, void *vecs_dev, int32_t *niter,
+                      int32_t *converged);
+
 /* ---- batched Green chains ------------------------------------------------
  * Many compute_dynamic chains (green_class_compute_dynamic.f90:191-334) at
  * once, as compute_greenAA issues them for every sector, particle/hole part,
