@@ -183,18 +183,20 @@ __device__ __forceinline__ uint2 ldu2(const uint32_t *p)
 //   alpha = <s',v'> + gamma |v'|^2,  delta = alpha - gamma,
 //   beta^2 = |s'|^2 - 2 delta <s',v'> + delta^2 |v'|^2,
 // a difference of numbers of size beta^2 + delta^2 instead of |w|^2.
-__device__ __forceinline__ double step_gamma(const RowArgs &a)
+// The step index of a launch: the argument, or the device counter.
+__device__ __forceinline__ int step_index(const RowArgs &a) { return a.kdev ? *a.kdev : a.k; }
+__device__ __forceinline__ double step_gamma(const RowArgs &a, int k)
 {
-    return a.mode == kModeFirst ? a.gamma1 : a.tri_diag[a.k - 1];
+    return a.mode == kModeFirst ? a.gamma1 : a.tri_diag[k - 1];
 }
-__device__ __forceinline__ void lanczos_finalize(const RowArgs &a)
+__device__ __forceinline__ void lanczos_finalize(const RowArgs &a, int k)
 {
     const double sss = a.sums_out[0], ssv = a.sums_out[1], svv = a.sums_out[2];
-    const double g = step_gamma(a);
+    const double g = step_gamma(a, k);
     const double al = ssv + g * svv;
     const double de = al - g;
     const double b2 = sss - 2.0 * de * ssv + de * de * svv;
-    const int slot = (a.mode == kModeFirst) ? 0 : a.k;
+    const int slot = (a.mode == kModeFirst) ? 0 : k;
     double b = b2 > 0.0 ? sqrt(b2) : 0.0;
     const bool finite = isfinite(al) && isfinite(b2);
     if (!finite) { a.flags[1] = 1; b = 0.0; }
@@ -204,6 +206,7 @@ __device__ __forceinline__ void lanczos_finalize(const RowArgs &a)
     a.tri_diag[slot] = finite ? al : 0.0;
     a.tri_sub[slot + 1] = b;
     if (!(b >= a.cutoff) && a.flags[0] == 0) a.flags[0] = slot + 1;
+    if (a.kdev && a.mode == kModeStep) *a.kdev = k + 1;
 }
 
 }  // namespace edk

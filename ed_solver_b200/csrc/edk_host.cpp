@@ -91,6 +91,13 @@ struct edk_ctx {
     DevBuf work[2][5];
     size_t tri_cap = 0;
     int reduce_grid = 0;
+    bool graphs = true;      // replay pairs of fused Lanczos steps as a CUDA graph
+    cudaStream_t capture_stream = nullptr;   // private stream the graphs are captured on
+    // pinned host copies of alpha, beta and the flags for the overlapped
+    // convergence checks of Lanczos pass 1
+    double *pin_tri = nullptr;
+    size_t pin_cap = 0;
+    cudaEvent_t pin_ev = nullptr;
     int kernel_path = 0;     // 0 = fastest applicable row kernel, 1 = generic row kernel only,
                              // 2/3 = the fast kernel where applicable
     // optional event timing of row-kernel launches: (class, start, stop)
@@ -131,6 +138,9 @@ struct edk_ctx {
     }
     ~edk_ctx() {
         drain_timing();
+        if (capture_stream) cudaStreamDestroy(capture_stream);
+        if (pin_tri) cudaFreeHost(pin_tri);
+        if (pin_ev) cudaEventDestroy(pin_ev);
         for (auto e : event_pool) cudaEventDestroy(e);
     }
 
@@ -401,6 +411,13 @@ struct Krylov {
     void *psi = nullptr;
     double cutoff = 1e-25;
     double gamma1 = 0.0;    // shift of the first stored vector (energy scale of the chain)
+    // two consecutive fused steps captured as a CUDA graph at step gk0; the
+    // buffer rotation has period 2, so the graph replays from every step of
+    // the same parity (the step index comes from a device counter)
+    cudaGraphExec_t gexec = nullptr;
+    int gk0 = -1;
+    bool graph_off = false;
+    ~Krylov() { if (gexec) cudaGraphExecDestroy(gexec); }
 };
 
 // v1 = start/|start| into w[1]; tri_sub[0] = |start|; psi = coef[0]*v1 when psi set
@@ -464,6 +481,90 @@ int krylov_step(Krylov &K)
     return EDK_OK;
 }
 
+// Fused steps until K.k == target.  From step 2 on, when the context allows
+// graphs and no per-launch timing is recorded, pairs of steps run as one CUDA
+// graph launch (captured once per Krylov run; the first steps, which also time
+// the row kernel's launch shapes, run as plain launches).
+int krylov_run(Krylov &K, int target)
+{
+    edk_ctx *c = K.h->ctx;
+    while (K.k < target) {
+        const bool eligible = c->graphs && !c->timing && !K.graph_off && K.k >= 2 && target - K.k >= 2;
+        if (eligible && !K.gexec) {
+            // capture two steps with the device step counter, then restore the host state
+            const Krylov save_state{K.h, K.dtype, {}, K.ivk, K.ivkm1, K.is, K.is_out, K.k};
+            const int64_t launches0 = c->launches;
+            cudaGraph_t g = nullptr;
+            // capture on a private stream (the context's may be the legacy default stream,
+            // which cannot be captured); nothing runs during capture
+            if (!c->capture_stream &&
+                cudaStreamCreateWithFlags(&c->capture_stream, cudaStreamNonBlocking) != cudaSuccess) {
+                c->capture_stream = nullptr;
+                K.graph_off = true;
+                continue;
+            }
+            cudaStream_t user_stream = c->stream;
+            c->stream = c->capture_stream;
+            if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+                c->stream = user_stream;
+                (void)cudaGetLastError();
+                K.graph_off = true;
+                continue;
+            }
+            int rc1 = EDK_OK;
+            for (int s = 0; s < 2 && rc1 == EDK_OK; ++s) {
+                RowArgs a = base_args(K.h);
+                a.cutoff = K.cutoff;
+                a.gamma1 = K.gamma1;
+                a.mode = kModeStep;
+                a.k = K.k;
+                a.kdev = c->flags.as<int>() + 8;
+                a.x = K.w[K.is];
+                a.y = K.w[K.is_out];
+                a.vk = K.w[K.ivk];
+                a.vkm1 = K.w[K.ivkm1];
+                a.vout = K.w[K.ivkm1];
+                a.psi = K.psi;
+                a.psi_coef = K.psi_coef;
+                rc1 = rows(K.h, K.dtype, a);
+                std::swap(K.ivk, K.ivkm1);
+                std::swap(K.is, K.is_out);
+                K.k += 1;
+            }
+            const cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+            c->stream = user_stream;
+            K.ivk = save_state.ivk; K.ivkm1 = save_state.ivkm1; K.is = save_state.is; K.is_out = save_state.is_out;
+            K.k = save_state.k;
+            c->launches = launches0;
+            c->last_error.clear();
+            if (rc1 == EDK_OK && e2 == cudaSuccess && g &&
+                cudaGraphInstantiate(&K.gexec, g, 0) == cudaSuccess) {
+                K.gk0 = K.k;
+            } else {
+                K.gexec = nullptr;
+                K.graph_off = true;          // fall back to plain launches for this run
+                (void)cudaGetLastError();
+            }
+            if (g) cudaGraphDestroy(g);
+            continue;
+        }
+        if (eligible && K.gexec && ((K.k - K.gk0) & 1) == 0) {
+            int rc = c->cuda(launch_set_int(c->flags.as<int>() + 8, K.k, c->stream), "step counter");
+            c->launches++;
+            if (rc) return rc;
+            while (target - K.k >= 2) {
+                if ((rc = c->cuda(cudaGraphLaunch(K.gexec, c->stream), "graph launch"))) return rc;
+                c->launches += 2;
+                K.k += 2;
+            }
+            continue;
+        }
+        int rc = krylov_step(K);
+        if (rc) return rc;
+    }
+    return EDK_OK;
+}
+
 struct TriHost {
     std::vector<double> diag, sub;
     int flags[2] = {0, 0};
@@ -484,6 +585,51 @@ int fetch_tri(edk_ctx *c, int n, TriHost &t)
                                  c->stream), "d2h flags");
     if (rc) return rc;
     return c->cuda(cudaStreamSynchronize(c->stream), "sync");
+}
+
+// Enqueue the copy of alpha_1..alpha_{n+1}, beta_0..beta_{n+1} and the flags
+// into pinned host memory and record an event after it; the host can then
+// queue more steps before waiting on the event (tri_wait).
+int tri_enqueue(edk_ctx *c, int n)
+{
+    const size_t need = (size_t)(2 * n + 8);
+    if (need > c->pin_cap) {
+        if (c->pin_tri) cudaFreeHost(c->pin_tri);
+        c->pin_tri = nullptr;
+        c->pin_cap = 0;
+        const size_t cap = std::max<size_t>(need, 4096);
+        int rc = c->cuda(cudaMallocHost(reinterpret_cast<void **>(&c->pin_tri), sizeof(double) * cap), "pinned tri");
+        if (rc) return rc;
+        c->pin_cap = cap;
+    }
+    if (!c->pin_ev) {
+        int rc = c->cuda(cudaEventCreateWithFlags(&c->pin_ev, cudaEventDisableTiming), "event");
+        if (rc) return rc;
+    }
+    c->d2h_bytes += (int64_t)sizeof(double) * (2 * n + 3) + 8;
+    double *d = c->pin_tri, *sb = c->pin_tri + (n + 1);
+    int *fl = reinterpret_cast<int *>(c->pin_tri + (2 * n + 3));
+    int rc = c->cuda(cudaMemcpyAsync(d, c->tri_diag.p, sizeof(double) * (n + 1), cudaMemcpyDeviceToHost, c->stream),
+                     "d2h tri");
+    if (rc) return rc;
+    rc = c->cuda(cudaMemcpyAsync(sb, c->tri_sub.p, sizeof(double) * (n + 2), cudaMemcpyDeviceToHost, c->stream),
+                 "d2h tri");
+    if (rc) return rc;
+    rc = c->cuda(cudaMemcpyAsync(fl, c->flags.p, sizeof(int) * 2, cudaMemcpyDeviceToHost, c->stream), "d2h flags");
+    if (rc) return rc;
+    return c->cuda(cudaEventRecord(c->pin_ev, c->stream), "event");
+}
+
+int tri_wait(edk_ctx *c, int n, TriHost &t)
+{
+    int rc = c->cuda(cudaEventSynchronize(c->pin_ev), "sync tri");
+    if (rc) return rc;
+    t.diag.assign(c->pin_tri, c->pin_tri + (n + 1));
+    t.sub.assign(c->pin_tri + (n + 1), c->pin_tri + (2 * n + 3));
+    const int *fl = reinterpret_cast<const int *>(c->pin_tri + (2 * n + 3));
+    t.flags[0] = fl[0];
+    t.flags[1] = fl[1];
+    return EDK_OK;
 }
 
 const double *ran_tab_for(edk_ctx *c, const double *user_tab, int *rc)
@@ -623,6 +769,13 @@ int edk_internal_h_sibling(edk_h *h, int nup, int ndn, edk_h **out)
 
 // The basis states of one spin species of the sector (increasing order).
 const uint64_t *edk_internal_h_states(const edk_h *h, int spin) { return h->tab[spin].states.data(); }
+
+int edk_ctx_set_graphs(edk_ctx *ctx, int enable)
+{
+    if (!ctx) return EDK_ERR_INVALID;
+    ctx->graphs = enable != 0;
+    return EDK_OK;
+}
 
 int edk_ctx_set_kernel_path(edk_ctx *ctx, int path)
 {
@@ -857,13 +1010,21 @@ int edk_lanczos_e0(edk_h *h, const edk_lanczos_opts *o, edk_lanczos_result *r)
     TriHost T;
     int checked = 0, stop_at = 0, status = EDK_OK, target_rank = 0;
     if (o->use_target) ne = 1;
+    // batches of `every` steps; the next batch is queued before the host checks
+    // the previous one, so the device keeps running while the host bisects
+    int queued = std::min(niter_max, K.k + every);
+    if ((rc = krylov_run(K, queued))) return rc;
+    if ((rc = tri_enqueue(c, queued))) return rc;
     while (!stop_at) {
-        const int target = std::min(niter_max, K.k + every);
-        while (K.k < target)
-            if ((rc = krylov_step(K))) return rc;
-        if ((rc = fetch_tri(c, K.k, T))) return rc;
+        const int ready = queued;
+        if (ready < niter_max) {
+            queued = std::min(niter_max, K.k + every);
+            if ((rc = krylov_run(K, queued))) return rc;
+        }
+        if ((rc = tri_wait(c, ready, T))) return rc;
+        if (queued > ready && (rc = tri_enqueue(c, queued))) return rc;
         if (T.flags[1]) return c->fail(EDK_ERR_NOT_FINITE, "non-finite Lanczos coefficient");
-        for (int it = checked + 1; it <= K.k; ++it) {
+        for (int it = checked + 1; it <= ready; ++it) {
             const int m = std::min(ne, it);
             if (o->use_target) {
                 // refinement restart: follow the Ritz value nearest the target
@@ -899,8 +1060,8 @@ int edk_lanczos_e0(edk_h *h, const edk_lanczos_opts *o, edk_lanczos_result *r)
             }
             for (int j = 0; j < m; ++j) last[j] = valp[j];
         }
-        checked = K.k;
-        if (!stop_at && K.k >= niter_max) stop_at = niter_max;
+        checked = ready;
+        if (!stop_at && ready >= niter_max) stop_at = niter_max;
     }
     // eigenpairs of T_{stop_at}
     const int n = stop_at;
@@ -960,8 +1121,7 @@ int edk_lanczos_gs(edk_h *h, const edk_lanczos_opts *o, int32_t niter, const dou
     if ((rc = krylov_start(K, o->start_dev, tab, nullptr))) return rc;
     // iterations 1..niter-1 produce v_2..v_niter (the last H*v is not needed
     // by the eigenvector but keeps one kernel for every step)
-    while (K.k < niter)
-        if ((rc = krylov_step(K))) return rc;
+    if ((rc = krylov_run(K, niter))) return rc;
     if (niter == 1) {
         // nothing beyond psi = coef[0] v1
     }
@@ -1063,8 +1223,7 @@ int edk_green_chain(edk_h *t, int dtype, const void *start_dev, int32_t nitergre
         return EDK_OK;
     }
     if (rc) return rc;
-    while (K.k < niter)
-        if ((rc = krylov_step(K))) return rc;
+    if ((rc = krylov_run(K, niter))) return rc;
     TriHost T;
     if ((rc = fetch_tri(c, K.k, T))) return rc;
     if (T.flags[1]) return c->fail(EDK_ERR_NOT_FINITE, "non-finite Lanczos coefficient");

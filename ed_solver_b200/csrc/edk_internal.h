@@ -73,6 +73,8 @@ struct RowArgs {
     double *tri_diag = nullptr;    // device alpha array (Dagotto layout, 0-based alpha_{k+1} at [k])
     double *tri_sub = nullptr;     // device beta array (tri_sub[k] = beta_{k+1})
     int k = 0;                     // 1-based step index of v_k
+    int *kdev = nullptr;           // when set (step mode), the index is read from here and the
+                                   // last block advances it: consecutive steps replayable as a graph
     double gamma1 = 0.0;           // shift of the first stored vector s_2 = H v_1 - gamma1 v_1
     double eshift = 0.0;           // residual mode: e
     double cutoff = 1e-25;
@@ -129,6 +131,7 @@ bool fast_rows_ok(const HamDev &H, int elem_bytes);
 int fast_shapes(const HamDev &H, int elem_bytes, int num_sms, FastShape *out, int cap);
 cudaError_t launch_rows_fast(const HamDev &H, int dtype, const RowArgs &a, int num_sms, const FastShape &s,
                              cudaStream_t st);
+cudaError_t launch_set_int(int *p, int v, cudaStream_t st);
 cudaError_t launch_start_vector(int dtype, int64_t n, const double *ran_tab_dev,
                                 const void *user_start, void *v, double *partials,
                                 unsigned *counter, double *sums_out, int grid, cudaStream_t st);

@@ -76,17 +76,18 @@ __global__ void __launch_bounds__(NTHR, MINB) row_fast_kernel(const HamDev H, co
     // delta_k = alpha_k - gamma_k; the new vector is s' = w_{k+1} - gamma_{k+1} v_{k+1}
     // with gamma_{k+1} = alpha_k
     double delta = 0.0, gam = 0.0, gam1 = a.gamma1, beta_k = 0.0, beta_k1 = 0.0, inv_b = 0.0, cpsi = 0.0;
+    const int ks = step_index(a);
     if (a.mode == kModeStep) {
-        beta_k1 = a.tri_sub[a.k];
+        beta_k1 = a.tri_sub[ks];
         // the chain already ended (breakdown recorded by an earlier launch)
         if (!(beta_k1 >= a.cutoff) || a.flags[0] != 0) return;
-        const double alpha = a.tri_diag[a.k - 1];
-        gam = a.k >= 2 ? a.tri_diag[a.k - 2] : a.gamma1;
+        const double alpha = a.tri_diag[ks - 1];
+        gam = ks >= 2 ? a.tri_diag[ks - 2] : a.gamma1;
         delta = alpha - gam;
         gam1 = alpha;
-        beta_k = a.k >= 2 ? a.tri_sub[a.k - 1] : 0.0;
+        beta_k = ks >= 2 ? a.tri_sub[ks - 1] : 0.0;
         inv_b = 1.0 / beta_k1;
-        if (a.psi_coef) cpsi = a.psi_coef[a.k];
+        if (a.psi_coef) cpsi = a.psi_coef[ks];
     }
     {
         for (int i = threadIdx.x; i < H.up.npal; i += blockDim.x) pal_s[i] = H.up.pal[i];
@@ -292,7 +293,7 @@ __global__ void __launch_bounds__(NTHR, MINB) row_fast_kernel(const HamDev H, co
     if (a.mode == kModeHv) return;
     double v[4] = {s0, s1, s2, 0.0};
     if (grid_sum<4>(v, a.partials, a.counter, a.sums_out))
-        if (a.mode == kModeFirst || a.mode == kModeStep) lanczos_finalize(a);
+        if (a.mode == kModeFirst || a.mode == kModeStep) lanczos_finalize(a, ks);
 }
 
 // Launch of one instance: grid = SMs x resident blocks, at most one block per

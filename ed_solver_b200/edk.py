@@ -169,6 +169,7 @@ def lib():
         "edk_ctx_launch_count": (I64, [P]),
         "edk_ctx_timing": (C.c_int, [P, C.c_int]),
         "edk_ctx_set_kernel_path": (C.c_int, [P, C.c_int]),
+        "edk_ctx_set_graphs": (C.c_int, [P, C.c_int]),
         "edk_ctx_timing_elements": (C.c_int, [P, C.c_int, P]),
         "edk_ctx_transfer_bytes": (C.c_int, [P, P, P]),
         "edk_ctx_clear_cache": (C.c_int, [P]),
@@ -303,6 +304,10 @@ class Context:
     def set_kernel_path(self, path: int):
         """0: fastest applicable row kernel (default); 1: generic row kernel only."""
         self.check(lib().edk_ctx_set_kernel_path(self.h, int(path)), "edk_ctx_set_kernel_path")
+
+    def set_graphs(self, enable: bool):
+        """Replay pairs of fused Lanczos steps as CUDA graphs (default on)."""
+        self.check(lib().edk_ctx_set_graphs(self.h, int(bool(enable))), "set_graphs")
 
     def timing(self, enable: bool):
         self.check(lib().edk_ctx_timing(self.h, int(enable)), "edk_ctx_timing")

@@ -82,6 +82,11 @@ int edk_ctx_timing(edk_ctx *ctx, int enable);
  * 16+i (i < 12) = the fast kernel with its i-th feasible launch shape (modulo
  * their number), for measurements. */
 int edk_ctx_set_kernel_path(edk_ctx *ctx, int path);
+/* 1 (default): Lanczos passes and Green chains replay pairs of fused steps as
+ * one CUDA graph launch (captured once per run, from the third step on, on
+ * the context's stream; not while per-launch timing is on); 0: plain launches.
+ * Results are identical either way. */
+int edk_ctx_set_graphs(edk_ctx *ctx, int enable);
 int edk_ctx_timing_report(edk_ctx *ctx, int which, int64_t *launches, double *total_ms);
 /* Sum over the timed launches of class `which` of the sector dimension each
  * processed (for algorithmic-byte accounting). */

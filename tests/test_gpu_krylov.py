@@ -205,3 +205,25 @@ def test_block_lanczos_against_dense_ed(ctx):
             r = h.hmult(V[e]) - E[e] * V[e]
             assert float(torch.linalg.norm(r)) < 1e-6
     assert abs(ref[1] - ref[0]) < 1e-9          # the symmetric model does have a degenerate ground level
+
+
+def test_graph_replayed_steps_equal_plain_launches(ctx):
+    """Pairs of fused steps replayed as a CUDA graph give the same Krylov
+    coefficients, eigenvector and Green function, bit for bit, as plain
+    launches (ns=8 and the ns=14 (7,7) sector, pass 1, pass 2 and a chain)."""
+    import torch
+    for name, sec in [("c1", (4, 4)), ("c3", (7, 7))]:
+        w = workload(name)
+        h = edk.Hamiltonian(ctx, w.model, *sec)
+        res = []
+        for g in (False, True):
+            ctx.set_graphs(g)
+            r = h.lanczos_e0("f64", nitermax=60, tolerance=0.0, check_every=7)
+            psi = h.lanczos_gs(r["vecp"][0])
+            phi, ts = h.apply_c(psi, 0, 0, True)
+            ht = edk.Hamiltonian(ctx, w.model, *ts)
+            G, dg, sd, n = ht.green_chain(phi, 41, r["E"][0], 1, matsubara(w.beta, 16))
+            res.append((r["diag"], r["subdiag"], psi.cpu().numpy(), G, dg))
+        ctx.set_graphs(True)
+        for a, b in zip(res[0], res[1]):
+            assert np.array_equal(a, b)
