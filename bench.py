@@ -118,10 +118,8 @@ class ClockSampler:
 
 
 def _dist():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from ed_solver_b200.replicas import env
+    return env()
 
 
 def _model():
@@ -188,21 +186,14 @@ def run_ours(args):
     import numpy as np
     import torch
     from ed_solver_b200 import edk
+    from ed_solver_b200.replicas import Replicas
     ws, rank, local = _dist()
     torch.cuda.set_device(local)
-    dist = None
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    rep = Replicas("nccl", timeout_s=600.0, device=local)
     ctx = edk.Context(local)
     model = _model()
     stream = torch.cuda.current_stream(local)
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize(local)
+    barrier = rep.barrier
 
     # ---- warm-up (tables built once and kept on the context) ----
     for _ in range(args.warmup):
@@ -223,11 +214,7 @@ def run_ours(args):
     n5, t5, e5 = ctx.timing_report(5)          # first Lanczos step, FP32
     ctx.timing(False)
     clocks = clk.summary()
-    t_max = ms
-    if dist is not None:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
+    t_max = rep.max(ms)
     value = ws * args.steps / (t_max * 1e-3)
     res = results[-1]
 
@@ -291,9 +278,7 @@ def run_ours(args):
                                  "docc": float(res["docc"][0]), "docc_fp64": float(r64["docc"][0])},
             "mixed": {"hv_steps": res["lanczos_steps"] + res["green_steps"], "e0": res["e0"]},
         }
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    rep.close()
     ctx.close()
     if out is not None:
         print(json.dumps(out), flush=True)
