@@ -86,6 +86,72 @@ def star_model(eps_imp, U, eps_bath, V, orbital_of_bath=None, nc=1, Uprime=None,
     return AIMModel(nc, nb, ec, eb, vbc, u, jj, jhund=float(J), cutoff=cutoff)
 
 
+@dataclasses.dataclass
+class NambuModel:
+    """Superconducting AIM in the Nambu (Sz) basis: ``base`` plus the bath
+    pairing ``pb`` (nb x nb, Pb(k,k') of bath_class.f90:956-986) and, when the
+    reference's PAIRING_IMP_TO_BATH is on, the impurity-to-bath pairing
+    ``pvbc`` (2, nb, nc) (bath_class.f90:998-1022).  ``on_fly`` selects the
+    term order of HAIMsz_mult_fly_r (ed_solver/HAIMsz.f90:615-808) instead of
+    the tabulated HAIMsz_multr (ed_solver/HAIMsz.f90:453-589); the on-the-fly
+    order keeps every non-zero element (no cutoff_hamilt_param).
+
+    The sector of ``npart`` Nambu particles in 2*ns orbitals holds the states
+    with N_up + (ns - N_dn) = npart: up orbitals on bits 0..ns-1 as in one spin
+    species of the (N_up, N_dn) basis, down holes on bits ns..2ns-1.
+    Eigenvalues of the Nambu operator plus ``energy_shift`` are the physical
+    energies (eigen_sector_class.f90:329).
+    """
+    base: AIMModel
+    pb: np.ndarray
+    pvbc: Optional[np.ndarray] = None
+    on_fly: bool = False
+
+    @property
+    def nc(self) -> int:
+        return self.base.nc
+
+    @property
+    def nb(self) -> int:
+        return self.base.nb
+
+    @property
+    def ns(self) -> int:
+        return self.base.ns
+
+    @property
+    def energy_shift(self) -> float:
+        """energy_global_shift + energy_global_shift2: the down-spin diagonal of Ec and Eb."""
+        m = self.base
+        s1 = 0.0
+        for c in range(m.nc):
+            s1 += float(m.ec[1, c, c])
+        s2 = 0.0
+        for k in range(m.nb):
+            s2 += float(m.eb[1, k, k])
+        return s1 + s2
+
+
+def nambu_star_model(eps_imp, U, eps_bath, V, delta, cutoff=1e-3, on_fly=False, pvbc=None) -> NambuModel:
+    """One-orbital star AIM with an s-wave superconducting bath: Pb = diag(delta)."""
+    base = star_model(eps_imp, U, eps_bath, V, cutoff=cutoff)
+    delta = np.asarray(delta, dtype=np.float64)
+    pb = np.diag(np.broadcast_to(delta, (base.nb,)).copy())
+    return NambuModel(base, pb, None if pvbc is None else np.asarray(pvbc, np.float64), bool(on_fly))
+
+
+def nambu_workload(ns: int, seed: int = 7, on_fly: bool = False) -> NambuModel:
+    """Seeded one-orbital superconducting AIM with ns-1 bath sites: U=2 at half
+    filling, bath levels uniform in [-2,2], hybridisations in [0.2,0.5], pairing
+    amplitudes in [0.1,0.4] (numpy default_rng(seed), drawn in that order)."""
+    rng = np.random.default_rng(seed)
+    nb = ns - 1
+    eb = rng.uniform(-2.0, 2.0, nb)
+    v = rng.uniform(0.2, 0.5, nb)
+    d = rng.uniform(0.1, 0.4, nb)
+    return nambu_star_model(-1.0, 2.0, eb, v, d, on_fly=on_fly)
+
+
 # --------------------------------------------------------------------------
 # synthetic workloads
 # --------------------------------------------------------------------------

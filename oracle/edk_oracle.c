@@ -255,6 +255,7 @@ typedef struct orc_h {
     int umask[ORC_MAXNC * ORC_MAXNC];
     int offdiag_coulomb, hund;
     double jhund;
+    struct orc_sz *sz;             /* Nambu sector (HAIMsz) when non-NULL */
 } orc_h;
 
 static void build_spin(const orc_model *m, int spin, int np, orc_spin_table *t)
@@ -299,9 +300,12 @@ orc_h *orc_h_new(const orc_model *m, int nup, int ndn)
     return h;
 }
 
+static void orc_sz_free(struct orc_sz *z);
+
 void orc_h_free(orc_h *h)
 {
     if (!h) return;
+    if (h->sz) orc_sz_free(h->sz);
     for (int s = 0; s < 2; ++s) {
         free(h->t[s].st); free(h->t[s].ptr); free(h->t[s].tgt);
         free(h->t[s].val); free(h->t[s].diag);
@@ -343,8 +347,11 @@ static inline int between_sign(uint64_t s, int a, int b)
     return (__builtin_popcountll(s & mask) & 1) ? -1 : 1;
 }
 
+static void orc_sz_hmult(const struct orc_sz *z, const double *x, double *y);
+
 void orc_hmult(const orc_h *h, const double *x, double *y)
 {
+    if (h->sz) { orc_sz_hmult(h->sz, x, y); return; }
     const int nc = h->nc, nb = h->nb;
     const int64_t sec = h->dup, ddn = h->ddn;
     const orc_spin_table *tu = &h->t[0], *td = &h->t[1];
@@ -878,4 +885,365 @@ int orc_lanczos_steps(const orc_h *h, const double *v0, int nsteps, double *diag
     }
     free(vin); free(tmp); free(vout);
     return done;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Nambu (Sz) sectors: HAIMsz (HAIMsz.f90:51-1027)                            */
+/* ------------------------------------------------------------------------- */
+
+/* Superconducting bath on top of orc_model (bath_class.f90:956-1022):
+ * pb[k][k'] = Pb(k,k') (NULL = no pairing), pvbc[s][k][c] = PVbc_s(k,c)
+ * (NULL unless PAIRING_IMP_TO_BATH).  on_fly = 1 follows HAIMsz_mult_fly_r's
+ * order (HAIMsz.f90:615-808), 0 the tabulated HAIMsz_multr (:453-589). */
+typedef struct {
+    orc_model base;
+    const double *pb, *pvbc;
+    int32_t on_fly;
+} orc_model_sz;
+
+#define ORC_SZ_MAXNB 16
+
+typedef struct orc_sz {
+    int nc, nb, ns, npart, on_fly, nimp, nbath;   /* nimp = 2nc, nbath = 2nb Nambu orbitals */
+    int imp_bit[2 * ORC_MAXNC], bath_bit[2 * ORC_SZ_MAXNB];
+    double *ecn, *ebn, *vbcn;                     /* Nambu matrices, row-major */
+    double u[ORC_MAXNC * ORC_MAXNC];
+    int umask[ORC_MAXNC * ORC_MAXNC], offdiag_coulomb;
+    double cutoff, shift1, shift2;
+    int64_t dim;
+    uint64_t *st;                                 /* sector states, ascending */
+    double *quart;                                /* QUART_INT_SZ */
+    double *diag;                                 /* diagsz (tabulated order) */
+    int64_t *ptr, *tgt;                           /* offdiagsz CSR (tabulated order) */
+    double *val;
+} orc_sz;
+
+/* Position of s among the states of its popcount in increasing order
+ * (Hilbert%rank of new_fermion_Hilbert_space, quantum_fermion_hilbert_class.f90:385-404),
+ * through the combinatorial number system: sum over the i-th lowest set bit p_i of C(p_i, i+1). */
+int64_t orc_colex_rank(uint64_t s)
+{
+    int64_t r = 0;
+    int i = 0;
+    while (s) {
+        int p = __builtin_ctzll(s);
+        r += orc_binom(p, i + 1);
+        ++i;
+        s &= s - 1;
+    }
+    return r;
+}
+
+/* Nambu_Ec (impurity_class.f90:1018-1037), Nambu_Eb (bath_class.f90:956-986),
+ * Nambu_Vbc (bath_class.f90:998-1022); Nambu orbital order of new_AIM2
+ * (quantum_algebra_Anderson_Impurity_class2.f90:88-100): impurity up sites then
+ * impurity down sites (bits nb+c and ns+nb+c), bath up then bath down (bits k, ns+k). */
+static void sz_nambu(const orc_model_sz *m, orc_sz *z)
+{
+    const int nc = m->base.nc, nb = m->base.nb, ns = nc + nb, NI = 2 * nc, NB = 2 * nb;
+    const double *ec = m->base.ec, *eb = m->base.eb, *vb = m->base.vbc;
+    z->ecn = (double *)calloc((size_t)NI * NI, sizeof(double));
+    z->ebn = (double *)calloc((size_t)(NB > 0 ? NB * NB : 1), sizeof(double));
+    z->vbcn = (double *)calloc((size_t)(NB > 0 ? NB * NI : 1), sizeof(double));
+    for (int i = 0; i < nc; ++i) {
+        z->imp_bit[i] = nb + i;
+        z->imp_bit[nc + i] = ns + nb + i;
+        for (int j = 0; j < nc; ++j) {
+            z->ecn[i * NI + j] = ec[i * nc + j];
+            z->ecn[(nc + i) * NI + nc + j] = -ec[nc * nc + j * nc + i];
+        }
+    }
+    for (int k = 0; k < nb; ++k) {
+        z->bath_bit[k] = k;
+        z->bath_bit[nb + k] = ns + k;
+        for (int l = 0; l < nb; ++l) {
+            z->ebn[k * NB + l] = eb[k * nb + l];
+            z->ebn[(nb + k) * NB + nb + l] = -eb[nb * nb + l * nb + k];
+            if (m->pb) {
+                z->ebn[k * NB + nb + l] = m->pb[k * nb + l];
+                z->ebn[(nb + k) * NB + l] = m->pb[l * nb + k];
+            }
+        }
+        for (int c = 0; c < nc; ++c) {
+            z->vbcn[k * NI + c] = vb[k * nc + c];
+            z->vbcn[(nb + k) * NI + nc + c] = -vb[nb * nc + k * nc + c];
+            if (m->pvbc) {
+                z->vbcn[(nb + k) * NI + c] = m->pvbc[k * nc + c];
+                z->vbcn[k * NI + nc + c] = m->pvbc[nb * nc + k * nc + c];
+            }
+        }
+    }
+    /* energy_global_shift = sum(diag(Ec(2))), energy_global_shift2 =
+     * -sum(diag(lower block of EbNambu)); eigenvalues get + shift + shift2
+     * (eigen_sector_class.f90:329) */
+    double s1 = 0.0, s2 = 0.0;
+    for (int c = 0; c < nc; ++c) s1 = s1 + ec[nc * nc + c * nc + c];
+    for (int k = 0; k < nb; ++k) s2 = s2 + z->ebn[(nb + k) * NB + nb + k];
+    z->shift1 = s1;
+    z->shift2 = -s2;
+}
+
+static inline int sz_between_sign(uint64_t s, int a, int b) { return between_sign(s, a, b); }
+
+/* hop tgt <- src on s: 0 when nil; else target state and the Jordan-Wigner sign
+ * (hop, quantum_fermion_ket_class.f90:483-492: destroy then create) */
+static inline int sz_hop(uint64_t s, int tgt, int src, uint64_t *out, int *sign)
+{
+    return ket_hop(s, tgt, src, out, sign);
+}
+
+/* tab_HAIM2 for the Nambu AIM2 (HAIM_offdiag_arrays.f90:419-526): visits the
+ * off-diagonal targets of s in the tabulated order. */
+static int sz_visit(const orc_sz *z, uint64_t s, uint64_t *ts, double *tv)
+{
+    const int NI = z->nimp, NB = z->nbath;
+    int n = 0, sg;
+    uint64_t out;
+    for (int i = 0; i < NI; ++i)
+        for (int j = 0; j < NI; ++j) {
+            double h = z->ecn[i * NI + j];
+            if (i == j || h == 0.0 || !(fabs(h) > z->cutoff)) continue;
+            if (sz_hop(s, z->imp_bit[i], z->imp_bit[j], &out, &sg)) {
+                if (ts) { ts[n] = out; tv[n] = h * (double)sg; }
+                ++n;
+            }
+        }
+    for (int i = 0; i < NB; ++i)
+        for (int j = 0; j < NB; ++j) {
+            double h = z->ebn[i * NB + j];
+            if (i == j || h == 0.0 || !(fabs(h) > z->cutoff)) continue;
+            if (sz_hop(s, z->bath_bit[i], z->bath_bit[j], &out, &sg)) {
+                if (ts) { ts[n] = out; tv[n] = h * (double)sg; }
+                ++n;
+            }
+        }
+    for (int k = 0; k < NB; ++k)
+        for (int c = 0; c < NI; ++c) {
+            double h = z->vbcn[k * NI + c];
+            if (h == 0.0 || !(fabs(h) > z->cutoff)) continue;
+            if (sz_hop(s, z->bath_bit[k], z->imp_bit[c], &out, &sg)) {     /* impurity -> bath */
+                if (ts) { ts[n] = out; tv[n] = h * (double)sg; }
+                ++n;
+            }
+            if (sz_hop(s, z->imp_bit[c], z->bath_bit[k], &out, &sg)) {     /* bath -> impurity */
+                if (ts) { ts[n] = out; tv[n] = h * (double)sg; }
+                ++n;
+            }
+        }
+    return n;
+}
+
+/* QUART_INT_SZ of one state (tab_HAIMsz, HAIMsz.f90:106-177): the down
+ * occupation is the complement of the hole orbital's.  The Slater-type Hund
+ * term is not reached: HAIMsz_mult* stop when |Jhund| > 1e-5. */
+static double sz_quart(const orc_sz *z, uint64_t s)
+{
+    const int nc = z->nc;
+    double q = 0.0;
+    for (int s1 = 0; s1 < nc; ++s1) {
+        const int b1u = bt(s, z->imp_bit[s1]), b1d = !bt(s, z->imp_bit[nc + s1]);
+        const int n1 = b1u + b1d;
+        if (n1 == 2 && z->umask[s1 * nc + s1]) q = q + z->u[s1 * nc + s1];
+        if (z->offdiag_coulomb && n1 != 0)
+            for (int s2 = s1 + 1; s2 < nc; ++s2) {
+                if (!z->umask[s1 * nc + s2]) continue;
+                const int n2 = bt(s, z->imp_bit[s2]) + !bt(s, z->imp_bit[nc + s2]);
+                q = q + z->u[s1 * nc + s2] * (double)n1 * (double)n2;
+            }
+    }
+    return q;
+}
+
+static void orc_sz_free(orc_sz *z)
+{
+    if (!z) return;
+    free(z->ecn); free(z->ebn); free(z->vbcn); free(z->st); free(z->quart);
+    free(z->diag); free(z->ptr); free(z->tgt); free(z->val);
+    free(z);
+}
+
+/* new_HAIMsz (HAIMsz.f90:51-82) on the sector of `npart` Nambu particles in
+ * 2*ns orbitals (new_fermion_sector with norbs = 2*ns).  offdiag_coulomb is the
+ * intended "U has a non-zero off-diagonal element" (:68; the reference evaluates
+ * it before filling its is_diag mask). */
+orc_h *orc_h_new_sz(const orc_model_sz *m, int npart)
+{
+    const int nc = m->base.nc, nb = m->base.nb, ns = nc + nb;
+    if (nc < 1 || nc > ORC_MAXNC || nb < 0 || nb > ORC_SZ_MAXNB || 2 * ns > 32) return NULL;
+    if (npart < 0 || npart > 2 * ns) return NULL;
+    if (fabs(m->base.jhund) > 1e-5) return NULL;   /* HAIMsz.f90:470-473 */
+    orc_sz *z = (orc_sz *)calloc(1, sizeof(orc_sz));
+    z->nc = nc; z->nb = nb; z->ns = ns; z->npart = npart; z->on_fly = m->on_fly;
+    z->nimp = 2 * nc; z->nbath = 2 * nb;
+    z->cutoff = m->base.cutoff;
+    sz_nambu(m, z);
+    for (int i = 0; i < nc * nc; ++i) {
+        z->u[i] = m->base.u[i];
+        z->umask[i] = m->base.u[i] != 0.0;
+    }
+    for (int i = 0; i < nc; ++i)
+        for (int j = 0; j < nc; ++j)
+            if (i != j && z->umask[i * nc + j]) z->offdiag_coulomb = 1;
+    z->dim = orc_binom(2 * ns, npart);
+    const int64_t d = z->dim;
+    z->st = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)(d > 0 ? d : 1));
+    {
+        /* increasing order: next state of the same popcount (Gosper) */
+        uint64_t s = npart == 0 ? 0 : ((1ull << npart) - 1ull);
+        for (int64_t i = 0; i < d; ++i) {
+            z->st[i] = s;
+            if (s == 0) break;
+            uint64_t c = s & (~s + 1ull), r = s + c;
+            s = (((r ^ s) >> 2) / c) | r;
+        }
+    }
+    z->quart = (double *)malloc(sizeof(double) * (size_t)(d > 0 ? d : 1));
+    z->diag = (double *)malloc(sizeof(double) * (size_t)(d > 0 ? d : 1));
+    z->ptr = (int64_t *)malloc(sizeof(int64_t) * (size_t)(d + 1));
+    int64_t nnz = 0;
+    for (int64_t i = 0; i < d; ++i) nnz += sz_visit(z, z->st[i], NULL, NULL);
+    z->tgt = (int64_t *)malloc(sizeof(int64_t) * (size_t)(nnz > 0 ? nnz : 1));
+    z->val = (double *)malloc(sizeof(double) * (size_t)(nnz > 0 ? nnz : 1));
+    const int cap = z->nimp * z->nimp + z->nbath * z->nbath + 2 * z->nimp * z->nbath + 1;
+    uint64_t *ts = (uint64_t *)malloc(sizeof(uint64_t) * cap);
+    double *tv = (double *)malloc(sizeof(double) * cap);
+    z->ptr[0] = 0;
+    for (int64_t i = 0; i < d; ++i) {
+        const uint64_t s = z->st[i];
+        z->quart[i] = sz_quart(z, s);
+        double dg = 0.0;                                  /* HAIM_offdiag_arrays.f90:419-427 */
+        for (int o = 0; o < z->nimp; ++o)
+            if (bt(s, z->imp_bit[o])) dg = dg + z->ecn[o * z->nimp + o];
+        for (int o = 0; o < z->nbath; ++o)
+            if (bt(s, z->bath_bit[o])) dg = dg + z->ebn[o * z->nbath + o];
+        z->diag[i] = dg;
+        int n = sz_visit(z, s, ts, tv);
+        for (int e = 0; e < n; ++e) {
+            z->tgt[z->ptr[i] + e] = orc_colex_rank(ts[e]);
+            z->val[z->ptr[i] + e] = tv[e];
+        }
+        z->ptr[i + 1] = z->ptr[i] + n;
+    }
+    free(ts); free(tv);
+    orc_h *h = (orc_h *)calloc(1, sizeof(orc_h));
+    h->nc = nc; h->nb = nb; h->ns = ns;
+    h->dim = d; h->dup = d; h->ddn = 1;
+    h->sz = z;
+    return h;
+}
+
+double orc_sz_shift(const orc_h *h) { return h->sz ? h->sz->shift1 + h->sz->shift2 : 0.0; }
+
+/* Export per-state QUART_INT_SZ, diagsz and the CSR; any pointer may be NULL.
+ * Returns the entry count. */
+int64_t orc_sz_table(const orc_h *h, uint64_t *st, double *quart, double *diag, int64_t *ptr,
+                     int64_t *tgt, double *val)
+{
+    const orc_sz *z = h->sz;
+    if (!z) return -1;
+    const int64_t d = z->dim, nnz = z->ptr[d];
+    if (st) memcpy(st, z->st, sizeof(uint64_t) * d);
+    if (quart) memcpy(quart, z->quart, sizeof(double) * d);
+    if (diag) memcpy(diag, z->diag, sizeof(double) * d);
+    if (ptr) memcpy(ptr, z->ptr, sizeof(int64_t) * (d + 1));
+    if (tgt) memcpy(tgt, z->tgt, sizeof(int64_t) * nnz);
+    if (val) memcpy(val, z->val, sizeof(double) * nnz);
+    return nnz;
+}
+
+/* HAIMsz_multr with USE_CC (HAIMsz.f90:453-589) or HAIMsz_mult_fly_r
+ * (HAIMsz.f90:615-808), real FP64, sequential per element. */
+static void orc_sz_hmult(const orc_sz *z, const double *x, double *y)
+{
+    const int64_t d = z->dim;
+    const int NI = z->nimp, NB = z->nbath;
+    if (!z->on_fly) {
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < d; ++i) {
+            double v = z->quart[i] * x[i];
+            v = v + z->diag[i] * x[i];
+            for (int64_t e = z->ptr[i]; e < z->ptr[i + 1]; ++e) v = v + z->val[e] * x[z->tgt[e]];
+            y[i] = v;
+        }
+        return;
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < d; ++i) {
+        const uint64_t s = z->st[i];
+        double v = z->quart[i] * x[i];
+        for (int o = 0; o < NI; ++o)
+            if (bt(s, z->imp_bit[o])) v = v + z->ecn[o * NI + o] * x[i];
+        for (int o = 0; o < NB; ++o)
+            if (bt(s, z->bath_bit[o])) v = v + z->ebn[o * NB + o] * x[i];
+        /* one hop: source orbital a occupied, target b empty; sign from the
+         * occupied orbitals strictly between (:686-694) */
+#define SZ_FLY_HOP(a, b, hval)                                                     \
+        do {                                                                       \
+            const uint64_t o_ = (s & ~(1ull << (a)));                              \
+            if (!bt(o_, (b))) {                                                    \
+                const uint64_t t_ = o_ | (1ull << (b));                            \
+                const double hh_ = (hval) * (double)sz_between_sign(t_, (a), (b)); \
+                v = v + hh_ * x[orc_colex_rank(t_)];                               \
+            }                                                                      \
+        } while (0)
+        for (int j = 0; j < NI; ++j) {
+            if (!bt(s, z->imp_bit[j])) continue;
+            for (int o = 0; o < NI; ++o)
+                if (o != j && z->ecn[o * NI + j] != 0.0) SZ_FLY_HOP(z->imp_bit[j], z->imp_bit[o], z->ecn[o * NI + j]);
+        }
+        for (int j = 0; j < NB; ++j) {
+            if (!bt(s, z->bath_bit[j])) continue;
+            for (int o = 0; o < NB; ++o)
+                if (o != j && z->ebn[o * NB + j] != 0.0) SZ_FLY_HOP(z->bath_bit[j], z->bath_bit[o], z->ebn[o * NB + j]);
+        }
+        for (int j = 0; j < NI; ++j) {                  /* impurity -> bath (:733-760) */
+            if (!bt(s, z->imp_bit[j])) continue;
+            for (int o = 0; o < NB; ++o)
+                if (z->vbcn[o * NI + j] != 0.0) SZ_FLY_HOP(z->imp_bit[j], z->bath_bit[o], z->vbcn[o * NI + j]);
+        }
+        for (int o = 0; o < NB; ++o) {                  /* bath -> impurity (:762-790) */
+            if (!bt(s, z->bath_bit[o])) continue;
+            for (int j = 0; j < NI; ++j)
+                if (z->vbcn[o * NI + j] != 0.0) SZ_FLY_HOP(z->bath_bit[o], z->imp_bit[j], z->vbcn[o * NI + j]);
+        }
+#undef SZ_FLY_HOP
+        y[i] = v;
+    }
+}
+
+/* apply_Csz_updo / apply_Csz_N_updo (apply_C.f90:344-483) on a Nambu vector:
+ * physical c[+]_{site,spin}.  Spin up acts on the up orbital as written; spin
+ * down acts on the hole orbital with the roles of c and c+ exchanged (CASE(2)
+ * of :373-379).  projected = 1 is apply_Csz_N_updo: up only where the down
+ * orbital of the site is occupied (its hole empty), down only where the up
+ * orbital is occupied.  apply_Csz (:273-333) on Nambu orbital iorb is the
+ * spin-up case for iorb < nc and the spin-down case with dagger flipped for
+ * iorb >= nc.  out has binom(2ns, npart +/- 1) elements and is overwritten.
+ * Returns the target npart, or -1. */
+int orc_apply_csz(const orc_h *h, int site, int spin, int dagger, int projected, const double *in,
+                  double *out)
+{
+    const orc_sz *z = h->sz;
+    if (!z || site < 0 || site >= z->nc) return -1;
+    const int bit = spin == 0 ? z->imp_bit[site] : z->imp_bit[z->nc + site];
+    const int create = spin == 0 ? dagger : !dagger;
+    const int npt = z->npart + (create ? 1 : -1);
+    if (npt < 0 || npt > 2 * z->ns) return -1;
+    const int64_t dt = orc_binom(2 * z->ns, npt);
+    memset(out, 0, sizeof(double) * (size_t)dt);
+    for (int64_t i = 0; i < z->dim; ++i) {
+        if (in[i] == 0.0) continue;
+        const uint64_t s = z->st[i];
+        if (projected) {
+            const int nup = bt(s, z->imp_bit[site]), ndn = bt(s, z->imp_bit[z->nc + site]);
+            if (spin == 0 ? (ndn != 0) : (nup != 1)) continue;
+        }
+        uint64_t o;
+        int sg = 1;
+        const int ok = create ? ket_create(s, bit, &o, &sg) : ket_destroy(s, bit, &o, &sg);
+        if (!ok) continue;
+        const int64_t j = orc_colex_rank(o);
+        out[j] = out[j] + (double)sg * in[i];
+    }
+    return npt;
 }

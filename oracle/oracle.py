@@ -88,6 +88,16 @@ def lib():
         L.orc_num_threads.restype = i32
         L.orc_lanczos_steps.restype = i32
         L.orc_lanczos_steps.argtypes = [P, P, i32, P, P]
+        L.orc_h_new_sz.restype = P
+        L.orc_h_new_sz.argtypes = [P, i32]
+        L.orc_sz_shift.restype = d
+        L.orc_sz_shift.argtypes = [P]
+        L.orc_sz_table.restype = i64
+        L.orc_sz_table.argtypes = [P, P, P, P, P, P, P]
+        L.orc_apply_csz.restype = i32
+        L.orc_apply_csz.argtypes = [P, i32, i32, i32, i32, P, P]
+        L.orc_colex_rank.restype = i64
+        L.orc_colex_rank.argtypes = [C.c_uint64]
         _LIB = L
     return _LIB
 
@@ -393,6 +403,206 @@ def dense_sector_h(model: AIMModel, nup: int, ndn: int) -> np.ndarray:
                         if ru_ and rd_:
                             j = ru[ru_[1]] + rd[rd_[1]] * dup
                             H[j, i] += JJ[c, c2] * ru_[0] * rd_[0]
+    return H
+
+
+# ---------------------------------------------------------------------------
+# Nambu (Sz) sectors: HAIMsz (ed_solver/HAIMsz.f90:51-1027)
+# ---------------------------------------------------------------------------
+
+class _CModelSz(C.Structure):
+    _fields_ = [("base", _CModel), ("pb", C.c_void_p), ("pvbc", C.c_void_p), ("on_fly", C.c_int32)]
+
+
+def _cmodel_sz(m):
+    cm, arrs = _cmodel(m.base)
+    pb = np.ascontiguousarray(m.pb, np.float64)
+    pv = None if m.pvbc is None else np.ascontiguousarray(m.pvbc, np.float64)
+    cs = _CModelSz(cm, pb.ctypes.data, None if pv is None else pv.ctypes.data, int(bool(m.on_fly)))
+    return cs, (arrs, pb, pv)
+
+
+class OracleSz:
+    """new_HAIMsz / HAIMsz_mult for the sector of `npart` Nambu particles.
+
+    Usable wherever the oracle drivers take an OracleH (Lanczos passes, Green
+    chains): the C handle dispatches H*v to the Nambu operator."""
+
+    def __init__(self, model, npart: int):
+        self.model = model
+        self.npart = npart
+        cs, self._keep = _cmodel_sz(model)
+        self._cs = cs
+        self.h = lib().orc_h_new_sz(C.byref(cs), npart)
+        if not self.h:
+            raise ValueError("unsupported Nambu model or sector")
+        self.dim = int(lib().orc_h_dim(self.h))
+        self.shift = float(lib().orc_sz_shift(self.h))
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            lib().orc_h_free(h)
+            self.h = None
+
+    def hmult(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(self.dim, dtype=np.float64)
+        lib().orc_hmult(self.h, _p(x), _p(y))
+        return y
+
+    def table(self):
+        """(states, QUART_INT_SZ, diagsz, ptr, tgt, val) of the tabulated operator."""
+        d = self.dim
+        nnz = int(lib().orc_sz_table(self.h, None, None, None, None, None, None))
+        st = np.zeros(d, np.uint64)
+        q = np.zeros(d)
+        dg = np.zeros(d)
+        ptr = np.zeros(d + 1, np.int64)
+        tgt = np.zeros(max(nnz, 1), np.int64)
+        val = np.zeros(max(nnz, 1))
+        lib().orc_sz_table(self.h, _p(st), _p(q), _p(dg), _p(ptr), _p(tgt), _p(val))
+        return st, q, dg, ptr, tgt[:nnz], val[:nnz]
+
+    def dense(self) -> np.ndarray:
+        H = np.zeros((self.dim, self.dim))
+        e = np.zeros(self.dim)
+        for i in range(self.dim):
+            e[i] = 1.0
+            H[:, i] = self.hmult(e)
+            e[i] = 0.0
+        return H
+
+    def apply_c(self, vec: np.ndarray, site: int, spin: int, dagger: bool, projected: bool = False):
+        """apply_Csz_updo / apply_Csz_N_updo (apply_C.f90:344-483): (vector, target npart)."""
+        vec = np.ascontiguousarray(vec, np.float64)
+        create = bool(dagger) if spin == 0 else not dagger
+        npt = self.npart + (1 if create else -1)
+        if not 0 <= npt <= 2 * self.model.ns:
+            raise ValueError("target sector out of range")
+        out = np.zeros(binom(2 * self.model.ns, npt))
+        r = lib().orc_apply_csz(self.h, site, spin, int(bool(dagger)), int(bool(projected)), _p(vec), _p(out))
+        if r != npt:
+            raise ValueError("orc_apply_csz failed")
+        return out, npt
+
+
+def colex_rank(state: int) -> int:
+    return int(lib().orc_colex_rank(int(state)))
+
+
+def nambu_one_body(model) -> Tuple[np.ndarray, np.ndarray]:
+    """The Nambu one-body matrix over the 2*ns bits (numpy, from the physical
+    parameters): returns (h, bits) with h[a, b] the coefficient of b+_a b_b.
+    Down-spin entries enter particle-hole transformed: -t_dn^T."""
+    m = model.base
+    nc, nb, ns = m.nc, m.nb, m.ns
+    h = np.zeros((2 * ns, 2 * ns))
+    up = lambda o: o
+    hole = lambda o: ns + o
+    imp = lambda c: nb + c
+    for a in range(nc):
+        for b in range(nc):
+            h[up(imp(a)), up(imp(b))] += m.ec[0, a, b]
+            h[hole(imp(a)), hole(imp(b))] -= m.ec[1, b, a]
+    for k in range(nb):
+        for l in range(nb):
+            h[up(k), up(l)] += m.eb[0, k, l]
+            h[hole(k), hole(l)] -= m.eb[1, l, k]
+            h[up(k), hole(l)] += model.pb[k, l]
+            h[hole(l), up(k)] += model.pb[k, l]
+        for c in range(nc):
+            for (a, b, t) in ((up(k), up(imp(c)), m.vbc[0, k, c]), (hole(k), hole(imp(c)), -m.vbc[1, k, c])):
+                h[a, b] += t
+                h[b, a] += t
+            if model.pvbc is not None:
+                for (a, b, t) in ((hole(k), up(imp(c)), model.pvbc[0, k, c]),
+                                  (up(k), hole(imp(c)), model.pvbc[1, k, c])):
+                    h[a, b] += t
+                    h[b, a] += t
+    return h
+
+
+def dense_physical_sz(model, npart: int) -> np.ndarray:
+    """Physical Hamiltonian on the fixed-Sz subspace N_up - N_dn = npart - ns,
+    built from explicit fermion operators in an ordering unrelated to the Nambu
+    one (spin-orbital index 2*o + spin, Jordan-Wigner over that order):
+
+    H = sum_s t^s_ab c+_as c_bs + sum_kl Pb(k,l) (c+_k,up c+_l,dn + h.c.)
+      + sum_kc PVbc_1(k,c) (c+_c,up c+_k,dn + h.c.) + PVbc_2(k,c) (c+_k,up c+_c,dn + h.c.)
+      + sum_c U_cc n_c,up n_c,dn + sum_{c<c'} U_cc' n_c n_c'
+
+    with t^s collecting Ec, Eb, Vbc.  Its eigenvalues equal those of the Nambu
+    sector plus the energy shift."""
+    m = model.base
+    nc, nb, ns = m.nc, m.nb, m.ns
+    no = 2 * ns
+    idx = lambda o, s: 2 * o + s
+    states = [st for st in range(1 << no)
+              if sum((st >> idx(o, 0)) & 1 for o in range(ns)) - sum((st >> idx(o, 1)) & 1 for o in range(ns))
+              == npart - ns]
+    rk = {st: i for i, st in enumerate(states)}
+    D = len(states)
+    H = np.zeros((D, D))
+
+    def op(st, p, create):
+        occ = (st >> p) & 1
+        if occ == create:
+            return None
+        sg = -1 if bin(st & ((1 << p) - 1)).count("1") & 1 else 1
+        return sg, st ^ (1 << p)
+
+    def apply_seq(st, ops):
+        sg = 1
+        for p, cr in reversed(ops):
+            r = op(st, p, cr)
+            if r is None:
+                return None
+            sg *= r[0]
+            st = r[1]
+        return sg, st
+
+    terms = []     # (coef, [(p, create), ...]) applied right to left
+    imp = lambda c: nb + c
+    for s in range(2):
+        t = np.zeros((ns, ns))
+        t[nb:, nb:] = m.ec[s]
+        t[:nb, :nb] = m.eb[s]
+        t[:nb, nb:] = m.vbc[s]
+        t[nb:, :nb] = m.vbc[s].T
+        for a in range(ns):
+            for b in range(ns):
+                if t[a, b] != 0:
+                    terms.append((t[a, b], [(idx(a, s), 1), (idx(b, s), 0)]))
+    for k in range(nb):
+        for l in range(nb):
+            p = model.pb[k, l]
+            if p != 0:
+                terms.append((p, [(idx(k, 0), 1), (idx(l, 1), 1)]))
+                terms.append((p, [(idx(l, 1), 0), (idx(k, 0), 0)]))
+    if model.pvbc is not None:
+        for k in range(nb):
+            for c in range(nc):
+                p1, p2 = model.pvbc[0, k, c], model.pvbc[1, k, c]
+                if p1 != 0:
+                    terms.append((p1, [(idx(imp(c), 0), 1), (idx(k, 1), 1)]))
+                    terms.append((p1, [(idx(k, 1), 0), (idx(imp(c), 0), 0)]))
+                if p2 != 0:
+                    terms.append((p2, [(idx(k, 0), 1), (idx(imp(c), 1), 1)]))
+                    terms.append((p2, [(idx(imp(c), 1), 0), (idx(k, 0), 0)]))
+    for j, st in enumerate(states):
+        n = lambda o, s: (st >> idx(o, s)) & 1
+        e = 0.0
+        for c in range(nc):
+            e += m.u[c, c] * n(imp(c), 0) * n(imp(c), 1)
+            for c2 in range(c + 1, nc):
+                e += m.u[c, c2] * (n(imp(c), 0) + n(imp(c), 1)) * (n(imp(c2), 0) + n(imp(c2), 1))
+        H[j, j] += e
+        for coef, ops in terms:
+            r = apply_seq(st, ops)
+            if r is None:
+                continue
+            H[rk[r[1]], j] += coef * r[0]
     return H
 
 
