@@ -209,4 +209,64 @@ __device__ __forceinline__ void lanczos_finalize(const RowArgs &a, int k)
     if (a.kdev && a.mode == kModeStep) *a.kdev = k + 1;
 }
 
+
+// Per-launch scalars of the fused Lanczos step (kModeStep, see edk_kernels.cu):
+// s = w_k - gamma_k v_k was stored by the previous launch, delta_k = alpha_k -
+// gamma_k, and the new stored vector is s' = w_{k+1} - alpha_k v_{k+1}.
+struct StepScalars {
+    double delta = 0.0, gam = 0.0, gam1 = 0.0, beta_k = 0.0, beta_k1 = 0.0, inv_b = 0.0, cpsi = 0.0;
+};
+// false: a step launch after the chain ended (breakdown recorded earlier).
+__device__ __forceinline__ bool step_scalars(const RowArgs &a, int ks, StepScalars &sc)
+{
+    sc.gam1 = a.gamma1;
+    if (a.mode != kModeStep) return true;
+    sc.beta_k1 = a.tri_sub[ks];
+    if (!(sc.beta_k1 >= a.cutoff) || a.flags[0] != 0) return false;
+    const double alpha = a.tri_diag[ks - 1];
+    sc.gam = ks >= 2 ? a.tri_diag[ks - 2] : a.gamma1;
+    sc.delta = alpha - sc.gam;
+    sc.gam1 = alpha;
+    sc.beta_k = ks >= 2 ? a.tri_sub[ks - 1] : 0.0;
+    sc.inv_b = 1.0 / sc.beta_k1;
+    if (a.psi_coef) sc.cpsi = a.psi_coef[ks];
+    return true;
+}
+
+// Writes element i of the launch's outputs from acc = (H x)_i and x_i, and
+// adds its contribution to the reduction sums (the epilogue of every mode).
+template <typename T>
+__device__ __forceinline__ void row_epilogue(const RowArgs &a, const StepScalars &sc, int64_t i, double acc, T xo,
+                                             double &s0, double &s1, double &s2)
+{
+    if (a.mode == kModeHv) {
+        static_cast<T *>(a.y)[i] = (T)acc;
+    } else if (a.mode == kModeFirst) {
+        const double v = (double)xo;
+        const T st = (T)(acc - sc.gam1 * v);
+        static_cast<T *>(a.y)[i] = st;
+        const double sd = (double)st;
+        s0 += sd * sd; s1 += sd * v; s2 += v * v;
+    } else if (a.mode == kModeStep) {
+        const double sv = (double)xo;
+        const double vk = (double)static_cast<const T *>(a.vk)[i];
+        const double vm = a.vkm1 ? (double)static_cast<const T *>(a.vkm1)[i] : 0.0;
+        const T vt = (T)((sv - sc.delta * vk) * sc.inv_b);
+        const double hv1 = (acc - sc.delta * (sv + sc.gam * vk + sc.beta_k * vm)) * sc.inv_b;
+        const double w = hv1 - sc.beta_k1 * vk;
+        const T wt = (T)(w - sc.gam1 * (double)vt);
+        static_cast<T *>(a.y)[i] = wt;
+        static_cast<T *>(a.vout)[i] = vt;
+        if (a.psi) {
+            T *p = static_cast<T *>(a.psi) + i;
+            *p = (T)((double)*p + sc.cpsi * (double)vt);
+        }
+        const double wd = (double)wt, vd = (double)vt;
+        s0 += wd * wd; s1 += wd * vd; s2 += vd * vd;
+    } else {   // kModeResid
+        const double rr = acc - a.eshift * (double)xo;
+        s0 += rr * rr; s2 += (double)xo * (double)xo;
+    }
+}
+
 }  // namespace edk

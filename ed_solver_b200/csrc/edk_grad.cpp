@@ -38,6 +38,7 @@ void edk_internal_h_info(const edk_h *h, int *nc, int *nb, int *nup, int *ndn);
 void edk_internal_add_launches(edk_ctx *ctx, int64_t n);
 int edk_internal_h_sibling(edk_h *h, int nup, int ndn, edk_h **out);
 const uint64_t *edk_internal_h_states(const edk_h *h, int spin);
+int edk_internal_h_is_sz(const edk_h *h);
 }
 
 using namespace edk;
@@ -113,6 +114,7 @@ int ops_setup(edk_h *h, int np, const edk_param *prm, Ops &o)
     o.ctx = edk_internal_h_ctx(h);
     o.st = edk_internal_stream(o.ctx);
     if (np < 1 || np > kMaxGradParams || !prm) return o.fail(EDK_ERR_INVALID, "1..64 parameters");
+    if (edk_internal_h_is_sz(h)) return o.fail(EDK_ERR_UNSUPPORTED, "parameter gradients of a Nambu sector");
     int nc, nb, nup, ndn;
     edk_internal_h_info(h, &nc, &nb, &nup, &ndn);
     edk_h_dims(h, &o.dim, &o.dup, &o.ddn);

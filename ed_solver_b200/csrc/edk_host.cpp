@@ -227,6 +227,13 @@ struct edk_h {
     // fast-kernel launch shape per element type, chosen by timing on first use
     FastShape fast_shape[2];
     bool fast_tuned[2] = {false, false};
+    // Nambu (Sz) sector: its tables replace the (N_up, N_dn) ones
+    SzHost *sz = nullptr;
+    int npart = -1;
+    edk_h() = default;
+    edk_h(const edk_h &) = delete;
+    edk_h &operator=(const edk_h &) = delete;
+    ~edk_h() { if (sz) sz_destroy(sz); }
 };
 
 namespace {
@@ -366,15 +373,18 @@ int rows(edk_h *h, int dtype, const RowArgs &a)
 {
     edk_ctx *c = h->ctx;
     const int eb = dtype == EDK_F64 ? 8 : 4;
-    LaunchCfg cfg = plan_rows(h->H, eb, c->num_sms);
-    // the fast kernel uses 2-element vector accesses: every vector must be
-    // aligned to twice the element size
-    auto al = [&](const void *p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) % (2 * eb)) == 0; };
-    const bool aligned = al(a.x) && al(a.y) && al(a.vk) && al(a.vkm1) && al(a.vout) && al(a.psi);
-    cfg.fast = c->kernel_path != 1 && aligned && fast_rows_ok(h->H, eb);
-    if (cfg.fast) {
-        int rc = fast_shape_for(h, dtype, a, cfg.fast_shape);
-        if (rc) return rc;
+    LaunchCfg cfg;
+    if (!h->sz) {
+        cfg = plan_rows(h->H, eb, c->num_sms);
+        // the fast kernel uses 2-element vector accesses: every vector must be
+        // aligned to twice the element size
+        auto al = [&](const void *p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) % (2 * eb)) == 0; };
+        const bool aligned = al(a.x) && al(a.y) && al(a.vk) && al(a.vkm1) && al(a.vout) && al(a.psi);
+        cfg.fast = c->kernel_path != 1 && aligned && fast_rows_ok(h->H, eb);
+        if (cfg.fast) {
+            int rc = fast_shape_for(h, dtype, a, cfg.fast_shape);
+            if (rc) return rc;
+        }
     }
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;
     if (c->timing) {
@@ -382,7 +392,8 @@ int rows(edk_h *h, int dtype, const RowArgs &a)
         ev_b = c->get_event();
         cudaEventRecord(ev_a, c->stream);
     }
-    cudaError_t e = launch_rows(h->H, dtype, a, cfg, c->stream);
+    cudaError_t e = h->sz ? launch_sz_rows(sz_dev(h->sz), dtype, a, c->num_sms, c->stream)
+                          : launch_rows(h->H, dtype, a, cfg, c->stream);
     if (c->timing) {
         cudaEventRecord(ev_b, c->stream);
         c->timed.push_back({a.mode + (dtype == EDK_F32 ? 4 : 0), ev_a, ev_b, (double)h->dim});
@@ -758,6 +769,8 @@ void edk_internal_h_info(const edk_h *h, int *nc, int *nb, int *nup, int *ndn)
 
 void edk_internal_add_launches(edk_ctx *ctx, int64_t n) { ctx->launches += n; }
 
+int edk_internal_h_is_sz(const edk_h *h) { return h->sz ? 1 : 0; }
+
 // A Hamiltonian of another (nup, ndn) sector of the same model.
 int edk_internal_h_sibling(edk_h *h, int nup, int ndn, edk_h **out)
 {
@@ -927,6 +940,81 @@ int edk_h_create(edk_ctx *ctx, const edk_model *m, int nup, int ndn, edk_h **out
     return EDK_OK;
 }
 
+int edk_h_create_sz(edk_ctx *ctx, const edk_model_sz *m, int npart, edk_h **out)
+{
+    if (!ctx || !m || !out) return EDK_ERR_INVALID;
+    *out = nullptr;
+    std::unique_ptr<edk_h> h(new (std::nothrow) edk_h);
+    if (!h) return EDK_ERR_NOMEM;
+    h->ctx = ctx;
+    std::string err;
+    int rc = sz_create(m, npart, ctx->stream, &h->sz, &err);
+    if (rc) return ctx->fail(rc, "%s", err.c_str());
+    ModelHost &mh = h->model;
+    mh.nc = m->base.nc;
+    mh.nb = m->base.nb;
+    mh.jhund = m->base.jhund;
+    mh.cutoff = m->base.cutoff_hamilt_param;
+    h->npart = npart;
+    h->dim = sz_dev(h->sz).sec.dim;
+    h->dup = h->dim;
+    h->ddn = 1;
+    ctx->h2d_bytes += sz_upload_bytes(h->sz);
+    *out = h.release();
+    return EDK_OK;
+}
+
+int edk_h_sz_info(const edk_h *h, int32_t *npart, double *energy_shift)
+{
+    if (!h) return EDK_ERR_INVALID;
+    if (npart) *npart = h->sz ? h->npart : -1;
+    if (energy_shift) *energy_shift = h->sz ? sz_shift(h->sz) : 0.0;
+    return EDK_OK;
+}
+
+int edk_apply_csz(edk_h *src, int dtype, int site, int spin, int dagger, int projected, int site2, int sign2,
+                  const void *in_dev, void *out_dev, int64_t *out_dim, int32_t *out_npart)
+{
+    if (!src || !in_dev || !out_dev || spin < 0 || spin > 1 || (dtype != EDK_F64 && dtype != EDK_F32))
+        return EDK_ERR_INVALID;
+    edk_ctx *c = src->ctx;
+    if (!src->sz) return c->fail(EDK_ERR_INVALID, "edk_apply_csz needs a Nambu sector (edk_h_create_sz)");
+    const SzDev &S = sz_dev(src->sz);
+    if (site < 0 || site >= S.nc || site2 >= S.nc || site2 == site)
+        return c->fail(EDK_ERR_INVALID, "site outside the impurity (or site2 == site)");
+    const int ns = S.ns;
+    // spin up: the up orbital as written; spin down: the hole orbital with c, c+ exchanged
+    const int create = spin == 0 ? (dagger != 0) : (dagger == 0);
+    const int npt = src->npart + (create ? 1 : -1);
+    if (npt < 0 || npt > 2 * ns) return c->fail(EDK_ERR_INVALID, "target Nambu sector outside [0, 2 ns]");
+    std::string err;
+    const SzSectorDev *tgt = nullptr;
+    int rc = sz_sector(src->sz, npt, c->stream, &tgt, &err);
+    if (rc) return c->fail(rc, "%s", err.c_str());
+    auto op = [&](int st_site, int sgn) {
+        SzOp o;
+        const int up_bit = S.nb + st_site, hole_bit = ns + S.nb + st_site;
+        o.bit = 1u << (spin == 0 ? up_bit : hole_bit);
+        o.create = create;
+        o.sgn = sgn;
+        if (projected) {
+            // apply_Csz_N_updo (apply_C.f90:444-458): up needs the site's down
+            // occupied (hole empty), down needs its up occupied
+            o.pmask = 1u << (spin == 0 ? hole_bit : up_bit);
+            o.pwant = spin == 0 ? 0u : o.pmask;
+        }
+        return o;
+    };
+    SzOp ops[2] = {op(site, 1), SzOp()};
+    int nop = 1;
+    if (site2 >= 0) { ops[1] = op(site2, sign2 < 0 ? -1 : 1); nop = 2; }
+    if (out_dim) *out_dim = tgt->dim;
+    if (out_npart) *out_npart = npt;
+    rc = c->cuda(launch_sz_apply_c(dtype, S, *tgt, nop, ops, in_dev, out_dev, c->num_sms, c->stream), "apply_csz");
+    c->launches++;
+    return rc;
+}
+
 int edk_h_destroy(edk_h *h)
 {
     if (!h) return EDK_OK;
@@ -948,6 +1036,7 @@ int edk_h_table(const edk_h *h, int spin, int64_t *nnz, int64_t *ptr_host, int32
                 double *val_host, double *diag_host)
 {
     if (!h || spin < 0 || spin > 1) return EDK_ERR_INVALID;
+    if (h->sz) return h->ctx->fail(EDK_ERR_UNSUPPORTED, "a Nambu sector has no spin tables");
     const SpinTableHost &t = h->tab[spin];
     if (nnz) *nnz = (int64_t)t.tgt.size();
     if (ptr_host)
@@ -1142,6 +1231,7 @@ int edk_apply_c(edk_h *src, int dtype, int site, int spin, int dagger, int site2
 {
     if (!src || !in_dev || !out_dev || spin < 0 || spin > 1) return EDK_ERR_INVALID;
     edk_ctx *c = src->ctx;
+    if (src->sz) return c->fail(EDK_ERR_INVALID, "a Nambu sector takes edk_apply_csz");
     const ModelHost &m = src->model;
     if (site < 0 || site >= m.nc || site2 >= m.nc) return c->fail(EDK_ERR_INVALID, "site outside impurity");
     const int ns = m.nc + m.nb;
@@ -1284,6 +1374,7 @@ int edk_double_occ(edk_h *h, int dtype, const void *psi_dev, int site, double *d
 {
     if (!h || !psi_dev || site < 0 || site >= h->model.nc) return EDK_ERR_INVALID;
     edk_ctx *c = h->ctx;
+    if (h->sz) return c->fail(EDK_ERR_UNSUPPORTED, "double occupancy of a Nambu sector");
     int rc = c->cuda(launch_double_occ(dtype, h->H, 1 << site, 1 << site, psi_dev, c->partials.as<double>(),
                                        c->counter.as<unsigned>(), c->sums.as<double>() + 4, c->reduce_grid,
                                        c->stream), "double occ");
@@ -1335,6 +1426,10 @@ extern "C" int edk_green_batch(edk_ctx *c, int dtype, int32_t nchain, const edk_
     for (int i = 0; i < nchain; ++i)
         if (!ch[i].target || !ch[i].start_dev || ch[i].out < 0 || ch[i].out >= nout || (ch[i].iph != 1 && ch[i].iph != 2))
             return c->fail(EDK_ERR_INVALID, "chain %d: bad target/start/out/iph", i);
+    if (mode != 1)
+        for (int i = 0; i < nchain; ++i)
+            if (ch[i].target->sz)
+                return c->fail(EDK_ERR_UNSUPPORTED, "chain %d: Nambu targets run with mode 1", i);
     cudaStream_t st = c->stream;
     int rc;
     if (mode == 1) {

@@ -122,6 +122,66 @@ cudaError_t launch_batch(int dtype, int R, const HamDev *hams, const BatchItem *
                          cudaStream_t st);
 int batch_max_blocks_per_sm(int dtype, int R, int block, int64_t maxdup);
 
+// ---- Nambu (Sz) sectors (edk_sz.cpp, edk_sz.cu) ----------------------------
+// A Nambu state is 2*ns bits: low half l = up orbitals, high half h = down
+// holes.  The states of popcount npart in increasing order group into rows
+// of equal h (ascending); inside a row the low halves of popcount
+// npart - |h| run in increasing order, so rank = off_h[h] + rank_low[l].
+constexpr int kMaxSzNs = 16;
+constexpr int kMaxSzTerms = 4096;
+
+// One off-diagonal term c+_tgt c_src in the reference's visiting order.
+struct SzTerm {
+    uint32_t src, tgt;     // single-bit masks
+    uint32_t btw;          // orbitals strictly between: their parity is the Jordan-Wigner sign
+    uint32_t pad;
+    double h;
+};
+
+struct SzSectorDev {
+    int npart = 0, nrows = 0, maxlen = 0;
+    int64_t dim = 0;
+    const uint32_t *row_h = nullptr;   // nrows high halves present in the sector, ascending
+    const uint32_t *off_h = nullptr;   // 2^ns: rank of the first state of high half h
+};
+
+struct SzDev {
+    int ns = 0, nb = 0, nc = 0;
+    int order = 0;                          // 0: HAIMsz_multr, 1: HAIMsz_mult_fly_r
+    SzSectorDev sec;
+    const uint16_t *rank_low = nullptr;     // 2^ns: rank of l among the low halves of its popcount
+    const uint16_t *low_states = nullptr;   // 2^ns low halves grouped by popcount, ascending
+    const int32_t *class_start = nullptr;   // ns+2: start of popcount class k in low_states
+    int nterm = 0;
+    const SzTerm *terms = nullptr;
+    int ndiag = 0;                          // Nambu orbitals in the order of the diagonal sum
+    const uint32_t *diag_bit = nullptr;
+    const double *diag_e = nullptr;
+    const double *quart = nullptr;          // 4^nc: QUART_INT_SZ by impurity configuration
+                                            // (up bits | hole bits << nc)
+};
+
+struct SzHost;   // host tables and device copies of one Nambu sector (edk_sz.cpp)
+int sz_create(const edk_model_sz *m, int npart, cudaStream_t st, SzHost **out, std::string *err);
+void sz_destroy(SzHost *z);
+const SzDev &sz_dev(const SzHost *z);
+double sz_shift(const SzHost *z);
+int64_t sz_upload_bytes(const SzHost *z);
+// Row tables of the sector npart (another sector of the same model), cached
+// on z; used for the targets of c and c+.
+int sz_sector(SzHost *z, int npart, cudaStream_t st, const SzSectorDev **out, std::string *err);
+
+cudaError_t launch_sz_rows(const SzDev &S, int dtype, const RowArgs &a, int num_sms, cudaStream_t st);
+// out[t] over the target sector = sum over the (one or two) operators of
+// sign * in[source(t)]; operator o: bit[o] toggled, create[o] (the target has
+// the bit), source states with (s & pmask[o]) == pwant[o] only, sgn[o] = +-1.
+struct SzOp {
+    uint32_t bit = 0, pmask = 0, pwant = 0;
+    int create = 0, sgn = 1;
+};
+cudaError_t launch_sz_apply_c(int dtype, const SzDev &src, const SzSectorDev &tgt, int nop, const SzOp *ops,
+                              const void *in, void *out, int num_sms, cudaStream_t st);
+
 // ---- kernel launchers (edk_kernels.cu) ------------------------------------
 LaunchCfg plan_rows(const HamDev &H, int elem_bytes, int num_sms);
 cudaError_t launch_rows(const HamDev &H, int dtype, const RowArgs &a, const LaunchCfg &cfg,

@@ -1,0 +1,185 @@
+// Device kernels of the Nambu (Sz) sectors: H*v of HAIMsz_multr /
+// HAIMsz_mult_fly_r (HAIMsz.f90:453-808) fused with the Lanczos modes of the
+// row kernel, and c / c+ of apply_Csz_updo / apply_Csz_N_updo
+// (apply_C.f90:344-483).
+//
+// One thread block per row of equal high half h (the down holes), threads
+// over the row's low halves, so the x reads of the own row and of targets
+// that keep h are coalesced.  Per element:
+//   acc = QUART_INT_SZ * x                               (table by impurity configuration)
+//   tabulated order: acc += (sum of the occupied orbitals' diagonal energies) * x
+//   on-the-fly order: acc += e_o * x for each occupied orbital o in turn
+//   acc += (+-t) * x[rank(target)] for each term c+_tgt c_src in the list whose
+//          source is occupied and target empty (sign: parity of the occupied
+//          orbitals strictly between)
+// in the reference's order with separate multiply and add, so the FP64 result
+// equals a sequential FP64 evaluation bit for bit.
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "edk_internal.h"
+#include "edk_device.cuh"
+
+namespace edk {
+
+namespace {
+
+constexpr int kSzBlock = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(kSzBlock) sz_row_kernel(const SzDev S, const RowArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SzTerm *ts = reinterpret_cast<SzTerm *>(smem_raw);
+    const int nq = 1 << (2 * S.nc);
+    double *qs = reinterpret_cast<double *>(ts + S.nterm);
+    double *des = qs + nq;
+    uint32_t *dbs = reinterpret_cast<uint32_t *>(des + S.ndiag);
+    for (int t = threadIdx.x; t < S.nterm; t += blockDim.x) ts[t] = S.terms[t];
+    for (int t = threadIdx.x; t < nq; t += blockDim.x) qs[t] = S.quart[t];
+    for (int t = threadIdx.x; t < S.ndiag; t += blockDim.x) { des[t] = S.diag_e[t]; dbs[t] = S.diag_bit[t]; }
+
+    const int ks = step_index(a);
+    StepScalars sc;
+    if (!step_scalars(a, ks, sc)) return;
+    __syncthreads();
+
+    const T *__restrict__ x = static_cast<const T *>(a.x);
+    const int ns = S.ns, nb = S.nb, nc = S.nc, nterm = S.nterm, ndiag = S.ndiag;
+    const uint32_t lowmask = (1u << ns) - 1u, cm = (1u << nc) - 1u;
+    const uint32_t *__restrict__ off_h = S.sec.off_h;
+    const uint16_t *__restrict__ rank_low = S.rank_low;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int r = blockIdx.x; r < S.sec.nrows; r += gridDim.x) {
+        const uint32_t h = S.sec.row_h[r];
+        const int k = S.sec.npart - __popc(h);
+        const int c0 = S.class_start[k], len = S.class_start[k + 1] - c0;
+        const int64_t base = off_h[h];
+        const uint32_t hs = h << ns;
+        for (int c = threadIdx.x; c < len; c += blockDim.x) {
+            const uint32_t s = (uint32_t)S.low_states[c0 + c] | hs;
+            const int64_t i = base + c;
+            const T xo = x[i];
+            const uint32_t cfg = ((s >> nb) & cm) | (((s >> (ns + nb)) & cm) << nc);
+            double acc = fmul(qs[cfg], (double)xo);
+            if (S.order == 0) {
+                double d = 0.0;
+                for (int o = 0; o < ndiag; ++o)
+                    if (s & dbs[o]) d = fadd(d, des[o]);
+                acc = hmadd<T>(acc, d, xo);
+            } else {
+                for (int o = 0; o < ndiag; ++o)
+                    if (s & dbs[o]) acc = hmadd<T>(acc, des[o], xo);
+            }
+            for (int t = 0; t < nterm; ++t) {
+                const uint32_t src = ts[t].src, tgt = ts[t].tgt;
+                if (!(s & src) || (s & tgt)) continue;
+                const uint32_t s2t = s ^ src ^ tgt;
+                const int64_t j = (int64_t)off_h[s2t >> ns] + rank_low[s2t & lowmask];
+                const double hv = (__popc(s & ts[t].btw) & 1) ? -ts[t].h : ts[t].h;
+                acc = hmadd<T>(acc, hv, __ldg(x + j));
+            }
+            row_epilogue<T>(a, sc, i, acc, xo, s0, s1, s2);
+        }
+    }
+    if (a.mode == kModeHv) return;
+    double v[4] = {s0, s1, s2, 0.0};
+    if (grid_sum<4>(v, a.partials, a.counter, a.sums_out))
+        if (a.mode == kModeFirst || a.mode == kModeStep) lanczos_finalize(a, ks);
+}
+
+// Gather form of the reference's scatter: every target state looks up its
+// source; the map is one-to-one, so each target receives at most one term per
+// operator, in operator order.
+template <typename T>
+__global__ void sz_apply_c_kernel(const SzDev S, const SzSectorDev tgt, int nop, SzOp o0, SzOp o1,
+                                  const T *__restrict__ in, T *__restrict__ out)
+{
+    const int ns = S.ns;
+    const uint32_t lowmask = (1u << ns) - 1u;
+    for (int r = blockIdx.x; r < tgt.nrows; r += gridDim.x) {
+        const uint32_t h = tgt.row_h[r];
+        const int k = tgt.npart - __popc(h);
+        const int c0 = S.class_start[k], len = S.class_start[k + 1] - c0;
+        const int64_t base = tgt.off_h[h];
+        for (int c = threadIdx.x; c < len; c += blockDim.x) {
+            const uint32_t t = (uint32_t)S.low_states[c0 + c] | (h << ns);
+            T acc = T(0);
+            for (int q = 0; q < nop; ++q) {
+                const SzOp o = q == 0 ? o0 : o1;
+                if (((t & o.bit) != 0u) != (o.create != 0)) continue;
+                const uint32_t s = t ^ o.bit;
+                if ((s & o.pmask) != o.pwant) continue;
+                // create / destroy sign: occupied orbitals above the bit, on the result
+                const uint32_t above = t & ~((o.bit << 1) - 1u);
+                const int sg = (__popc(above) & 1) ? -o.sgn : o.sgn;
+                const T v = in[(int64_t)S.sec.off_h[s >> ns] + S.rank_low[s & lowmask]];
+                if (q == 0) acc = sg > 0 ? v : -v;
+                else acc = sg > 0 ? fadd(acc, v) : fsub(acc, v);
+            }
+            out[base + c] = acc;
+        }
+    }
+}
+
+size_t sz_smem(const SzDev &S)
+{
+    return (size_t)S.nterm * sizeof(SzTerm) + sizeof(double) * ((size_t)1 << (2 * S.nc)) +
+           (size_t)S.ndiag * (sizeof(double) + sizeof(uint32_t));
+}
+
+int sz_block(int maxlen)
+{
+    int b = ((maxlen + 31) / 32) * 32;
+    if (b > kSzBlock) b = kSzBlock;
+    if (b < 32) b = 32;
+    return b;
+}
+
+}  // namespace
+
+cudaError_t launch_sz_rows(const SzDev &S, int dtype, const RowArgs &a, int num_sms, cudaStream_t st)
+{
+    const size_t smem = sz_smem(S);
+    const int block = sz_block(S.sec.maxlen);
+    int per_sm = 2048 / block;
+    if (per_sm > 16) per_sm = 16;
+    int grid = num_sms * per_sm;
+    if (grid > S.sec.nrows) grid = S.sec.nrows;
+    if (grid < 1) grid = 1;
+    if (dtype == EDK_F64) {
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(sz_row_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess) return e;
+        }
+        sz_row_kernel<double><<<grid, block, smem, st>>>(S, a);
+    } else {
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(sz_row_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess) return e;
+        }
+        sz_row_kernel<float><<<grid, block, smem, st>>>(S, a);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sz_apply_c(int dtype, const SzDev &src, const SzSectorDev &tgt, int nop, const SzOp *ops,
+                              const void *in, void *out, int num_sms, cudaStream_t st)
+{
+    if (nop < 1 || nop > 2) return cudaErrorInvalidValue;
+    const SzOp o0 = ops[0], o1 = nop > 1 ? ops[1] : SzOp();
+    const int block = sz_block(tgt.maxlen);
+    int grid = num_sms * (2048 / block);
+    if (grid > tgt.nrows) grid = tgt.nrows;
+    if (grid < 1) grid = 1;
+    if (dtype == EDK_F64)
+        sz_apply_c_kernel<double><<<grid, block, 0, st>>>(src, tgt, nop, o0, o1, static_cast<const double *>(in),
+                                                          static_cast<double *>(out));
+    else
+        sz_apply_c_kernel<float><<<grid, block, 0, st>>>(src, tgt, nop, o0, o1, static_cast<const float *>(in),
+                                                         static_cast<float *>(out));
+    return cudaGetLastError();
+}
+
+}  // namespace edk

@@ -44,6 +44,10 @@ class _Model(C.Structure):
                 ("jhund", C.c_double), ("cutoff_hamilt_param", C.c_double)]
 
 
+class _ModelSz(C.Structure):
+    _fields_ = [("base", _Model), ("pb", C.c_void_p), ("pvbc", C.c_void_p), ("on_fly", C.c_int32)]
+
+
 class _LanczosOpts(C.Structure):
     _fields_ = [("nitermax", C.c_int32), ("neigen", C.c_int32), ("tolerance", C.c_double),
                 ("demax", C.c_double), ("cutoff_min_lanczos_vec", C.c_double), ("dtype", C.c_int32),
@@ -194,6 +198,10 @@ def lib():
         "edk_block_lanczos": (C.c_int, [P, P, P, P, P, P]),
         "edk_grad_e0": (C.c_int, [P, P, I32, P, P]),
         "edk_grad_green": (C.c_int, [P, P, D, I32, P, I32, I32, P, P, D, I32, P, D, P, P, P]),
+        "edk_h_create_sz": (C.c_int, [P, P, C.c_int, P]),
+        "edk_h_sz_info": (C.c_int, [P, P, P]),
+        "edk_apply_csz": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, P, P,
+                                    P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -216,6 +224,15 @@ def model_struct(m: AIMModel):
     arrs = m.arrays()
     s = _Model(m.nc, m.nb, *[a.ctypes.data for a in arrs], float(m.jhund), float(m.cutoff))
     return s, arrs
+
+
+def model_struct_sz(m):
+    """edk_model_sz of a NambuModel (keeps the arrays alive through the second value)."""
+    base, arrs = model_struct(m.base)
+    pb = np.ascontiguousarray(m.pb, np.float64)
+    pv = None if m.pvbc is None else np.ascontiguousarray(m.pvbc, np.float64)
+    s = _ModelSz(base, pb.ctypes.data, None if pv is None else pv.ctypes.data, int(bool(m.on_fly)))
+    return s, (arrs, pb, pv)
 
 
 # ---------------------------------------------------------------------------
@@ -552,6 +569,43 @@ class Hamiltonian:
                                              sd.ctypes.data, C.byref(nd)), "edk_green_chain")
         n = nd.value
         return G[0::2] + 1j * G[1::2], dg[:n].copy(), sd[:n].copy(), n
+
+
+class HamiltonianSz(Hamiltonian):
+    """One Nambu (Sz) sector Hamiltonian on the device (new_HAIMsz, HAIMsz.f90:51-82):
+    `npart` Nambu particles in 2*ns orbitals.  H*v, both Lanczos passes, Green
+    chains, residuals and block Lanczos work as for an (N_up, N_dn) sector;
+    physical energies are eigenvalues + ``energy_shift``."""
+
+    def __init__(self, ctx: Context, model, npart: int):
+        self.ctx = ctx
+        self.model = model
+        self.npart = npart
+        self.nup = self.ndn = None
+        ms, self._keep = model_struct_sz(model)
+        h = C.c_void_p()
+        ctx.check(lib().edk_h_create_sz(ctx.h, C.byref(ms), npart, C.byref(h)), "edk_h_create_sz")
+        self.h = h
+        d, du, dd = C.c_int64(), C.c_int64(), C.c_int64()
+        lib().edk_h_dims(h, C.byref(d), C.byref(du), C.byref(dd))
+        self.dim, self.dup, self.ddn = d.value, du.value, dd.value
+        n, sh = C.c_int32(), C.c_double()
+        lib().edk_h_sz_info(h, C.byref(n), C.byref(sh))
+        self.energy_shift = sh.value
+
+    def apply_c(self, vec, site, spin, dagger, site2=-1, sign2=1, projected=False):
+        """apply_Csz_updo (projected: apply_Csz_N_updo) -> (tensor in the target sector, npart')."""
+        import torch
+        create = bool(dagger) if spin == 0 else not dagger
+        npt = self.npart + (1 if create else -1)
+        if not 0 <= npt <= 2 * self.model.ns:
+            raise ValueError("target sector outside the Hilbert space")
+        out = torch.empty(binom(2 * self.model.ns, npt), dtype=vec.dtype, device=vec.device)
+        od, on = C.c_int64(), C.c_int32()
+        self.ctx.check(lib().edk_apply_csz(self.h, _dtype_code(vec.dtype), site, spin, int(bool(dagger)),
+                                           int(bool(projected)), site2, sign2, _ptr(vec), _ptr(out),
+                                           C.byref(od), C.byref(on)), "edk_apply_csz")
+        return out, on.value
 
 
 def cf_eval(ctx: Context, chains, wn, ld=None):

@@ -384,6 +384,51 @@ typedef struct edk_solve_result {
 
 int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_solve_result *r);
 
+/* ---- Nambu (Sz) sectors: HAIMsz (HAIMsz.f90:51-1027) ----------------------
+ * The superconducting basis of new_HAIMsz: one species of 2*ns orbitals, up
+ * orbitals on bits 0..ns-1 (bath k -> bit k, impurity c -> bit nb+c) and the
+ * particle-hole transformed down orbitals on bits ns..2ns-1 (a set bit is an
+ * empty down orbital).  The sector of npart Nambu particles holds the states
+ * of popcount npart (N_up + ns - N_dn = npart) in increasing order; vectors
+ * have binom(2ns, npart) elements.  The Nambu matrices are those of
+ * Nambu_Ec / Nambu_Eb / Nambu_Vbc (impurity_class.f90:1018-1037,
+ * bath_class.f90:956-1022): [Ec_up, 0; 0, -Ec_dn^T], [Eb_up, Pb; Pb^T, -Eb_dn^T],
+ * [Vbc_up, PVbc_2; PVbc_1, -Vbc_dn].  Physical energies are the Nambu
+ * eigenvalues plus energy_shift = sum_c Ec_dn(c,c) + sum_k Eb_dn(k,k)
+ * (eigen_sector_class.f90:329).  Requires ns <= 16, |jhund| <= 1e-5 (the
+ * reference STOPs otherwise, HAIMsz.f90:470-473). */
+typedef struct edk_model_sz {
+    edk_model base;              /* normal part (jj unused) */
+    const double *pb;            /* [nb][nb] bath pairing Pb(k,k'); NULL = none */
+    const double *pvbc;          /* [2][nb][nc] impurity-to-bath pairing PVbc_s(k,c) of
+                                    PAIRING_IMP_TO_BATH; NULL = off */
+    int32_t on_fly;              /* 0: term order of the tabulated HAIMsz_multr (HAIMsz.f90:453-589),
+                                    off-diagonal terms with |t| <= cutoff dropped; 1: order of
+                                    HAIMsz_mult_fly_r (HAIMsz.f90:615-808), every non-zero term */
+} edk_model_sz;
+
+/* new_H for a Nambu sector.  The handle works with edk_hmult(_host),
+ * edk_lanczos_e0/gs, edk_green_chain, edk_residual and edk_block_lanczos
+ * like an (N_up, N_dn) one; edk_h_dims reports dim_up = dim, dim_dn = 1.
+ * In EDK_F64, H*v adds per element in the reference's order of the selected
+ * variant, bit-identical to a sequential FP64 evaluation. */
+int edk_h_create_sz(edk_ctx *ctx, const edk_model_sz *m, int npart, edk_h **out);
+/* npart (-1 for an (N_up, N_dn) sector) and energy_shift (0 there). */
+int edk_h_sz_info(const edk_h *h, int32_t *npart, double *energy_shift);
+/* apply_Csz_updo / apply_Csz_N_updo (apply_C.f90:344-483): physical
+ * c[+]_{site,spin} on a Nambu vector.  Spin 0 creates (dagger = 1) or
+ * destroys on the up orbital; spin 1 acts on the hole orbital with c and c+
+ * exchanged (c+_dn empties the hole).  projected = 1 (apply_Csz_N_updo) keeps
+ * only source states whose other spin on the site is occupied.  apply_Csz
+ * (:273-333) on Nambu orbital iorb is site iorb, spin 0 for iorb < nc, and
+ * site iorb-nc, spin 1, dagger flipped for iorb >= nc.  site2 >= 0 adds
+ * sign2 * the same operator on site2.  out_dev (same dtype, fully
+ * overwritten) lives in the sector npart +/- 1: binom(2ns, npart +/- 1)
+ * elements, returned in out_dim; its Hamiltonian is edk_h_create_sz with
+ * the returned *out_npart. */
+int edk_apply_csz(edk_h *src, int dtype, int site, int spin, int dagger, int projected, int site2, int sign2,
+                  const void *in_dev, void *out_dev, int64_t *out_dim, int32_t *out_npart);
+
 #ifdef __cplusplus
 }
 #endif
