@@ -392,6 +392,88 @@ def run_c4(args):
     ctx.close()
 
 
+def run_sz(args):
+    """Nambu (Sz) sectors: H*v (on-the-fly term order, HAIMsz_mult_fly_r) and
+    fused Lanczos steps of the half-filled sector of the one-orbital
+    superconducting star model (seeded synthetic bath, s-wave pairing on every
+    bath site) at ns = 14 (40,116,600 states)
+    and ns = 16 (601,080,390 states), FP64 and FP32 vectors, timed with CUDA
+    events on the context's stream (inputs larger than L2).  Algorithmic bytes
+    per state: H*v reads x and writes y (2 elements); a fused step reads s,
+    v_k, v_k-1 and writes s', v_k+1 (5 elements).  The CPU oracle's H*v
+    (OpenMP, all host threads) is timed once at ns = 14 beside it."""
+    import numpy as np
+    import torch
+    from ed_solver_b200 import edk
+    from ed_solver_b200.model import nambu_workload
+    peak, peak_kind = _peaks()
+    ctx = edk.Context(0)
+    out = {"workload": "nambu_star_halffilled", "peak_hbm_gbs": peak, "peak": peak_kind, "cases": []}
+    for ns in (14, 16):
+        m = nambu_workload(ns, on_fly=True)
+        h = edk.HamiltonianSz(ctx, m, ns)
+        for dt, eb in (("f64", 8), ("f32", 4)):
+            tdt = torch.float64 if dt == "f64" else torch.float32
+            x = torch.randn(h.dim, dtype=tdt, device="cuda")
+            y = torch.empty_like(x)
+            for _ in range(3):
+                h.hmult(x, out=y)
+            ctx.timing(True)
+            for _ in range(max(args.steps, 5)):
+                h.hmult(x, out=y)
+            cls = 0 + (4 if dt == "f32" else 0)
+            n, ms, el = ctx.timing_report(cls)
+            ctx.timing(False)
+            hv_ms = ms / max(n, 1)
+            del x, y
+            torch.cuda.empty_cache()
+            ctx.timing(True)
+            r = h.lanczos_e0(dt, nitermax=24, tolerance=0.0, check_every=24)
+            ns_, ms_s, _ = ctx.timing_report(2 + (4 if dt == "f32" else 0))
+            ctx.timing(False)
+            st_ms = ms_s / max(ns_, 1)
+            case = {"ns": ns, "dim": h.dim, "dtype": dt,
+                    "hv_ms": hv_ms, "hv_gbs": 2 * eb * h.dim / hv_ms * 1e-6,
+                    "step_ms": st_ms, "step_gbs": 5 * eb * h.dim / st_ms * 1e-6, "step_launches": ns_,
+                    "e0_24_steps": float(r["E"][0]) + h.energy_shift}
+            case["hv_frac"] = case["hv_gbs"] / peak
+            case["step_frac"] = case["step_gbs"] / peak
+            out["cases"].append(case)
+            print(json.dumps(case), flush=True)
+        h.close()
+        torch.cuda.empty_cache()
+    if not args.no_cpu:
+        import oracle as O
+        m = nambu_workload(14, on_fly=True)
+        ho = O.OracleSz(m, 14)
+        xv = np.random.default_rng(0).standard_normal(ho.dim)
+        t0 = time.perf_counter()
+        ho.hmult(xv)
+        t1 = time.perf_counter()
+        out["cpu_oracle_hv_ms_ns14"] = (t1 - t0) * 1e3
+        out["cpu_threads"] = O.num_threads()
+    print(json.dumps(out), flush=True)
+    ctx.close()
+
+
+def run_sz_case(args):
+    """Three FP64 H*v launches of the ns = 14 half-filled Nambu sector (0.64 GB
+    of vectors): the small case for per-kernel ncu captures of the Nambu kernel."""
+    import torch
+    from ed_solver_b200 import edk
+    from ed_solver_b200.model import nambu_workload
+    ctx = edk.Context(0)
+    h = edk.HamiltonianSz(ctx, nambu_workload(14, on_fly=True), 14)
+    x = torch.randn(h.dim, dtype=torch.float64, device="cuda")
+    y = torch.empty_like(x)
+    for _ in range(3):
+        h.hmult(x, out=y)
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel_case": "ns14 Nambu FP64 H*v", "dim": h.dim}), flush=True)
+    h.close()
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -405,7 +487,16 @@ def main():
                     help="time the 32 parameter gradients of E0 + G and check them by central differences")
     ap.add_argument("--grad-fd", type=int, default=4, help="parameters checked by central differences (--grad)")
     ap.add_argument("--c4", action="store_true", help="time the many-small-sectors solve, batched vs per chain")
+    ap.add_argument("--sz", action="store_true", help="time H*v and fused steps of Nambu (Sz) sectors")
+    ap.add_argument("--sz-case", action="store_true", help="three Nambu H*v launches (profiling case)")
     args = ap.parse_args()
+    if args.sz_case:
+        run_sz_case(args)
+        return
+    if args.sz:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        run_sz(args)
+        return
     if args.c4:
         run_c4(args)
         return

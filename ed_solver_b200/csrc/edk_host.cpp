@@ -392,7 +392,7 @@ int rows(edk_h *h, int dtype, const RowArgs &a)
         ev_b = c->get_event();
         cudaEventRecord(ev_a, c->stream);
     }
-    cudaError_t e = h->sz ? launch_sz_rows(sz_dev(h->sz), dtype, a, c->num_sms, c->stream)
+    cudaError_t e = h->sz ? launch_sz_rows(sz_dev(h->sz), dtype, a, c->num_sms, c->kernel_path == 1, c->stream)
                           : launch_rows(h->H, dtype, a, cfg, c->stream);
     if (c->timing) {
         cudaEventRecord(ev_b, c->stream);

@@ -171,7 +171,9 @@ int64_t sz_upload_bytes(const SzHost *z);
 // on z; used for the targets of c and c+.
 int sz_sector(SzHost *z, int npart, cudaStream_t st, const SzSectorDev **out, std::string *err);
 
-cudaError_t launch_sz_rows(const SzDev &S, int dtype, const RowArgs &a, int num_sms, cudaStream_t st);
+// simple = 1: every state walks the whole term list (for A/B checks); 0: the
+// per-row compacted lists with the own row staged where it fits.
+cudaError_t launch_sz_rows(const SzDev &S, int dtype, const RowArgs &a, int num_sms, int simple, cudaStream_t st);
 // out[t] over the target sector = sum over the (one or two) operators of
 // sign * in[source(t)]; operator o: bit[o] toggled, create[o] (the target has
 // the bit), source states with (s & pmask[o]) == pwant[o] only, sgn[o] = +-1.

@@ -25,8 +25,151 @@ namespace {
 
 constexpr int kSzBlock = 256;
 
-template <typename T>
+// One term of a row's compacted list: the high-half part of the term's
+// condition held for the row, so only the low-half part is left per state.
+struct RowTerm {
+    uint32_t lsrc, ltgt;   // low-half masks the state must have / lack (0: none)
+    uint32_t lbtw;         // low-half orbitals between source and target (sign)
+    uint32_t lflip;        // lsrc | ltgt: the low-half bits the term flips
+    uint32_t joff;         // rank of the first state of the target row
+    uint32_t own;          // 1: the target row is this row
+    double hv;             // the term's value with the high-half sign applied
+};
+
+// Ordered compaction over a block: returns the position of this thread's
+// element among the passing ones of its chunk (valid when pass) and adds the
+// chunk's count to *total (read after the call by every thread).
+__device__ __forceinline__ int block_compact(bool pass, int *warp_cnt, int *total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    const unsigned b = __ballot_sync(0xffffffffu, pass);
+    if (lane == 0) warp_cnt[warp] = __popc(b);
+    __syncthreads();
+    int before = *total;
+    for (int w = 0; w < warp; ++w) before += warp_cnt[w];
+    const int pos = before + __popc(b & ((1u << lane) - 1u));
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = *total;
+        for (int w = 0; w < nw; ++w) t += warp_cnt[w];
+        *total = t;
+    }
+    __syncthreads();
+    return pos;
+}
+
+// Row kernel with per-row compaction of the term and diagonal lists and (when
+// STAGE) the row's own x staged in shared memory.  Same arithmetic, in the
+// same order, as sz_row_simple_kernel.
+template <typename T, bool STAGE>
 __global__ void __launch_bounds__(kSzBlock) sz_row_kernel(const SzDev S, const RowArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int warp_cnt[32];
+    __shared__ int n_terms, n_diag;
+    const int nq = 1 << (2 * S.nc);
+    RowTerm *rt = reinterpret_cast<RowTerm *>(smem_raw);
+    double *qs = reinterpret_cast<double *>(rt + S.nterm);
+    double *de = qs + nq;                                          // row's diagonal energies
+    uint32_t *db = reinterpret_cast<uint32_t *>(de + S.ndiag);      // their low-half bit (0: hole, occupied)
+    T *xs = reinterpret_cast<T *>(db + ((S.ndiag + 3) & ~3));
+    for (int t = threadIdx.x; t < nq; t += blockDim.x) qs[t] = S.quart[t];
+
+    const int ks = step_index(a);
+    StepScalars sc;
+    if (!step_scalars(a, ks, sc)) return;
+
+    const T *__restrict__ x = static_cast<const T *>(a.x);
+    const int ns = S.ns, nb = S.nb, nc = S.nc, nterm = S.nterm, ndiag = S.ndiag;
+    const uint32_t lowmask = (1u << ns) - 1u, cm = (1u << nc) - 1u;
+    const uint32_t *__restrict__ off_h = S.sec.off_h;
+    const uint16_t *__restrict__ rank_low = S.rank_low;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int r = blockIdx.x; r < S.sec.nrows; r += gridDim.x) {
+        const uint32_t h = S.sec.row_h[r];
+        const int k = S.sec.npart - __popc(h);
+        const int c0 = S.class_start[k], len = S.class_start[k + 1] - c0;
+        const uint32_t base = off_h[h];
+        __syncthreads();                       // the previous row is done with the lists
+        if (threadIdx.x == 0) { n_terms = 0; n_diag = 0; }
+        // ---- compact the terms whose high-half condition holds on this row ----
+        for (int t0 = 0; t0 < nterm; t0 += blockDim.x) {
+            const int t = t0 + threadIdx.x;
+            bool pass = false;
+            SzTerm tm;
+            if (t < nterm) {
+                tm = S.terms[t];
+                const uint32_t hsrc = tm.src >> ns, htgt = tm.tgt >> ns;
+                pass = (h & hsrc) == hsrc && (h & htgt) == 0u;
+            }
+            const int pos = block_compact(pass, warp_cnt, &n_terms);
+            if (pass) {
+                const uint32_t hsrc = tm.src >> ns, htgt = tm.tgt >> ns;
+                const uint32_t h2 = h ^ hsrc ^ htgt;
+                RowTerm o;
+                o.lsrc = tm.src & lowmask;
+                o.ltgt = tm.tgt & lowmask;
+                o.lbtw = tm.btw & lowmask;
+                o.lflip = o.lsrc | o.ltgt;
+                o.joff = off_h[h2];
+                o.own = h2 == h;
+                o.hv = (__popc(h & (tm.btw >> ns)) & 1) ? -tm.h : tm.h;
+                rt[pos] = o;
+            }
+        }
+        // ---- the diagonal orbitals: low-half ones kept, occupied holes kept ----
+        for (int t0 = 0; t0 < ndiag; t0 += blockDim.x) {
+            const int t = t0 + threadIdx.x;
+            bool pass = false;
+            uint32_t bit = 0u;
+            if (t < ndiag) {
+                bit = S.diag_bit[t];
+                pass = (bit & lowmask) != 0u || (h & (bit >> ns)) != 0u;
+            }
+            const int pos = block_compact(pass, warp_cnt, &n_diag);
+            if (pass) { de[pos] = S.diag_e[t]; db[pos] = bit & lowmask; }
+        }
+        if (STAGE) stage_row<T>(xs, x + base, len);
+        __syncthreads();
+        const int nt = n_terms, nd = n_diag;
+        const uint32_t hcfg = ((h >> nb) & cm) << nc;
+        for (int c = threadIdx.x; c < len; c += blockDim.x) {
+            const uint32_t l = (uint32_t)S.low_states[c0 + c];
+            const int64_t i = (int64_t)base + c;
+            const T xo = STAGE ? xs[c] : x[i];
+            double acc = fmul(qs[((l >> nb) & cm) | hcfg], (double)xo);
+            if (S.order == 0) {
+                double d = 0.0;
+                for (int o = 0; o < nd; ++o)
+                    if (!db[o] || (l & db[o])) d = fadd(d, de[o]);
+                acc = hmadd<T>(acc, d, xo);
+            } else {
+                for (int o = 0; o < nd; ++o)
+                    if (!db[o] || (l & db[o])) acc = hmadd<T>(acc, de[o], xo);
+            }
+            for (int t = 0; t < nt; ++t) {
+                const uint32_t lsrc = rt[t].lsrc, ltgt = rt[t].ltgt;
+                if ((l & lsrc) != lsrc || (l & ltgt)) continue;
+                const uint32_t lflip = rt[t].lflip;
+                const int col = lflip ? (int)rank_low[l ^ lflip] : c;
+                const double hv = (__popc(l & rt[t].lbtw) & 1) ? -rt[t].hv : rt[t].hv;
+                T xj;
+                if (STAGE && rt[t].own) xj = xs[col];
+                else xj = __ldg(x + (int64_t)rt[t].joff + col);
+                acc = hmadd<T>(acc, hv, xj);
+            }
+            row_epilogue<T>(a, sc, i, acc, xo, s0, s1, s2);
+        }
+    }
+    if (a.mode == kModeHv) return;
+    double v[4] = {s0, s1, s2, 0.0};
+    if (grid_sum<4>(v, a.partials, a.counter, a.sums_out))
+        if (a.mode == kModeFirst || a.mode == kModeStep) lanczos_finalize(a, ks);
+}
+
+// Reference form: every state walks the whole term list (kernel path 1).
+template <typename T>
+__global__ void __launch_bounds__(kSzBlock) sz_row_simple_kernel(const SzDev S, const RowArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SzTerm *ts = reinterpret_cast<SzTerm *>(smem_raw);
@@ -135,33 +278,50 @@ int sz_block(int maxlen)
     return b;
 }
 
+template <typename K>
+cudaError_t launch_one(K kern, int grid, int block, size_t smem, const SzDev &S, const RowArgs &a, cudaStream_t st)
+{
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    kern<<<grid, block, smem, st>>>(S, a);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
-cudaError_t launch_sz_rows(const SzDev &S, int dtype, const RowArgs &a, int num_sms, cudaStream_t st)
+cudaError_t launch_sz_rows(const SzDev &S, int dtype, const RowArgs &a, int num_sms, int simple, cudaStream_t st)
 {
-    const size_t smem = sz_smem(S);
     const int block = sz_block(S.sec.maxlen);
     int per_sm = 2048 / block;
     if (per_sm > 16) per_sm = 16;
+    const size_t eb = dtype == EDK_F64 ? 8 : 4;
+    if (simple) {
+        int grid = num_sms * per_sm;
+        if (grid > S.sec.nrows) grid = S.sec.nrows;
+        if (grid < 1) grid = 1;
+        const size_t smem = sz_smem(S);
+        return dtype == EDK_F64 ? launch_one(sz_row_simple_kernel<double>, grid, block, smem, S, a, st)
+                                : launch_one(sz_row_simple_kernel<float>, grid, block, smem, S, a, st);
+    }
+    size_t smem = (size_t)S.nterm * sizeof(RowTerm) + sizeof(double) * ((size_t)1 << (2 * S.nc)) +
+                  (size_t)S.ndiag * sizeof(double) + (size_t)((S.ndiag + 3) & ~3) * sizeof(uint32_t);
+    // stage the own row when it leaves room for four blocks per SM
+    const size_t row_bytes = (size_t)S.sec.maxlen * eb;
+    const bool stage = smem + row_bytes <= 52 * 1024;
+    if (stage) smem += row_bytes;
+    int by_smem = (int)((228 * 1024) / (smem + 1024));
+    if (by_smem < per_sm) per_sm = by_smem;
+    if (per_sm < 1) per_sm = 1;
     int grid = num_sms * per_sm;
     if (grid > S.sec.nrows) grid = S.sec.nrows;
     if (grid < 1) grid = 1;
-    if (dtype == EDK_F64) {
-        if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(sz_row_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem);
-            if (e != cudaSuccess) return e;
-        }
-        sz_row_kernel<double><<<grid, block, smem, st>>>(S, a);
-    } else {
-        if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(sz_row_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem);
-            if (e != cudaSuccess) return e;
-        }
-        sz_row_kernel<float><<<grid, block, smem, st>>>(S, a);
-    }
-    return cudaGetLastError();
+    if (dtype == EDK_F64)
+        return stage ? launch_one(sz_row_kernel<double, true>, grid, block, smem, S, a, st)
+                     : launch_one(sz_row_kernel<double, false>, grid, block, smem, S, a, st);
+    return stage ? launch_one(sz_row_kernel<float, true>, grid, block, smem, S, a, st)
+                 : launch_one(sz_row_kernel<float, false>, grid, block, smem, S, a, st);
 }
 
 cudaError_t launch_sz_apply_c(int dtype, const SzDev &src, const SzSectorDev &tgt, int nop, const SzOp *ops,

@@ -1101,7 +1101,9 @@ orc_h *orc_h_new_sz(const orc_model_sz *m, int npart)
     z->diag = (double *)malloc(sizeof(double) * (size_t)(d > 0 ? d : 1));
     z->ptr = (int64_t *)malloc(sizeof(int64_t) * (size_t)(d + 1));
     int64_t nnz = 0;
-    for (int64_t i = 0; i < d; ++i) nnz += sz_visit(z, z->st[i], NULL, NULL);
+    /* the on-the-fly variant tabulates nothing but QUART_INT_SZ (HAIMsz.f90:124) */
+    if (!z->on_fly)
+        for (int64_t i = 0; i < d; ++i) nnz += sz_visit(z, z->st[i], NULL, NULL);
     z->tgt = (int64_t *)malloc(sizeof(int64_t) * (size_t)(nnz > 0 ? nnz : 1));
     z->val = (double *)malloc(sizeof(double) * (size_t)(nnz > 0 ? nnz : 1));
     const int cap = z->nimp * z->nimp + z->nbath * z->nbath + 2 * z->nimp * z->nbath + 1;
@@ -1117,7 +1119,7 @@ orc_h *orc_h_new_sz(const orc_model_sz *m, int npart)
         for (int o = 0; o < z->nbath; ++o)
             if (bt(s, z->bath_bit[o])) dg = dg + z->ebn[o * z->nbath + o];
         z->diag[i] = dg;
-        int n = sz_visit(z, s, ts, tv);
+        int n = z->on_fly ? 0 : sz_visit(z, s, ts, tv);
         for (int e = 0; e < n; ++e) {
             z->tgt[z->ptr[i] + e] = orc_colex_rank(ts[e]);
             z->val[z->ptr[i] + e] = tv[e];

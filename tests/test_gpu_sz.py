@@ -36,8 +36,15 @@ MODELS = {
 }
 
 
+@pytest.fixture(params=[0, 1], ids=["compacted-rows", "whole-term-list"])
+def kpath(request, ctx):
+    ctx.set_kernel_path(request.param)
+    yield request.param
+    ctx.set_kernel_path(0)
+
+
 @pytest.mark.parametrize("name", sorted(MODELS))
-def test_hmult_fp64_bit_exact(ctx, name):
+def test_hmult_fp64_bit_exact(ctx, kpath, name):
     import torch
     m = MODELS[name]()
     rng = np.random.default_rng(1)
@@ -51,7 +58,7 @@ def test_hmult_fp64_bit_exact(ctx, name):
         assert np.array_equal(y, ho.hmult(x)), npart
 
 
-def test_hmult_fp64_bit_exact_ns12(ctx):
+def test_hmult_fp64_bit_exact_ns12(ctx, kpath):
     """ns=12 half-filled Nambu sector: 2.7M states, rows of up to 924 low halves."""
     import torch
     m = nambu_workload(12)
@@ -63,7 +70,7 @@ def test_hmult_fp64_bit_exact_ns12(ctx):
 
 
 @pytest.mark.parametrize("name", ["star8", "two_orbital_pvbc_fly"])
-def test_hmult_fp32(ctx, name):
+def test_hmult_fp32(ctx, kpath, name):
     import torch
     m = MODELS[name]()
     h = edk.HamiltonianSz(ctx, m, m.ns)
