@@ -24,6 +24,7 @@ namespace edk {
 namespace {
 
 constexpr int kSzBlock = 256;
+constexpr int kChunk = 8;      // gathers issued together per state
 
 // One term of a row's compacted list: the high-half part of the term's
 // condition held for the row, so only the low-half part is left per state.
@@ -62,7 +63,7 @@ __device__ __forceinline__ int block_compact(bool pass, int *warp_cnt, int *tota
 // STAGE) the row's own x staged in shared memory.  Same arithmetic, in the
 // same order, as sz_row_simple_kernel.
 template <typename T, bool STAGE>
-__global__ void __launch_bounds__(kSzBlock) sz_row_kernel(const SzDev S, const RowArgs a)
+__global__ void __launch_bounds__(kSzBlock, 3) sz_row_kernel(const SzDev S, const RowArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int warp_cnt[32];
@@ -147,16 +148,33 @@ __global__ void __launch_bounds__(kSzBlock) sz_row_kernel(const SzDev S, const R
                 for (int o = 0; o < nd; ++o)
                     if (!db[o] || (l & db[o])) acc = hmadd<T>(acc, de[o], xo);
             }
-            for (int t = 0; t < nt; ++t) {
-                const uint32_t lsrc = rt[t].lsrc, ltgt = rt[t].ltgt;
-                if ((l & lsrc) != lsrc || (l & ltgt)) continue;
-                const uint32_t lflip = rt[t].lflip;
-                const int col = lflip ? (int)rank_low[l ^ lflip] : c;
-                const double hv = (__popc(l & rt[t].lbtw) & 1) ? -rt[t].hv : rt[t].hv;
-                T xj;
-                if (STAGE && rt[t].own) xj = xs[col];
-                else xj = __ldg(x + (int64_t)rt[t].joff + col);
-                acc = hmadd<T>(acc, hv, xj);
+            // chunks of kChunk terms: every gather of the chunk is issued before
+            // the chunk is accumulated in order, so kChunk loads are in flight
+            for (int t0 = 0; t0 < nt; t0 += kChunk) {
+                T xv[kChunk];
+                double hv[kChunk];
+#pragma unroll
+                for (int u = 0; u < kChunk; ++u) {
+                    const int t = t0 + u;
+                    hv[u] = 0.0;
+                    xv[u] = T(0);
+                    if (t >= nt) continue;
+                    const uint32_t lsrc = rt[t].lsrc, ltgt = rt[t].ltgt;
+                    if ((l & lsrc) != lsrc || (l & ltgt)) continue;
+                    const uint32_t lflip = rt[t].lflip;
+                    const int col = lflip ? (int)rank_low[l ^ lflip] : c;
+                    hv[u] = (__popc(l & rt[t].lbtw) & 1) ? -rt[t].hv : rt[t].hv;
+                    if (STAGE && rt[t].own) xv[u] = xs[col];
+                    else xv[u] = __ldg(x + (int64_t)rt[t].joff + col);
+                }
+#pragma unroll
+                for (int u = 0; u < kChunk; ++u) {
+                    const int t = t0 + u;
+                    if (t >= nt) break;
+                    const uint32_t lsrc = rt[t].lsrc, ltgt = rt[t].ltgt;
+                    if ((l & lsrc) != lsrc || (l & ltgt)) continue;
+                    acc = hmadd<T>(acc, hv[u], xv[u]);
+                }
             }
             row_epilogue<T>(a, sc, i, acc, xo, s0, s1, s2);
         }
@@ -313,6 +331,7 @@ cudaError_t launch_sz_rows(const SzDev &S, int dtype, const RowArgs &a, int num_
     if (stage) smem += row_bytes;
     int by_smem = (int)((228 * 1024) / (smem + 1024));
     if (by_smem < per_sm) per_sm = by_smem;
+    if (per_sm > 3) per_sm = 3;              // the register budget of __launch_bounds__(256, 3)
     if (per_sm < 1) per_sm = 1;
     int grid = num_sms * per_sm;
     if (grid > S.sec.nrows) grid = S.sec.nrows;
