@@ -331,7 +331,8 @@ cudaError_t launch_sz_rows(const SzDev &S, int dtype, const RowArgs &a, int num_
     if (stage) smem += row_bytes;
     int by_smem = (int)((228 * 1024) / (smem + 1024));
     if (by_smem < per_sm) per_sm = by_smem;
-    if (per_sm > 3) per_sm = 3;              // the register budget of __launch_bounds__(256, 3)
+    const int reg_cap = 3 * kSzBlock / block;   // the register budget of __launch_bounds__(256, 3)
+    if (per_sm > reg_cap) per_sm = reg_cap;
     if (per_sm < 1) per_sm = 1;
     int grid = num_sms * per_sm;
     if (grid > S.sec.nrows) grid = S.sec.nrows;
