@@ -138,6 +138,17 @@ struct SzTerm {
     double h;
 };
 
+// A maximal run of consecutive terms of one kind: 0 = both orbitals in the
+// low half (up-up), 1 = both in the high half (hole-hole), 2 = one in each
+// (pairing).  Up-up runs carry a table over the low halves: for low-half
+// position p (low_states order) entry k at ell[ell_off + k*2^ns + p] is the
+// k-th active term's target rank_low (16 bits) | sign (bit 16) | index in the
+// run (bits 17..31), or 0xFFFFFFFF after the last.
+struct SzRun {
+    int32_t kind, first, count, kell;
+    int64_t ell_off;
+};
+
 struct SzSectorDev {
     int npart = 0, nrows = 0, maxlen = 0;
     int64_t dim = 0;
@@ -159,6 +170,10 @@ struct SzDev {
     const double *diag_e = nullptr;
     const double *quart = nullptr;          // 4^nc: QUART_INT_SZ by impurity configuration
                                             // (up bits | hole bits << nc)
+    int nrun = 0;
+    const SzRun *runs = nullptr;
+    const int32_t *term_run = nullptr;      // nterm: run of each term
+    const uint32_t *ell = nullptr;          // the up-up runs' tables
 };
 
 struct SzHost;   // host tables and device copies of one Nambu sector (edk_sz.cpp)

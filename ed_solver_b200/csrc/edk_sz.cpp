@@ -8,6 +8,7 @@
 // the target's rank from two small tables (off_h, rank_low), and takes
 // QUART_INT_SZ from a table indexed by the impurity configuration.  The
 // only per-sector data are 2^ns row offsets.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -104,7 +105,7 @@ uint32_t between_mask(int a, int b)
 struct SzHost {
     int ns = 0, nb = 0, nc = 0;
     double shift = 0.0;
-    Buf rank_low, low_states, class_start, terms, diag_bit, diag_e, quart;
+    Buf rank_low, low_states, class_start, terms, diag_bit, diag_e, quart, runs, term_run, ell;
     Sector own;
     std::vector<std::unique_ptr<Sector>> others;
     SzDev dev;
@@ -276,18 +277,54 @@ int sz_create(const edk_model_sz *m, int npart, cudaStream_t st, SzHost **out, s
         }
     }
 
+    // ---- runs of one kind, and the tables of the up-up runs ----
+    const uint32_t lowmask = (1u << ns) - 1u;
+    std::vector<SzRun> runs;
+    std::vector<int32_t> term_run(terms.size());
+    for (size_t t = 0; t < terms.size(); ++t) {
+        const uint32_t both = terms[t].src | terms[t].tgt;
+        const int kind = (both & ~lowmask) == 0u ? 0 : (both & lowmask) == 0u ? 1 : 2;
+        if (runs.empty() || runs.back().kind != kind) runs.push_back(SzRun{kind, (int32_t)t, 0, 0, 0});
+        runs.back().count++;
+        term_run[t] = (int32_t)runs.size() - 1;
+    }
+    std::vector<uint32_t> ell;
+    for (auto &r : runs) {
+        if (r.kind != 0) continue;
+        std::vector<std::vector<uint32_t>> lists(nh);
+        int kmax = 0;
+        for (uint32_t p = 0; p < nh; ++p) {
+            const uint32_t l = lst[p];
+            for (int q = 0; q < r.count; ++q) {
+                const SzTerm &tm = terms[(size_t)r.first + q];
+                if (!(l & tm.src) || (l & tm.tgt)) continue;
+                const uint32_t l2 = l ^ tm.src ^ tm.tgt;
+                const uint32_t neg = (uint32_t)(__builtin_popcount(l & tm.btw) & 1);
+                lists[p].push_back((uint32_t)rlow[l2] | (neg << 16) | ((uint32_t)q << 17));
+            }
+            kmax = std::max<int>(kmax, (int)lists[p].size());
+        }
+        r.kell = kmax;
+        r.ell_off = (int64_t)ell.size();
+        ell.resize(ell.size() + (size_t)kmax * nh, 0xFFFFFFFFu);
+        for (uint32_t p = 0; p < nh; ++p)
+            for (size_t q = 0; q < lists[p].size(); ++q) ell[(size_t)r.ell_off + q * nh + p] = lists[p][q];
+    }
+
     cudaError_t e;
     std::string berr;
     if ((e = z->rank_low.put(rlow, st)) != cudaSuccess || (e = z->low_states.put(lst, st)) != cudaSuccess ||
         (e = z->class_start.put(cstart, st)) != cudaSuccess || (e = z->terms.put(terms, st)) != cudaSuccess ||
         (e = z->diag_bit.put(dbit, st)) != cudaSuccess || (e = z->diag_e.put(de, st)) != cudaSuccess ||
-        (e = z->quart.put(quart, st)) != cudaSuccess ||
+        (e = z->quart.put(quart, st)) != cudaSuccess || (e = z->runs.put(runs, st)) != cudaSuccess ||
+        (e = z->term_run.put(term_run, st)) != cudaSuccess || (e = z->ell.put(ell, st)) != cudaSuccess ||
         (e = build_sector(ns, npart, st, z->own, z->bytes, &berr)) != cudaSuccess) {
         *err = berr.empty() ? std::string("Nambu sector upload: ") + cudaGetErrorString(e) : berr;
         return e == cudaErrorMemoryAllocation ? EDK_ERR_NOMEM : (berr.empty() ? EDK_ERR_CUDA : EDK_ERR_UNSUPPORTED);
     }
     z->bytes += (int64_t)(rlow.size() * 2 + lst.size() * 2 + cstart.size() * 4 + terms.size() * sizeof(SzTerm) +
-                          dbit.size() * 12 + quart.size() * 8);
+                          dbit.size() * 12 + quart.size() * 8 + runs.size() * sizeof(SzRun) +
+                          term_run.size() * 4 + ell.size() * 4);
     SzDev &d = z->dev;
     d.ns = ns;
     d.nb = nb;
@@ -303,6 +340,10 @@ int sz_create(const edk_model_sz *m, int npart, cudaStream_t st, SzHost **out, s
     d.diag_bit = z->diag_bit.as<uint32_t>();
     d.diag_e = z->diag_e.as<double>();
     d.quart = z->quart.as<double>();
+    d.nrun = (int)runs.size();
+    d.runs = z->runs.as<SzRun>();
+    d.term_run = z->term_run.as<int32_t>();
+    d.ell = z->ell.as<uint32_t>();
     *out = z.release();
     return EDK_OK;
 }

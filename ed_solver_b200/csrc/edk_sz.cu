@@ -24,16 +24,18 @@ namespace edk {
 namespace {
 
 constexpr int kSzBlock = 256;
-constexpr int kChunk = 8;      // gathers issued together per state
 
-// One term of a row's compacted list: the high-half part of the term's
-// condition held for the row, so only the low-half part is left per state.
+// One entry of a row's list, in the order of the terms:
+//   kind 0: a whole up-up run (the per-state table of the run applies);
+//   kind 1: a hole-hole term active on the row: the same column of row joff;
+//   kind 2: a pairing term whose high-half condition holds on the row; the
+//           low-half condition (lsrc set, ltgt empty) is checked per state.
 struct RowTerm {
-    uint32_t lsrc, ltgt;   // low-half masks the state must have / lack (0: none)
+    uint32_t lsrc, ltgt;   // low-half masks the state must have / lack
     uint32_t lbtw;         // low-half orbitals between source and target (sign)
     uint32_t lflip;        // lsrc | ltgt: the low-half bits the term flips
     uint32_t joff;         // rank of the first state of the target row
-    uint32_t own;          // 1: the target row is this row
+    uint32_t kr;           // kind | run << 2
     double hv;             // the term's value with the high-half sign applied
 };
 
@@ -59,9 +61,11 @@ __device__ __forceinline__ int block_compact(bool pass, int *warp_cnt, int *tota
     return pos;
 }
 
-// Row kernel with per-row compaction of the term and diagonal lists and (when
-// STAGE) the row's own x staged in shared memory.  Same arithmetic, in the
-// same order, as sz_row_simple_kernel.
+constexpr uint32_t kEllEnd = 0xFFFFFFFFu;
+
+// Row kernel on per-row lists (see RowTerm); the own row is staged in shared
+// memory when STAGE.  Same arithmetic, in the same order, as
+// sz_row_simple_kernel.
 template <typename T, bool STAGE>
 __global__ void __launch_bounds__(kSzBlock, 3) sz_row_kernel(const SzDev S, const RowArgs a)
 {
@@ -70,11 +74,15 @@ __global__ void __launch_bounds__(kSzBlock, 3) sz_row_kernel(const SzDev S, cons
     __shared__ int n_terms, n_diag;
     const int nq = 1 << (2 * S.nc);
     RowTerm *rt = reinterpret_cast<RowTerm *>(smem_raw);
-    double *qs = reinterpret_cast<double *>(rt + S.nterm);
-    double *de = qs + nq;                                          // row's diagonal energies
-    uint32_t *db = reinterpret_cast<uint32_t *>(de + S.ndiag);      // their low-half bit (0: hole, occupied)
+    SzRun *runs = reinterpret_cast<SzRun *>(rt + S.nterm);
+    double *hs = reinterpret_cast<double *>(runs + S.nrun);         // term values
+    double *qs = hs + S.nterm;
+    double *de = qs + nq;                                           // row's diagonal energies
+    uint32_t *db = reinterpret_cast<uint32_t *>(de + S.ndiag);       // their low-half bit (0: hole, occupied)
     T *xs = reinterpret_cast<T *>(db + ((S.ndiag + 3) & ~3));
     for (int t = threadIdx.x; t < nq; t += blockDim.x) qs[t] = S.quart[t];
+    for (int t = threadIdx.x; t < S.nterm; t += blockDim.x) hs[t] = S.terms[t].h;
+    for (int t = threadIdx.x; t < S.nrun; t += blockDim.x) runs[t] = S.runs[t];
 
     const int ks = step_index(a);
     StepScalars sc;
@@ -83,8 +91,10 @@ __global__ void __launch_bounds__(kSzBlock, 3) sz_row_kernel(const SzDev S, cons
     const T *__restrict__ x = static_cast<const T *>(a.x);
     const int ns = S.ns, nb = S.nb, nc = S.nc, nterm = S.nterm, ndiag = S.ndiag;
     const uint32_t lowmask = (1u << ns) - 1u, cm = (1u << nc) - 1u;
+    const size_t nlow = (size_t)1 << ns;
     const uint32_t *__restrict__ off_h = S.sec.off_h;
     const uint16_t *__restrict__ rank_low = S.rank_low;
+    const uint32_t *__restrict__ ell = S.ell;
     double s0 = 0.0, s1 = 0.0, s2 = 0.0;
     for (int r = blockIdx.x; r < S.sec.nrows; r += gridDim.x) {
         const uint32_t h = S.sec.row_h[r];
@@ -93,28 +103,39 @@ __global__ void __launch_bounds__(kSzBlock, 3) sz_row_kernel(const SzDev S, cons
         const uint32_t base = off_h[h];
         __syncthreads();                       // the previous row is done with the lists
         if (threadIdx.x == 0) { n_terms = 0; n_diag = 0; }
-        // ---- compact the terms whose high-half condition holds on this row ----
+        // ---- the row's list ----
         for (int t0 = 0; t0 < nterm; t0 += blockDim.x) {
             const int t = t0 + threadIdx.x;
             bool pass = false;
             SzTerm tm;
+            int run = 0, kind = 0;
             if (t < nterm) {
                 tm = S.terms[t];
-                const uint32_t hsrc = tm.src >> ns, htgt = tm.tgt >> ns;
-                pass = (h & hsrc) == hsrc && (h & htgt) == 0u;
+                run = S.term_run[t];
+                kind = runs[run].kind;
+                if (kind == 0) {
+                    pass = runs[run].first == t;
+                } else {
+                    const uint32_t hsrc = tm.src >> ns, htgt = tm.tgt >> ns;
+                    pass = (h & hsrc) == hsrc && (h & htgt) == 0u;
+                }
             }
             const int pos = block_compact(pass, warp_cnt, &n_terms);
             if (pass) {
-                const uint32_t hsrc = tm.src >> ns, htgt = tm.tgt >> ns;
-                const uint32_t h2 = h ^ hsrc ^ htgt;
                 RowTerm o;
-                o.lsrc = tm.src & lowmask;
-                o.ltgt = tm.tgt & lowmask;
-                o.lbtw = tm.btw & lowmask;
-                o.lflip = o.lsrc | o.ltgt;
-                o.joff = off_h[h2];
-                o.own = h2 == h;
-                o.hv = (__popc(h & (tm.btw >> ns)) & 1) ? -tm.h : tm.h;
+                o.kr = (uint32_t)kind | ((uint32_t)run << 2);
+                if (kind == 0) {
+                    o.lsrc = o.ltgt = o.lbtw = o.lflip = o.joff = 0u;
+                    o.hv = 0.0;
+                } else {
+                    const uint32_t h2 = h ^ (tm.src >> ns) ^ (tm.tgt >> ns);
+                    o.lsrc = tm.src & lowmask;
+                    o.ltgt = tm.tgt & lowmask;
+                    o.lbtw = tm.btw & lowmask;
+                    o.lflip = o.lsrc | o.ltgt;
+                    o.joff = off_h[h2];
+                    o.hv = (__popc(h & (tm.btw >> ns)) & 1) ? -tm.h : tm.h;
+                }
                 rt[pos] = o;
             }
         }
@@ -148,32 +169,40 @@ __global__ void __launch_bounds__(kSzBlock, 3) sz_row_kernel(const SzDev S, cons
                 for (int o = 0; o < nd; ++o)
                     if (!db[o] || (l & db[o])) acc = hmadd<T>(acc, de[o], xo);
             }
-            // chunks of kChunk terms: every gather of the chunk is issued before
-            // the chunk is accumulated in order, so kChunk loads are in flight
-            for (int t0 = 0; t0 < nt; t0 += kChunk) {
-                T xv[kChunk];
-                double hv[kChunk];
+            for (int e = 0; e < nt; ++e) {
+                const uint32_t kr = rt[e].kr;
+                if ((kr & 3u) == 0u) {
+                    // up-up run: this state's active terms from the run's table,
+                    // four entries loaded ahead of their use
+                    const SzRun &R = runs[kr >> 2];
+                    const uint32_t *tab = ell + R.ell_off + (size_t)(c0 + c);
+                    const double *hr = hs + R.first;
+                    for (int q0 = 0; q0 < R.kell; q0 += 4) {
+                        uint32_t u[4];
 #pragma unroll
-                for (int u = 0; u < kChunk; ++u) {
-                    const int t = t0 + u;
-                    hv[u] = 0.0;
-                    xv[u] = T(0);
-                    if (t >= nt) continue;
-                    const uint32_t lsrc = rt[t].lsrc, ltgt = rt[t].ltgt;
-                    if ((l & lsrc) != lsrc || (l & ltgt)) continue;
-                    const uint32_t lflip = rt[t].lflip;
-                    const int col = lflip ? (int)rank_low[l ^ lflip] : c;
-                    hv[u] = (__popc(l & rt[t].lbtw) & 1) ? -rt[t].hv : rt[t].hv;
-                    if (STAGE && rt[t].own) xv[u] = xs[col];
-                    else xv[u] = __ldg(x + (int64_t)rt[t].joff + col);
-                }
+                        for (int v = 0; v < 4; ++v) u[v] = q0 + v < R.kell ? __ldg(tab + (size_t)(q0 + v) * nlow) : kEllEnd;
+                        T xv[4];
 #pragma unroll
-                for (int u = 0; u < kChunk; ++u) {
-                    const int t = t0 + u;
-                    if (t >= nt) break;
-                    const uint32_t lsrc = rt[t].lsrc, ltgt = rt[t].ltgt;
+                        for (int v = 0; v < 4; ++v) {
+                            const int col = (int)(u[v] & 0xFFFFu);
+                            xv[v] = u[v] == kEllEnd ? T(0) : (STAGE ? xs[col] : __ldg(x + (int64_t)base + col));
+                        }
+#pragma unroll
+                        for (int v = 0; v < 4; ++v) {
+                            if (u[v] == kEllEnd) break;
+                            const double hv = hr[u[v] >> 17];
+                            acc = hmadd<T>(acc, (u[v] & 0x10000u) ? -hv : hv, xv[v]);
+                        }
+                        if (u[3] == kEllEnd) break;
+                    }
+                } else if ((kr & 3u) == 1u) {
+                    acc = hmadd<T>(acc, rt[e].hv, __ldg(x + (int64_t)rt[e].joff + c));
+                } else {
+                    const uint32_t lsrc = rt[e].lsrc, ltgt = rt[e].ltgt;
                     if ((l & lsrc) != lsrc || (l & ltgt)) continue;
-                    acc = hmadd<T>(acc, hv[u], xv[u]);
+                    const int col = (int)rank_low[l ^ rt[e].lflip];
+                    const double hv = (__popc(l & rt[e].lbtw) & 1) ? -rt[e].hv : rt[e].hv;
+                    acc = hmadd<T>(acc, hv, __ldg(x + (int64_t)rt[e].joff + col));
                 }
             }
             row_epilogue<T>(a, sc, i, acc, xo, s0, s1, s2);
@@ -323,8 +352,9 @@ cudaError_t launch_sz_rows(const SzDev &S, int dtype, const RowArgs &a, int num_
         return dtype == EDK_F64 ? launch_one(sz_row_simple_kernel<double>, grid, block, smem, S, a, st)
                                 : launch_one(sz_row_simple_kernel<float>, grid, block, smem, S, a, st);
     }
-    size_t smem = (size_t)S.nterm * sizeof(RowTerm) + sizeof(double) * ((size_t)1 << (2 * S.nc)) +
-                  (size_t)S.ndiag * sizeof(double) + (size_t)((S.ndiag + 3) & ~3) * sizeof(uint32_t);
+    size_t smem = (size_t)S.nterm * (sizeof(RowTerm) + sizeof(double)) + (size_t)S.nrun * sizeof(SzRun) +
+                  sizeof(double) * ((size_t)1 << (2 * S.nc)) + (size_t)S.ndiag * sizeof(double) +
+                  (size_t)((S.ndiag + 3) & ~3) * sizeof(uint32_t);
     // stage the own row when it leaves room for four blocks per SM
     const size_t row_bytes = (size_t)S.sec.maxlen * eb;
     const bool stage = smem + row_bytes <= 52 * 1024;
