@@ -67,7 +67,7 @@ constexpr uint32_t kEllEnd = 0xFFFFFFFFu;
 // memory when STAGE.  Same arithmetic, in the same order, as
 // sz_row_simple_kernel.
 template <typename T, bool STAGE>
-__global__ void __launch_bounds__(kSzBlock, 3) sz_row_kernel(const SzDev S, const RowArgs a)
+__global__ void __launch_bounds__(kSzBlock, 4) sz_row_kernel(const SzDev S, const RowArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int warp_cnt[32];
@@ -361,7 +361,7 @@ cudaError_t launch_sz_rows(const SzDev &S, int dtype, const RowArgs &a, int num_
     if (stage) smem += row_bytes;
     int by_smem = (int)((228 * 1024) / (smem + 1024));
     if (by_smem < per_sm) per_sm = by_smem;
-    const int reg_cap = 3 * kSzBlock / block;   // the register budget of __launch_bounds__(256, 3)
+    const int reg_cap = 4 * kSzBlock / block;   // the register budget of __launch_bounds__(256, 4)
     if (per_sm > reg_cap) per_sm = reg_cap;
     if (per_sm < 1) per_sm = 1;
     int grid = num_sms * per_sm;
