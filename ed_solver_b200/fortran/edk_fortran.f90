@@ -20,6 +20,13 @@ module edk_fortran
     real(c_double) :: cutoff_hamilt_param
   end type
 
+  ! Nambu (Sz) sectors: the normal part plus Pb(k,k') and PVbc_s(k,c) (bath_class.f90:956-1022)
+  type, bind(C) :: edk_model_sz
+    type(edk_model) :: base
+    type(c_ptr) :: pb, pvbc
+    integer(c_int32_t) :: on_fly
+  end type
+
   type, bind(C) :: edk_lanczos_opts
     integer(c_int32_t) :: nitermax, neigen
     real(c_double) :: tolerance, demax, cutoff_min_lanczos_vec
@@ -129,6 +136,31 @@ module edk_fortran
       real(c_double), intent(in) :: wn(*)
       real(c_double), intent(out) :: G(*), diag(*), subdiag(*)
       integer(c_int32_t) :: niter_done
+    end function
+
+    ! new_HAIMsz (HAIMsz.f90:51-82): the sector of npart Nambu particles
+    integer(c_int) function edk_h_create_sz(ctx, m, npart, h) bind(C, name="edk_h_create_sz")
+      import :: c_int, c_ptr, edk_model_sz
+      type(c_ptr), value :: ctx
+      type(edk_model_sz), intent(in) :: m
+      integer(c_int), value :: npart
+      type(c_ptr) :: h
+    end function
+    integer(c_int) function edk_h_sz_info(h, npart, energy_shift) bind(C, name="edk_h_sz_info")
+      import :: c_int, c_ptr, c_int32_t, c_double
+      type(c_ptr), value :: h
+      integer(c_int32_t) :: npart
+      real(c_double) :: energy_shift
+    end function
+    ! apply_Csz_updo / apply_Csz_N_updo (apply_C.f90:344-483)
+    integer(c_int) function edk_apply_csz(src, dtype, site, spin, dagger, projected, site2, sign2, vin, vout, &
+        out_dim, out_npart) bind(C, name="edk_apply_csz")
+      import :: c_int, c_ptr, c_int32_t, c_int64_t
+      type(c_ptr), value :: src
+      integer(c_int), value :: dtype, site, spin, dagger, projected, site2, sign2
+      type(c_ptr), value :: vin, vout
+      integer(c_int64_t) :: out_dim
+      integer(c_int32_t) :: out_npart
     end function
 
     ! <a| dH/dtheta_q |b> for every parameter (FP64 device vectors a, b)
