@@ -102,7 +102,8 @@ struct edk_ctx {
                              // 2/3 = the fast kernel where applicable
     // optional event timing of row-kernel launches: (class, start, stop)
     bool timing = false;
-    struct Timed { int cls; cudaEvent_t a, b; double elems; };
+    struct Timed { int cls; cudaEvent_t a, b; double elems; int n; };
+    bool capturing = false;  // a graph capture is in progress: launches are not timed
     std::vector<Timed> timed;
     std::vector<cudaEvent_t> event_pool;
     int64_t t_count[8] = {0};
@@ -128,7 +129,7 @@ struct edk_ctx {
             float ms = 0.f;
             if (cudaEventSynchronize(t.b) == cudaSuccess && cudaEventElapsedTime(&ms, t.a, t.b) == cudaSuccess) {
                 t_ms[t.cls] += ms;
-                t_count[t.cls] += 1;
+                t_count[t.cls] += t.n;
                 t_elems[t.cls] += t.elems;
             }
             event_pool.push_back(t.a);
@@ -387,17 +388,18 @@ int rows(edk_h *h, int dtype, const RowArgs &a)
         }
     }
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;
-    if (c->timing) {
+    const bool timed = c->timing && !c->capturing;
+    if (timed) {
         ev_a = c->get_event();
         ev_b = c->get_event();
         cudaEventRecord(ev_a, c->stream);
     }
     cudaError_t e = h->sz ? launch_sz_rows(sz_dev(h->sz), dtype, a, c->num_sms, c->kernel_path == 1, c->stream)
                           : launch_rows(h->H, dtype, a, cfg, c->stream);
-    if (c->timing) {
+    if (timed) {
         cudaEventRecord(ev_b, c->stream);
-        c->timed.push_back({a.mode + (dtype == EDK_F32 ? 4 : 0), ev_a, ev_b, (double)h->dim});
-        if (c->timed.size() > 4096) c->drain_timing();
+        c->timed.push_back({a.mode + (dtype == EDK_F32 ? 4 : 0), ev_a, ev_b, (double)h->dim, 1});
+        if (c->timed.size() > 16384) c->drain_timing();
     }
     c->launches++;
     return c->cuda(e, "row kernel");
@@ -500,7 +502,7 @@ int krylov_run(Krylov &K, int target)
 {
     edk_ctx *c = K.h->ctx;
     while (K.k < target) {
-        const bool eligible = c->graphs && !c->timing && !K.graph_off && K.k >= 2 && target - K.k >= 2;
+        const bool eligible = c->graphs && !K.graph_off && K.k >= 2 && target - K.k >= 2;
         if (eligible && !K.gexec) {
             // capture two steps with the device step counter, then restore the host state
             const Krylov save_state{K.h, K.dtype, {}, K.ivk, K.ivkm1, K.is, K.is_out, K.k};
@@ -516,8 +518,10 @@ int krylov_run(Krylov &K, int target)
             }
             cudaStream_t user_stream = c->stream;
             c->stream = c->capture_stream;
+            c->capturing = true;
             if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
                 c->stream = user_stream;
+                c->capturing = false;
                 (void)cudaGetLastError();
                 K.graph_off = true;
                 continue;
@@ -544,6 +548,7 @@ int krylov_run(Krylov &K, int target)
             }
             const cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
             c->stream = user_stream;
+            c->capturing = false;
             K.ivk = save_state.ivk; K.ivkm1 = save_state.ivkm1; K.is = save_state.is; K.is_out = save_state.is_out;
             K.k = save_state.k;
             c->launches = launches0;
@@ -564,7 +569,20 @@ int krylov_run(Krylov &K, int target)
             c->launches++;
             if (rc) return rc;
             while (target - K.k >= 2) {
+                // with per-launch timing on, a replay is timed as a whole: two fused steps
+                cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+                if (c->timing) {
+                    ev_a = c->get_event();
+                    ev_b = c->get_event();
+                    cudaEventRecord(ev_a, c->stream);
+                }
                 if ((rc = c->cuda(cudaGraphLaunch(K.gexec, c->stream), "graph launch"))) return rc;
+                if (c->timing) {
+                    cudaEventRecord(ev_b, c->stream);
+                    c->timed.push_back({kModeStep + (K.dtype == EDK_F32 ? 4 : 0), ev_a, ev_b,
+                                        2.0 * (double)K.h->dim, 2});
+                    if (c->timed.size() > 16384) c->drain_timing();
+                }
                 c->launches += 2;
                 K.k += 2;
             }

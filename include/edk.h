@@ -44,7 +44,7 @@ extern "C" {
 #define EDK_F32 1   /* FP32 vectors; H*v coefficients, accumulation, norms, alpha/beta in FP64 */
 
 typedef struct edk_ctx edk_ctx;   /* device, stream, workspaces */
-typedef struct edk_h edk_h;       /* one (N_up, N_dn) sector Hamiltonian on the device */
+typedef struct edk_h edk_h;       /* one sector Hamiltonian on the device: (N_up, N_dn) or Nambu */
 
 /* Anderson impurity model (replaces the AIM_type / JJmatrix globals read by
  * new_HAIMupdo, HAIMupdo.f90:53-121).  Matrices are row-major, spin-major:
@@ -83,9 +83,10 @@ int edk_ctx_timing(edk_ctx *ctx, int enable);
  * their number), for measurements. */
 int edk_ctx_set_kernel_path(edk_ctx *ctx, int path);
 /* 1 (default): Lanczos passes and Green chains replay pairs of fused steps as
- * one CUDA graph launch (captured once per run, from the third step on, on
- * the context's stream; not while per-launch timing is on); 0: plain launches.
- * Results are identical either way. */
+ * one CUDA graph launch (captured once per run, from the third step on, on a
+ * private stream, replayed on the context's stream); 0: plain launches.
+ * Results are identical either way.  With per-launch timing on, a replay is
+ * timed as a whole and counted as its two fused-step launches. */
 int edk_ctx_set_graphs(edk_ctx *ctx, int enable);
 int edk_ctx_timing_report(edk_ctx *ctx, int which, int64_t *launches, double *total_ms);
 /* Sum over the timed launches of class `which` of the sector dimension each

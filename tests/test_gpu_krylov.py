@@ -227,3 +227,23 @@ def test_graph_replayed_steps_equal_plain_launches(ctx):
         ctx.set_graphs(True)
         for a, b in zip(res[0], res[1]):
             assert np.array_equal(a, b)
+
+
+def test_timing_counts_graph_replays_as_their_launches(ctx):
+    """Per-launch timing with graph replay on: a replay is timed as a whole and
+    counted as its two fused steps, so the fused-step count equals the plain
+    launches' count and the coefficients stay bit-identical."""
+    w = workload("c3")
+    h = edk.Hamiltonian(ctx, w.model, 7, 7)
+    out = []
+    for g in (False, True):
+        ctx.set_graphs(g)
+        ctx.timing(True)
+        r = h.lanczos_e0("f64", nitermax=40, tolerance=0.0, check_every=40)
+        n, ms, el = ctx.timing_report(2)
+        ctx.timing(False)
+        out.append((r["diag"], n, ms, el))
+    ctx.set_graphs(True)
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1] == out[1][1] == len(out[0][0]) - 1
+    assert out[1][2] > 0.0 and out[1][3] == out[0][3]
