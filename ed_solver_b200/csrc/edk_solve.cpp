@@ -21,6 +21,7 @@
 // latency, so FP32 storage would add rounding without saving time.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -54,6 +55,7 @@ struct State {
     int dtype;                 // element type of psi
     DBuf psi;
     double boltz = 0.0;
+    int converged = 1;
 };
 
 }  // namespace
@@ -120,9 +122,62 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
     double e0_low = 1e300;
     const int cap = std::max(4, o->nitermax + 4);
     std::vector<double> diag(cap), sub(cap), vecp((size_t)cap * std::max(1, o->neigen));
-    for (int s = 0; s < o->nsectors; ++s) {
+    // ed.sector_bound_file: when present only the window around its bounds is scanned
+    int32_t bounds[6] = {0, 0, 0, 0, 1000, -1000};
+    bool bounds_present = false;
+    if (o->sector_bound_file) {
+        if (FILE *bf = std::fopen(o->sector_bound_file, "r")) {
+            std::fclose(bf);
+            if (edk_sector_bounds_read(o->sector_bound_file, bounds, nullptr) != EDK_OK)
+                return edk_internal_fail(ctx, EDK_ERR_INVALID, "unreadable sector bound file");
+            bounds_present = true;
+        }
+    }
+    if (o->gs_in) {
+        // the eigenstates of a GS.raw file replace the scan (solver.f90:70-81)
+        int32_t ne = 0;
+        int64_t tot = 0;
+        if (edk_gs_read(o->gs_in, 0, nullptr, &ne, 0, nullptr, &tot) != EDK_OK)
+            return edk_internal_fail(ctx, EDK_ERR_INVALID, "unreadable GS file");
+        std::vector<edk_gs_entry> ent((size_t)std::max(ne, 1));
+        std::vector<double> pool((size_t)std::max<int64_t>(tot, 1));
+        if (edk_gs_read(o->gs_in, ne, ent.data(), &ne, tot, pool.data(), &tot) != EDK_OK)
+            return edk_internal_fail(ctx, EDK_ERR_INVALID, "unreadable GS file");
+        for (int k = 0; k < ne; ++k) {
+            const edk_gs_entry &e = ent[k];
+            // INCONSISTENT INPUT SECTOR of init_solver (solver_init.h:174-178)
+            if (e.kind != 0 || e.norbs != ns) return edk_internal_fail(ctx, EDK_ERR_INVALID, "GS file: sector of another model");
+            edk_h *h = nullptr;
+            if ((rc = getH(e.nup, e.ndn, &h))) return rc;
+            int64_t dim = 0;
+            edk_h_dims(h, &dim, nullptr, nullptr);
+            if (e.n != dim) return edk_internal_fail(ctx, EDK_ERR_INVALID, "GS file: vector length");
+            auto stt = std::make_unique<State>();
+            stt->nup = e.nup; stt->ndn = e.ndn; stt->E = e.val; stt->E_pass1 = e.val;
+            stt->converged = e.converged;
+            stt->dtype = sector_dtype(dim);
+            DBuf p64((size_t)dim * 8);
+            if (!p64.p) return edk_internal_fail(ctx, EDK_ERR_NOMEM, "state vector");
+            cudaMemcpyAsync(p64.p, pool.data() + e.offset, (size_t)dim * 8, cudaMemcpyHostToDevice, st);
+            edk_internal_count(ctx, dim * 8, 0);
+            if (stt->dtype == EDK_F64) {
+                stt->psi = std::move(p64);
+            } else {
+                stt->psi = DBuf((size_t)dim * 4);
+                if ((rc = edk_convert(ctx, EDK_F64, EDK_F32, dim, p64.p, stt->psi.p))) return rc;
+            }
+            if (cudaStreamSynchronize(st) != cudaSuccess) return edk_internal_fail(ctx, EDK_ERR_CUDA, "upload");
+            states.push_back(std::move(stt));
+        }
+    }
+    for (int s = 0; s < (o->gs_in ? 0 : o->nsectors); ++s) {
         const int nu = o->sectors[2 * s], nd = o->sectors[2 * s + 1];
         if (nu < 0 || nu > ns || nd < 0 || nd > ns) return edk_internal_fail(ctx, EDK_ERR_INVALID, "sector");
+        if (bounds_present) {
+            // goforit of get_eigen_energies (solver.h:134-137)
+            const int w = o->iwindow;
+            if (!(nu <= bounds[1] + w && nd <= bounds[3] + w && nu >= bounds[0] - w && nd >= bounds[2] - w)) continue;
+        }
         edk_h *h = nullptr;
         if ((rc = getH(nu, nd, &h))) return rc;
         int64_t dim = 0;
@@ -179,6 +234,7 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
             for (int k = 0; k < lr.nkept; ++k) {
                 auto stt = std::make_unique<State>();
                 stt->nup = nu; stt->ndn = nd; stt->E = lr.E[k]; stt->E_pass1 = lr.E[k]; stt->dtype = sdt;
+                stt->converged = lr.converged[k];
                 stt->psi = DBuf((size_t)dim * ebytes);
                 if (!stt->psi.p) return edk_internal_fail(ctx, EDK_ERR_NOMEM, "state vector");
                 if ((rc = edk_lanczos_gs(h, &lo, lr.niter, lr.vecp + (size_t)k * lr.niter, stt->psi.p))) return rc;
@@ -231,6 +287,52 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
     double z = 0.0;
     for (auto &s : gs) z += std::exp(-o->beta * (s->E - e0));
     for (auto &s : gs) s->boltz = std::exp(-o->beta * (s->E - e0)) / z;
+    if (o->gs_out) {
+        // write_raw_eigensectorlist of the states in the window (solver.f90:104-108)
+        std::vector<edk_gs_entry> ent;
+        std::vector<double> pool;
+        for (size_t k = 0; k < gs.size(); ++k) {
+            edk_h *h = nullptr;
+            if ((rc = getH(gs[k]->nup, gs[k]->ndn, &h))) return rc;
+            int64_t dim = 0;
+            edk_h_dims(h, &dim, nullptr, nullptr);
+            edk_gs_entry e{};
+            e.kind = 0;
+            e.norbs = ns;
+            e.nup = gs[k]->nup;
+            e.ndn = gs[k]->ndn;
+            e.val = gs[k]->E;
+            e.converged = gs[k]->converged;
+            e.rank = (k > 0 && gs[k - 1]->nup == e.nup && gs[k - 1]->ndn == e.ndn) ? ent.back().rank + 1 : 1;
+            e.n = dim;
+            e.offset = (int64_t)pool.size();
+            pool.resize(pool.size() + (size_t)dim);
+            DBuf p64;
+            const void *p = gs[k]->psi.p;
+            if (gs[k]->dtype != EDK_F64) {
+                p64 = DBuf((size_t)dim * 8);
+                if ((rc = edk_convert(ctx, gs[k]->dtype, EDK_F64, dim, gs[k]->psi.p, p64.p))) return rc;
+                p = p64.p;
+            }
+            if (cudaMemcpyAsync(pool.data() + e.offset, p, (size_t)dim * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess)
+                return edk_internal_fail(ctx, EDK_ERR_CUDA, "state download");
+            edk_internal_count(ctx, 0, dim * 8);
+            ent.push_back(e);
+        }
+        if (edk_gs_write(o->gs_out, (int32_t)ent.size(), ent.data(), pool.data()) != EDK_OK)
+            return edk_internal_fail(ctx, EDK_ERR_INVALID, "cannot write the GS file");
+    }
+    if (bounds_present) {
+        // get_new_bounds (solver.h:374-415): the particle numbers of the kept states
+        int32_t nb6[6] = {1000, -1000, 1000, -1000, 1000, -1000};
+        for (auto &s : gs) {
+            nb6[0] = std::min(nb6[0], s->nup); nb6[1] = std::max(nb6[1], s->nup);
+            nb6[2] = std::min(nb6[2], s->ndn); nb6[3] = std::max(nb6[3], s->ndn);
+        }
+        if (edk_sector_bounds_write(o->sector_bound_file, nb6) != EDK_OK)
+            return edk_internal_fail(ctx, EDK_ERR_INVALID, "cannot write the sector bound file");
+    }
     r->e0 = e0;
     r->z = z;
     r->e0_lowprec = e0_low;

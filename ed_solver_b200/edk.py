@@ -67,7 +67,14 @@ class _SolveOpts(C.Structure):
                 ("check_every", C.c_int32), ("beta", C.c_double), ("demax0", C.c_double),
                 ("nitergreen", C.c_int32), ("nw", C.c_int32), ("spin_mask", C.c_int32), ("npairs", C.c_int32),
                 ("pairs", C.c_void_p), ("cutoff_dynamic", C.c_double), ("ran_tab", C.c_void_p),
-                ("residual_tol", C.c_double), ("green_mode", C.c_int32)]
+                ("residual_tol", C.c_double), ("green_mode", C.c_int32), ("gs_in", C.c_char_p),
+                ("gs_out", C.c_char_p), ("sector_bound_file", C.c_char_p), ("iwindow", C.c_int32)]
+
+
+class _GsEntry(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("norbs", C.c_int32), ("nup", C.c_int32), ("ndn", C.c_int32),
+                ("val", C.c_double), ("converged", C.c_int32), ("rank", C.c_int32), ("n", C.c_int64),
+                ("offset", C.c_int64)]
 
 
 class _SolveResult(C.Structure):
@@ -198,6 +205,10 @@ def lib():
         "edk_block_lanczos": (C.c_int, [P, P, P, P, P, P]),
         "edk_grad_e0": (C.c_int, [P, P, I32, P, P]),
         "edk_grad_green": (C.c_int, [P, P, D, I32, P, I32, I32, P, P, D, I32, P, D, P, P, P]),
+        "edk_gs_write": (C.c_int, [C.c_char_p, I32, P, P]),
+        "edk_gs_read": (C.c_int, [C.c_char_p, I32, P, P, I64, P, P]),
+        "edk_sector_bounds_read": (C.c_int, [C.c_char_p, P, P]),
+        "edk_sector_bounds_write": (C.c_int, [C.c_char_p, P]),
         "edk_h_create_sz": (C.c_int, [P, P, C.c_int, P]),
         "edk_h_sz_info": (C.c_int, [P, P, P]),
         "edk_apply_csz": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, P, P,
@@ -649,10 +660,65 @@ def green_batch(ctx: Context, chains, nitergreen: int, wn, nout: int, mode: int 
     return G[..., 0] + 1j * G[..., 1], stats
 
 
+def gs_write(path: str, entries):
+    """write_raw_eigensectorlist: entries = list of dict(kind (0 updo, 1 sz), norbs, nup, ndn,
+    val, converged, rank, vec); consecutive entries of one sector form one eigensector."""
+    arr = (_GsEntry * max(len(entries), 1))()
+    vecs, off = [], 0
+    for i, e in enumerate(entries):
+        v = np.ascontiguousarray(e["vec"], np.float64)
+        arr[i] = _GsEntry(int(e.get("kind", 0)), int(e["norbs"]), int(e["nup"]), int(e.get("ndn", -1)),
+                          float(e["val"]), int(bool(e.get("converged", True))), int(e.get("rank", i + 1)),
+                          len(v), off)
+        vecs.append(v)
+        off += len(v)
+    pool = np.concatenate(vecs) if vecs else np.zeros(1)
+    rc = lib().edk_gs_write(path.encode(), len(entries), C.cast(arr, C.c_void_p), pool.ctypes.data)
+    if rc:
+        raise EdkError(rc, f"edk_gs_write({path})")
+
+
+def gs_read(path: str):
+    """read_raw_eigensectorlist: the entries of a GS.raw file as dicts with their vectors."""
+    n, tot = C.c_int32(), C.c_int64()
+    rc = lib().edk_gs_read(path.encode(), 0, None, C.byref(n), 0, None, C.byref(tot))
+    if rc:
+        raise EdkError(rc, f"edk_gs_read({path})")
+    arr = (_GsEntry * max(n.value, 1))()
+    pool = np.zeros(max(tot.value, 1))
+    rc = lib().edk_gs_read(path.encode(), n.value, C.cast(arr, C.c_void_p), C.byref(n), tot.value,
+                           pool.ctypes.data, C.byref(tot))
+    if rc:
+        raise EdkError(rc, f"edk_gs_read({path})")
+    out = []
+    for i in range(n.value):
+        e = arr[i]
+        out.append(dict(kind=e.kind, norbs=e.norbs, nup=e.nup, ndn=e.ndn, val=e.val, converged=bool(e.converged),
+                        rank=e.rank, vec=pool[e.offset:e.offset + e.n].copy()))
+    return out
+
+
+def sector_bounds_read(path: str):
+    """ed.sector_bound_file: ((nupmin, nupmax), (ndnmin, ndnmax), (szmin, szmax) or None)."""
+    b = np.zeros(6, np.int32)
+    has = C.c_int32()
+    rc = lib().edk_sector_bounds_read(path.encode(), b.ctypes.data, C.byref(has))
+    if rc:
+        raise EdkError(rc, f"edk_sector_bounds_read({path})")
+    return (int(b[0]), int(b[1])), (int(b[2]), int(b[3])), ((int(b[4]), int(b[5])) if has.value else None)
+
+
+def sector_bounds_write(path: str, nup, ndn, sz=(1000, -1000)):
+    b = np.array([nup[0], nup[1], ndn[0], ndn[1], sz[0], sz[1]], np.int32)
+    rc = lib().edk_sector_bounds_write(path.encode(), b.ctypes.data)
+    if rc:
+        raise EdkError(rc, f"edk_sector_bounds_write({path})")
+
+
 def solve(ctx: Context, model: AIMModel, sectors, beta: float, nw: int, dtype="f64", neigen=1,
           nitermax=1000, tolerance=1e-12, tolerance_lowprec=1e-6, demax0=5.0, nitergreen=200,
           spins=(0, 1), pairs=None, cutoff_dynamic=1e-8, check_every=8, ran_tab=None, residual_tol=0.0,
-          green_mode=0):
+          green_mode=0, gs_in=None, gs_out=None, sector_bound_file=None, iwindow=1):
     """One impurity solve through the C-ABI (edk_solve): host inputs, host outputs.
 
     Returns dict(e0, z, residual, nstates, lanczos_steps, green_steps, G (2, npairs, nw) complex,
@@ -667,7 +733,9 @@ def solve(ctx: Context, model: AIMModel, sectors, beta: float, nw: int, dtype="f
     o = _SolveOpts(_dtype_code(dtype), len(sec) // 2, sec.ctypes.data, int(neigen), int(nitermax), float(tolerance),
                    float(tolerance_lowprec), int(check_every), float(beta), float(demax0), int(nitergreen),
                    int(nw), int(mask), len(pr) // 2, pr.ctypes.data, float(cutoff_dynamic),
-                   None if tab is None else tab.ctypes.data, float(residual_tol), int(green_mode))
+                   None if tab is None else tab.ctypes.data, float(residual_tol), int(green_mode),
+                   None if gs_in is None else gs_in.encode(), None if gs_out is None else gs_out.encode(),
+                   None if sector_bound_file is None else sector_bound_file.encode(), int(iwindow))
     G = np.zeros((2, len(pr) // 2, nw, 2))
     docc = np.zeros(model.nc)
     en = np.zeros(64)

@@ -27,6 +27,14 @@ module edk_fortran
     integer(c_int32_t) :: on_fly
   end type
 
+  ! one eigenstate of a GS.raw checkpoint (write_raw_eigensectorlist, eigen_sector_class.f90:514-567)
+  type, bind(C) :: edk_gs_entry
+    integer(c_int32_t) :: kind, norbs, nup, ndn
+    real(c_double) :: val
+    integer(c_int32_t) :: converged, rank
+    integer(c_int64_t) :: n, offset
+  end type
+
   type, bind(C) :: edk_lanczos_opts
     integer(c_int32_t) :: nitermax, neigen
     real(c_double) :: tolerance, demax, cutoff_min_lanczos_vec
@@ -136,6 +144,36 @@ module edk_fortran
       real(c_double), intent(in) :: wn(*)
       real(c_double), intent(out) :: G(*), diag(*), subdiag(*)
       integer(c_int32_t) :: niter_done
+    end function
+
+    ! GS.raw checkpoints and ed.sector_bound_file (host-only)
+    integer(c_int) function edk_gs_write(path, nentries, entries, pool) bind(C, name="edk_gs_write")
+      import :: c_int, c_char, c_int32_t, c_double, edk_gs_entry
+      character(kind=c_char), intent(in) :: path(*)
+      integer(c_int32_t), value :: nentries
+      type(edk_gs_entry), intent(in) :: entries(*)
+      real(c_double), intent(in) :: pool(*)
+    end function
+    integer(c_int) function edk_gs_read(path, cap, entries, nentries, vec_cap, pool, vec_total) &
+        bind(C, name="edk_gs_read")
+      import :: c_int, c_char, c_int32_t, c_int64_t, c_double, edk_gs_entry
+      character(kind=c_char), intent(in) :: path(*)
+      integer(c_int32_t), value :: cap
+      type(edk_gs_entry) :: entries(*)
+      integer(c_int32_t) :: nentries
+      integer(c_int64_t), value :: vec_cap
+      real(c_double) :: pool(*)
+      integer(c_int64_t) :: vec_total
+    end function
+    integer(c_int) function edk_sector_bounds_read(path, bounds, has_sz) bind(C, name="edk_sector_bounds_read")
+      import :: c_int, c_char, c_int32_t
+      character(kind=c_char), intent(in) :: path(*)
+      integer(c_int32_t) :: bounds(6), has_sz
+    end function
+    integer(c_int) function edk_sector_bounds_write(path, bounds) bind(C, name="edk_sector_bounds_write")
+      import :: c_int, c_char, c_int32_t
+      character(kind=c_char), intent(in) :: path(*)
+      integer(c_int32_t), intent(in) :: bounds(6)
     end function
 
     ! new_HAIMsz (HAIMsz.f90:51-82): the sector of npart Nambu particles

@@ -368,6 +368,16 @@ typedef struct edk_solve_opts {
     int32_t green_mode;          /* 0: the chains of target sectors below 2^20 states (FP64)
                                     run together in one persistent edk_green_batch launch per
                                     spin; 1: every chain on its own (edk_green_chain) */
+    const char *gs_in;           /* NULL, or a GS.raw file (edk_gs_write): its eigenstates replace
+                                    the sector scan, as solve_AIM does on its first call with an
+                                    old GS (solver.f90:70-81, solver_init.h:163-182) */
+    const char *gs_out;          /* NULL, or the path the eigenstates of the window are written to
+                                    in GS.raw form (solver.f90:104-108) */
+    const char *sector_bound_file;  /* NULL, or an ed.sector_bound_file: when it exists, only
+                                    sectors with nup, ndn within the bounds +/- iwindow are scanned
+                                    (solver.h:107-137), and the bounds of the states found are
+                                    written back to it (get_new_bounds, solver.h:374-415) */
+    int32_t iwindow;             /* window around the bounds (reference default 1) */
 } edk_solve_opts;
 
 typedef struct edk_solve_result {
@@ -384,6 +394,40 @@ typedef struct edk_solve_result {
 } edk_solve_result;
 
 int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_solve_result *r);
+
+/* ---- eigenstate checkpoints: GS.raw (eigen_sector_class.f90:514-567) ------
+ * The list-directed text file of write_raw_eigensectorlist: per sector a
+ * T record, the sector ('updo' then norbs and npart of each spin species,
+ * quantum_fermion_sector_class.f90:398-403; or 'sz' then norbs and npart,
+ * quantum_fermion_hilbert_class.f90:190-195) and its eigenlist (per state:
+ * T, the eigenvalue, the converged flag, the rank, the vector length and the
+ * vector, eigen_class.f90:479-491, rcvector_class.f90:217-229, closed by F);
+ * a final F.  The reader accepts any list-directed layout of those values
+ * (line breaks inside the vector, commas, r*c repeat counts, .TRUE./.FALSE.,
+ * quoted or bare sector names), as a Fortran READ(UNIT,*) does; each record
+ * of the reference's starts on a new line.  Host-only. */
+typedef struct edk_gs_entry {
+    int32_t kind;                /* 0: (N_up, N_dn) sector, 1: Nambu (sz) sector */
+    int32_t norbs;               /* orbitals per spin species (kind 0) or Nambu orbitals (kind 1) */
+    int32_t nup, ndn;            /* kind 0: particle numbers; kind 1: nup = npart, ndn = -1 */
+    double val;                  /* eigenvalue */
+    int32_t converged;
+    int32_t rank;
+    int64_t n;                   /* vector length */
+    int64_t offset;              /* first element of the vector in the vector pool */
+} edk_gs_entry;
+/* Entries of the same sector must be consecutive: each run is one eigensector. */
+int edk_gs_write(const char *path, int32_t nentries, const edk_gs_entry *entries, const double *vec_pool_host);
+/* Call with entries = NULL and vec_pool = NULL to get *nentries and
+ * *vec_total, then with capacities at least those; offsets are assigned in
+ * file order. */
+int edk_gs_read(const char *path, int32_t cap, edk_gs_entry *entries, int32_t *nentries, int64_t vec_cap,
+                double *vec_pool_host, int64_t *vec_total);
+/* ed.sector_bound_file (solver.h:107-119, 396-402): bounds[6] = nupmin, nupmax,
+ * ndnmin, ndnmax, szmin, szmax.  Reading a file without the third record
+ * leaves szmin = 1000, szmax = -1000 and sets *has_sz = 0.  Host-only. */
+int edk_sector_bounds_read(const char *path, int32_t *bounds, int32_t *has_sz);
+int edk_sector_bounds_write(const char *path, const int32_t *bounds);
 
 /* ---- Nambu (Sz) sectors: HAIMsz (HAIMsz.f90:51-1027) ----------------------
  * The superconducting basis of new_HAIMsz: one species of 2*ns orbitals, up

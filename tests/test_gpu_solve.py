@@ -111,3 +111,43 @@ def test_batched_chains_in_the_solve_equal_per_chain_runs(ctx):
     assert r0["nstates"] == r1["nstates"] and r0["e0"] == r1["e0"]
     assert r0["green_steps"] == r1["green_steps"]
     assert np.abs(r0["G"] - r1["G"]).max() < 1e-9 * max(1.0, np.abs(r1["G"]).max())
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_resume_from_gs_file_gives_the_same_green_function(ctx, tmp_path, dtype):
+    """gs_out writes the window's eigenstates in GS.raw form; a solve started
+    from that file (gs_in, no sector scan) gives the same E0, weights and G bit
+    for bit.  ns=14 (7,7) for the mixed path (its FP32 vectors round-trip
+    through FP64 exactly), ns=8 for FP64."""
+    w = workload("c3" if dtype == "f32" else "c1")
+    kw = dict(dtype=dtype, nitergreen=w.nitergreen if dtype == "f64" else 60, spins=(0, 1), tolerance=1e-12,
+              residual_tol=1e-10)
+    p = str(tmp_path / "GS.raw")
+    r1 = edk.solve(ctx, w.model, w.sectors, w.beta, 64, gs_out=p, **kw)
+    ents = edk.gs_read(p)
+    assert len(ents) == r1["nstates"]
+    assert ents[0]["val"] == r1["e0"] and (ents[0]["nup"], ents[0]["ndn"]) == w.sectors[0]
+    r2 = edk.solve(ctx, w.model, w.sectors, w.beta, 64, gs_in=p, **kw)
+    assert r2["lanczos_steps"] == 0
+    assert r2["e0"] == r1["e0"] and r2["z"] == r1["z"]
+    assert np.array_equal(r2["G"], r1["G"])
+
+
+def test_sector_bound_file_restricts_the_scan(ctx, tmp_path):
+    """With ed.sector_bound_file present only sectors within its bounds +/-
+    iwindow are scanned, and the file is rewritten with the bounds of the
+    states kept (two-orbital model, 121 sectors)."""
+    w = workload("c2")
+    kw = dict(dtype="f64", nitergreen=50, spins=(0,), pairs=[(0, 0)], tolerance=1e-10)
+    full = edk.solve(ctx, w.model, w.sectors, w.beta, 16, **kw)
+    nu, nd = full["sectors"][0]
+    p = str(tmp_path / "ed.sector_bound_file")
+    edk.sector_bounds_write(p, (nu, nu), (nd, nd))
+    r = edk.solve(ctx, w.model, w.sectors, w.beta, 16, sector_bound_file=p, iwindow=1, **kw)
+    assert r["lanczos_steps"] < full["lanczos_steps"]
+    assert abs(r["e0"] - full["e0"]) < 1e-9 * abs(full["e0"])
+    kept = set(r["sectors"])
+    b = edk.sector_bounds_read(p)
+    assert b[0] == (min(s[0] for s in kept), max(s[0] for s in kept))
+    assert b[1] == (min(s[1] for s in kept), max(s[1] for s in kept))
+    assert all(abs(s[0] - nu) <= 1 and abs(s[1] - nd) <= 1 for s in kept)
