@@ -69,12 +69,45 @@ void edk_internal_cache_put(edk_ctx *ctx, const char *key, size_t len, edk_h *h)
 cudaStream_t edk_internal_stream(edk_ctx *ctx);
 int edk_internal_fail(edk_ctx *ctx, int code, const char *msg);
 void edk_internal_count(edk_ctx *ctx, int64_t h2d, int64_t d2h);
+edk_ctx *edk_internal_h_ctx(edk_h *h);
 
 int edk_convert(edk_ctx *ctx, int from_dtype, int to_dtype, int64_t n, const void *in_dev, void *out_dev)
 {
     if (!ctx || !in_dev || !out_dev || n < 0) return EDK_ERR_INVALID;
     cudaError_t e = edk::launch_convert(from_dtype, to_dtype, n, in_dev, out_dev, edk_internal_stream(ctx));
     if (e != cudaSuccess) return edk_internal_fail(ctx, EDK_ERR_CUDA, cudaGetErrorString(e));
+    return EDK_OK;
+}
+
+int edk_full_ed(edk_h *h, double *E_host, double *V_host)
+{
+    if (!h || !E_host) return EDK_ERR_INVALID;
+    edk_ctx *ctx = edk_internal_h_ctx(h);
+    int64_t dim = 0;
+    edk_h_dims(h, &dim, nullptr, nullptr);
+    if (dim < 1 || dim > 4096) return edk_internal_fail(ctx, EDK_ERR_INVALID, "full ED: dimension outside [1, 4096]");
+    cudaStream_t st = edk_internal_stream(ctx);
+    // the FP64 matrix from H*v on the unit vectors
+    DBuf ein((size_t)dim * 8), hout((size_t)dim * 8), all((size_t)dim * dim * 8);
+    if (!ein.p || !hout.p || !all.p) return edk_internal_fail(ctx, EDK_ERR_NOMEM, "full ED");
+    std::vector<double> unit((size_t)dim, 0.0);
+    int rc;
+    for (int64_t i = 0; i < dim; ++i) {
+        unit.assign((size_t)dim, 0.0);
+        unit[(size_t)i] = 1.0;
+        if (cudaMemcpyAsync(ein.p, unit.data(), (size_t)dim * 8, cudaMemcpyHostToDevice, st) != cudaSuccess)
+            return edk_internal_fail(ctx, EDK_ERR_CUDA, "full ED upload");
+        if ((rc = edk_hmult(h, EDK_F64, dim, ein.p, (char *)all.p + (size_t)i * dim * 8))) return rc;
+        if (cudaStreamSynchronize(st) != cudaSuccess) return edk_internal_fail(ctx, EDK_ERR_CUDA, "full ED");
+    }
+    edk_internal_count(ctx, dim * dim * 8, dim * dim * 8);
+    std::vector<double> Hd((size_t)dim * dim), w, V;
+    if (cudaMemcpy(Hd.data(), all.p, (size_t)dim * dim * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return edk_internal_fail(ctx, EDK_ERR_CUDA, "full ED download");
+    // column i of the buffer is H e_i; H is symmetric, so the row-major reading is H
+    edk::dense_eigh((int)dim, Hd, w, V);
+    for (int64_t i = 0; i < dim; ++i) E_host[i] = w[(size_t)i];
+    if (V_host) std::memcpy(V_host, V.data(), sizeof(double) * (size_t)dim * dim);
     return EDK_OK;
 }
 

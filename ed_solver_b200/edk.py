@@ -71,6 +71,10 @@ class _SolveOpts(C.Structure):
                 ("gs_out", C.c_char_p), ("sector_bound_file", C.c_char_p), ("iwindow", C.c_int32)]
 
 
+class _ChilocSectors(C.Structure):
+    _fields_ = [("dim", C.c_int32 * 11), ("E", C.c_void_p * 11), ("C", C.c_void_p * 14)]
+
+
 class _GsEntry(C.Structure):
     _fields_ = [("kind", C.c_int32), ("norbs", C.c_int32), ("nup", C.c_int32), ("ndn", C.c_int32),
                 ("val", C.c_double), ("converged", C.c_int32), ("rank", C.c_int32), ("n", C.c_int64),
@@ -209,6 +213,8 @@ def lib():
         "edk_gs_read": (C.c_int, [C.c_char_p, I32, P, P, I64, P, P]),
         "edk_sector_bounds_read": (C.c_int, [C.c_char_p, P, P]),
         "edk_sector_bounds_write": (C.c_int, [C.c_char_p, P]),
+        "edk_full_ed": (C.c_int, [P, P, P]),
+        "edk_chiloc": (C.c_int, [P, I32, D, D, D, D, I32, I32, I32, P, I32, P, P, P]),
         "edk_h_create_sz": (C.c_int, [P, P, C.c_int, P]),
         "edk_h_sz_info": (C.c_int, [P, P, P]),
         "edk_apply_csz": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, P, P,
@@ -475,6 +481,14 @@ class Hamiltonian:
                        "edk_lanczos_gs")
         return psi
 
+    def full_ed(self, vectors=True):
+        """ED_diago: every eigenpair (E ascending, V columns) of this sector."""
+        E = np.zeros(self.dim)
+        V = np.zeros((self.dim, self.dim)) if vectors else None
+        self.ctx.check(lib().edk_full_ed(self.h, E.ctypes.data, None if V is None else V.ctypes.data),
+                       "edk_full_ed")
+        return E, V
+
     # ---- observables ----------------------------------------------------
     def double_occ(self, psi, site=0):
         d, n = C.c_double(), C.c_double()
@@ -658,6 +672,36 @@ def green_batch(ctx: Context, chains, nitergreen: int, wn, nout: int, mode: int 
                                     G.ctypes.data, int(mode), C.byref(st)), "edk_green_batch")
     stats = {f: getattr(st, f) for f, _ in _BatchStats._fields_}
     return G[..., 0] + 1j * G[..., 1], stats
+
+
+def chiloc(ctx: Context, E, M, w, beta: float, Z: float, gs_e: float, sites: int, nup: int, ndn: int,
+           ops=(1, 2), phi_eps: float = 1e-5):
+    """chi~_loc on the device for frequency triples w (nf x 3 complex): E[11]
+    sector energies (None outside the space), M[14] c+ matrices (target x
+    source), the reference's sector and matrix order.  Returns (pDNDN, pUPDN)
+    as complex arrays (None for an op not asked for)."""
+    w = np.asarray(w, np.complex128).reshape(-1, 3)
+    nf = len(w)
+    wr = np.ascontiguousarray(np.stack([w.real, w.imag], axis=-1).reshape(nf, 6))
+    st = _ChilocSectors()
+    keep = []
+    for q in range(11):
+        e = None if E[q] is None else np.ascontiguousarray(E[q], np.float64)
+        st.dim[q] = 0 if e is None else len(e)
+        st.E[q] = None if e is None else e.ctypes.data
+        keep.append(e)
+    for m in range(14):
+        x = None if M[m] is None else np.ascontiguousarray(M[m], np.float64)
+        st.C[m] = None if x is None else x.ctypes.data
+        keep.append(x)
+    mask = (1 if 1 in ops else 0) | (2 if 2 in ops else 0)
+    pd = np.zeros(2 * max(nf, 1))
+    pu = np.zeros(2 * max(nf, 1))
+    ctx.check(lib().edk_chiloc(ctx.h, mask, float(beta), float(Z), float(gs_e), float(phi_eps), int(sites),
+                               int(nup), int(ndn), C.byref(st), nf, wr.ctypes.data, pd.ctypes.data,
+                               pu.ctypes.data), "edk_chiloc")
+    f = lambda a: a[0:2 * nf:2] + 1j * a[1:2 * nf:2]
+    return (f(pd) if mask & 1 else None), (f(pu) if mask & 2 else None)
 
 
 def gs_write(path: str, entries):

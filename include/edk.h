@@ -474,6 +474,43 @@ int edk_h_sz_info(const edk_h *h, int32_t *npart, double *energy_shift);
 int edk_apply_csz(edk_h *src, int dtype, int site, int spin, int dagger, int projected, int site2, int sign2,
                   const void *in_dev, void *out_dev, int64_t *out_dim, int32_t *out_npart);
 
+/* ED_diago (ED_ARPACK.f90:590-715): every eigenpair of a sector by dense
+ * diagonalisation of the FP64 matrix that H*v gives on the unit vectors
+ * (cyclic Jacobi on the host).  E_host[dim] ascending; V_host (may be NULL)
+ * dim x dim row-major, column j = the eigenvector of E_host[j].  Sectors of
+ * at most 4096 states, either basis. */
+int edk_full_ed(edk_h *h, double *E_host, double *V_host);
+
+/* ---- local two-particle vertex chi~_loc (Chiloc_Wenhu_version3.cpp:29-989) ----
+ * chi_tilde_loc_ for many frequency triples at once: for each eigenstate i of
+ * the sector (nup, ndn) (energies E[0]), the Lehmann sum over the eigenstates
+ * j, k, l of its neighbour sectors of the Phi coefficients times four c+
+ * matrix elements, weighted by exp(-beta (E_i - gs_e)) / Z.  Sector slots:
+ *   0 i (nup,ndn)   1 pup (nup+1,ndn)   2 pdn (nup,ndn+1)   3 mup (nup-1,ndn)
+ *   4 mdn (nup,ndn-1)   5 p2dn (nup,ndn+2)   6 m2dn (nup,ndn-2)
+ *   7 puppdn (nup+1,ndn+1)   8 muppdn (nup-1,ndn+1)   9 pupmdn (nup+1,ndn-1)
+ *   10 mupmdn (nup-1,ndn-1)
+ * (dimension 0 for a sector outside the Hilbert space).  Matrix slots
+ * (<target| c+ |source>, row-major target x source, the reference's cp_*
+ * arrays):
+ *   0 i_cdup (pup<-i)  1 i_cddn (pdn<-i)  2 pup_cddn (puppdn<-pup)
+ *   3 pdn_cdup (puppdn<-pdn)  4 pdn_cddn (p2dn<-pdn)  5 mup_cdup (i<-mup)
+ *   6 mup_cddn (muppdn<-mup)  7 mdn_cddn (i<-mdn)  8 mdn_cdup (pupmdn<-mdn)
+ *   9 muppdn_cdup (pdn<-muppdn)  10 pupmdn_cddn (pup<-pupmdn)
+ *   11 mupmdn_cdup (mdn<-mupmdn)  12 mupmdn_cddn (mup<-mupmdn)  13 m2dn_cddn (mdn<-m2dn)
+ * w_host: nf x 6 doubles (re, im of w1, w2, w3).  op_mask bit 0: DNDN into
+ * pdndn_host, bit 1: UPDN into pupdn_host (nf x 2 doubles each).  phi_eps is
+ * the PHI_EPS threshold of the vanishing-denominator branches.  All arrays
+ * are host arrays. */
+typedef struct edk_chiloc_sectors {
+    int32_t dim[11];
+    const double *E[11];
+    const double *C[14];
+} edk_chiloc_sectors;
+int edk_chiloc(edk_ctx *ctx, int32_t op_mask, double beta, double Z, double gs_e, double phi_eps, int32_t sites,
+               int32_t nup, int32_t ndn, const edk_chiloc_sectors *s, int32_t nf, const double *w_host,
+               double *pdndn_host, double *pupdn_host);
+
 #ifdef __cplusplus
 }
 #endif

@@ -748,3 +748,89 @@ def lehmann_green(model: AIMModel, sectors, beta: float, wn: np.ndarray, site=0,
                 amp = float(vt[:, m] @ phi) ** 2
                 G += amp * (bn + bm) / (1j * wn - (wt[m] - w[n]))
     return G / z
+
+
+# ---------------------------------------------------------------------------
+# chi~_loc: the reference's own chi_tilde_loc_ (ed_solver/Chiloc_Wenhu_version3.cpp),
+# compiled unmodified into oracle/_ref by `make -C oracle ref`
+# ---------------------------------------------------------------------------
+
+CHILOC_SECTORS = [(0, 0), (1, 0), (0, 1), (-1, 0), (0, -1), (0, 2), (0, -2), (1, 1), (-1, 1), (1, -1), (-1, -1)]
+# (target slot, source slot, spin) of the 14 c+ matrices, in the reference's argument order
+CHILOC_MATRICES = [(1, 0, 0), (2, 0, 1), (7, 1, 1), (7, 2, 0), (5, 2, 1), (0, 3, 0), (8, 3, 1),
+                   (0, 4, 1), (9, 4, 0), (2, 8, 0), (1, 9, 1), (4, 10, 0), (3, 10, 1), (4, 6, 1)]
+_REF_CHILOC = None
+
+
+def ref_chiloc_path():
+    return os.path.join(_HERE, "_ref", "libchiloc_ref.so")
+
+
+def ref_chiloc_lib():
+    """The compiled reference (oracle/_ref/libchiloc_ref.so); None when it was not built."""
+    global _REF_CHILOC
+    if _REF_CHILOC is None and os.path.exists(ref_chiloc_path()):
+        _REF_CHILOC = C.CDLL(ref_chiloc_path())
+    return _REF_CHILOC
+
+
+def ref_chiloc(op, w, phi_eps, beta, Z, gs_e, sites, nup, ndn, E, M):
+    """chi_tilde_loc_ of the reference for one frequency triple w = (w1, w2, w3):
+    E[11] energy arrays, M[14] c+ matrices (target x source).  Returns
+    (pDNDN, pUPDN) as Python complex numbers."""
+    L = ref_chiloc_lib()
+    if L is None:
+        raise RuntimeError("oracle/_ref/libchiloc_ref.so is not built (make -C oracle ref)")
+    ci = lambda v: C.byref(C.c_int(int(v)))
+    cd = lambda v: C.byref(C.c_double(float(v)))
+    keep = []
+
+    def cplx(z):
+        a = np.array([z.real, z.imag], np.float64)
+        keep.append(a)
+        return a.ctypes.data_as(C.c_void_p)
+
+    def arr(a):
+        a = np.ascontiguousarray(a if a is not None and np.size(a) else np.zeros(1), np.float64).reshape(-1)
+        keep.append(a)
+        return a.ctypes.data_as(C.c_void_p)
+
+    args = [ci(op), cplx(w[0]), cplx(w[1]), cplx(w[2]), cd(phi_eps), cd(beta), cd(Z), cd(gs_e), ci(sites),
+            ci(nup), ci(ndn)]
+    for q in range(11):
+        args += [arr(E[q]), ci(0 if E[q] is None else len(E[q]))]
+    args += [ci(0)] * 28
+    for m in range(14):
+        args.append(arr(M[m]))
+    out_d = np.zeros(2)
+    out_u = np.zeros(2)
+    args += [out_d.ctypes.data_as(C.c_void_p), out_u.ctypes.data_as(C.c_void_p)]
+    L.chi_tilde_loc_(*args)
+    return complex(out_d[0], out_d[1]), complex(out_u[0], out_u[1])
+
+
+def chiloc_inputs(model: AIMModel, nup: int, ndn: int, site: int = 0):
+    """Full-ED eigenpairs of the 11 sectors around (nup, ndn) (dense Hmult__
+    columns, numpy eigh) and the 14 c+ matrices <t|c+_{site,spin}|s> between
+    their eigenbases (apply_Cupdo on every eigenvector), as the reference's
+    vertex tool assembles them (four_leg_vertex_matrices, Chiloc_four_leg.f90:200-444).
+    Returns (E[11] (None for sectors outside the space), M[14], V[11])."""
+    ns = model.ns
+    E, V = [None] * 11, [None] * 11
+    for q, (du, dd) in enumerate(CHILOC_SECTORS):
+        nu, nd = nup + du, ndn + dd
+        if 0 <= nu <= ns and 0 <= nd <= ns:
+            w, v = np.linalg.eigh(OracleH(model, nu, nd).dense())
+            E[q], V[q] = w, v
+    M = [None] * 14
+    for m, (t, s, spin) in enumerate(CHILOC_MATRICES):
+        if V[t] is None or V[s] is None:
+            continue
+        nu, nd = nup + CHILOC_SECTORS[s][0], ndn + CHILOC_SECTORS[s][1]
+        cols = []
+        for j in range(V[s].shape[1]):
+            out, _ = apply_c(model, nu, nd, site, spin, True, V[s][:, j])
+            cols.append(out)
+        CV = np.stack(cols, axis=1)                     # c+ V_s in the target's Fock basis
+        M[m] = V[t].T @ CV                               # target x source
+    return E, M, V
