@@ -456,6 +456,67 @@ def run_sz(args):
     ctx.close()
 
 
+def run_chiloc(args):
+    """The local vertex chi~_loc (DNDN and UPDN) of the ns = 4 star model
+    (1 impurity + 3 bath sites, U = 2, seeded bath), sector (2,2) (36 states;
+    neighbour sectors of 1 to 36 states), beta = 10, for 4096 frequency
+    triples (w1, w2, w3) = (i nu_a, i nu_b, i nu_c) on a grid of fermionic
+    Matsubara frequencies, every third one with w2 + w3 = 0.  One step = one
+    edk_chiloc call for all triples (inputs uploaded from host arrays, results
+    read back).  The reference's own chi_tilde_loc_ (oracle/_ref, serial C++)
+    is timed on the first 8 triples of the same batch."""
+    import numpy as np
+    import torch
+    from ed_solver_b200 import edk, vertex
+    from ed_solver_b200.model import star_model
+    rng = np.random.default_rng(5)
+    m = star_model(-1.0, 2.0, rng.uniform(-1.0, 1.0, 3), rng.uniform(0.3, 0.6, 3))
+    beta, eps, nup, ndn = 10.0, 1e-5, 2, 2
+    ctx = edk.Context(0)
+    E, M = vertex.vertex_inputs(ctx, m, nup, ndn)
+    Z, gs = vertex.partition(E, beta)
+    nu = lambda n: 1j * (2 * n + 1) * np.pi / beta
+    w = []
+    for a in range(-8, 8):
+        for b in range(-8, 8):
+            for c in range(-8, 8):
+                w.append((nu(a), nu(b), -nu(b) if (a + b + c) % 3 == 0 else nu(c)))
+    w = np.array(w)
+    nf = len(w)
+    # algorithmic work: (j, k, l) evaluations of every active term over all states i and triples
+    dims = [0 if e is None else len(e) for e in E]
+    for _ in range(2):
+        edk.chiloc(ctx, E, M, w, beta, Z, gs, m.ns, nup, ndn, phi_eps=eps)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    steps = max(args.steps, 3)
+    e0.record()
+    for _ in range(steps):
+        pd, pu = edk.chiloc(ctx, E, M, w, beta, Z, gs, m.ns, nup, ndn, phi_eps=eps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    out = {"workload": "chiloc_ns4_sector22_4096_triples", "dims": dims, "triples": nf,
+           "gpu_ms_per_call": ms, "gpu_triples_per_s": nf / (ms * 1e-3)}
+    if not args.no_cpu:
+        import oracle as O
+        if O.ref_chiloc_lib() is not None:
+            ns_cpu = 8
+            t0 = time.perf_counter()
+            ref = [(O.ref_chiloc(1, t, eps, beta, Z, gs, m.ns, nup, ndn, E, M)[0],
+                    O.ref_chiloc(2, t, eps, beta, Z, gs, m.ns, nup, ndn, E, M)[1]) for t in w[:ns_cpu]]
+            t1 = time.perf_counter()
+            out["cpu_reference"] = {"kind": "reference", "cores": 1, "sample": f"first {ns_cpu} triples",
+                                    "triples_per_s": ns_cpu / (t1 - t0)}
+            rd = np.array([r[0] for r in ref])
+            ru = np.array([r[1] for r in ref])
+            out["max_rel_diff_vs_reference"] = float(max(np.abs(pd[:ns_cpu] - rd).max() / np.abs(rd).max(),
+                                                         np.abs(pu[:ns_cpu] - ru).max() / np.abs(ru).max()))
+            out["speedup_vs_reference"] = out["gpu_triples_per_s"] / out["cpu_reference"]["triples_per_s"]
+    print(json.dumps(out), flush=True)
+    ctx.close()
+
+
 def run_sz_case(args):
     """Three FP64 H*v launches of the ns = 14 half-filled Nambu sector (0.64 GB
     of vectors): the small case for per-kernel ncu captures of the Nambu kernel."""
@@ -489,7 +550,12 @@ def main():
     ap.add_argument("--c4", action="store_true", help="time the many-small-sectors solve, batched vs per chain")
     ap.add_argument("--sz", action="store_true", help="time H*v and fused steps of Nambu (Sz) sectors")
     ap.add_argument("--sz-case", action="store_true", help="three Nambu H*v launches (profiling case)")
+    ap.add_argument("--chiloc", action="store_true", help="time the local vertex against the reference kernel")
     args = ap.parse_args()
+    if args.chiloc:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        run_chiloc(args)
+        return
     if args.sz_case:
         run_sz_case(args)
         return
