@@ -35,6 +35,13 @@ module edk_fortran
     integer(c_int64_t) :: n, offset
   end type
 
+  ! the sectors and c+ matrices of chi_tilde_loc_ (Chiloc_Wenhu_version3.cpp:106-150)
+  type, bind(C) :: edk_chiloc_sectors
+    integer(c_int32_t) :: dim(11)
+    type(c_ptr) :: E(11)
+    type(c_ptr) :: C(14)
+  end type
+
   type, bind(C) :: edk_lanczos_opts
     integer(c_int32_t) :: nitermax, neigen
     real(c_double) :: tolerance, demax, cutoff_min_lanczos_vec
@@ -144,6 +151,24 @@ module edk_fortran
       real(c_double), intent(in) :: wn(*)
       real(c_double), intent(out) :: G(*), diag(*), subdiag(*)
       integer(c_int32_t) :: niter_done
+    end function
+
+    ! ED_diago (ED_ARPACK.f90:590-715): every eigenpair of a small sector
+    integer(c_int) function edk_full_ed(h, E, V) bind(C, name="edk_full_ed")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h
+      real(c_double) :: E(*), V(*)
+    end function
+    ! chi_tilde_loc_ for nf frequency triples (w: nf x 6 doubles)
+    integer(c_int) function edk_chiloc(ctx, op_mask, beta, Z, gs_e, phi_eps, sites, nup, ndn, s, nf, w, &
+        pdndn, pupdn) bind(C, name="edk_chiloc")
+      import :: c_int, c_ptr, c_int32_t, c_double, edk_chiloc_sectors
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: op_mask, sites, nup, ndn, nf
+      real(c_double), value :: beta, Z, gs_e, phi_eps
+      type(edk_chiloc_sectors), intent(in) :: s
+      real(c_double), intent(in) :: w(*)
+      real(c_double) :: pdndn(*), pupdn(*)
     end function
 
     ! GS.raw checkpoints and ed.sector_bound_file (host-only)
