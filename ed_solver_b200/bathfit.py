@@ -232,7 +232,7 @@ def fit_green(ctx, model: AIMModel, G_target: np.ndarray, sector, wn: np.ndarray
         _, G = ImpurityGreen.apply(theta, prob)
         loss = (torch.abs(G.sum(0) - target) ** 2).mean()
         loss.backward()
-        hist.append(float(loss))
+        hist.append(float(loss.detach()))
         return loss
 
     opt.step(closure)

@@ -8,6 +8,7 @@ library sees raw pointers and the current torch stream).
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 import os
 from typing import Optional
 
@@ -325,6 +326,8 @@ class Context:
         if rc:
             raise EdkError(rc, "edk_ctx_create")
         self.h = h
+        # sector Hamiltonians of this context: destroyed before the context is
+        self._live = weakref.WeakSet()
 
     def check(self, rc, what=""):
         if rc not in (EDK_OK,):
@@ -363,6 +366,8 @@ class Context:
 
     def close(self):
         if getattr(self, "h", None):
+            for ham in list(getattr(self, "_live", ())):
+                ham.close()
             lib().edk_ctx_destroy(self.h)
             self.h = None
 
@@ -398,14 +403,16 @@ class Hamiltonian:
         h = C.c_void_p()
         ctx.check(lib().edk_h_create(ctx.h, C.byref(ms), nup, ndn, C.byref(h)), "edk_h_create")
         self.h = h
+        ctx._live.add(self)
         d, du, dd = C.c_int64(), C.c_int64(), C.c_int64()
         lib().edk_h_dims(h, C.byref(d), C.byref(du), C.byref(dd))
         self.dim, self.dup, self.ddn = d.value, du.value, dd.value
 
     def close(self):
-        if getattr(self, "h", None):
+        # a Hamiltonian is destroyed while its context lives (edk_h_destroy uses the context's stream)
+        if getattr(self, "h", None) and getattr(self.ctx, "h", None):
             lib().edk_h_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -611,6 +618,7 @@ class HamiltonianSz(Hamiltonian):
         h = C.c_void_p()
         ctx.check(lib().edk_h_create_sz(ctx.h, C.byref(ms), npart, C.byref(h)), "edk_h_create_sz")
         self.h = h
+        ctx._live.add(self)
         d, du, dd = C.c_int64(), C.c_int64(), C.c_int64()
         lib().edk_h_dims(h, C.byref(d), C.byref(du), C.byref(dd))
         self.dim, self.dup, self.ddn = d.value, du.value, dd.value

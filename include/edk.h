@@ -117,6 +117,8 @@ int edk_build_table(const edk_model *m, int spin, int npart, int64_t *dim, int64
 
 /* ---- sector Hamiltonian: new_H / delete_H / dimen_H (H_class.f90:28-58,149-152) */
 int edk_h_create(edk_ctx *ctx, const edk_model *m, int nup, int ndn, edk_h **out);
+/* Destroy every Hamiltonian a caller created on a context before destroying
+ * the context (the Hamiltonian synchronises on the context's stream). */
 int edk_h_destroy(edk_h *h);
 int edk_h_dims(const edk_h *h, int64_t *dim, int64_t *dim_up, int64_t *dim_dn);
 /* Export one spin species' table (tab_HAIM2, HAIM_offdiag_arrays.f90:210-606)
