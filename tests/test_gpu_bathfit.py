@@ -27,4 +27,3 @@ def test_fit_green_recovers_the_bath(ctx):
     fitted, hist = bathfit.fit_green(ctx, start, G, sector, wn, nitergreen=200, steps=40)
     # G of one sector does not fix the bath uniquely: the fit is judged by G
     assert hist[-1] < 1e-3 * hist[0]
-    assert min(hist) == hist[-1] or hist[-1] < 1e-8
