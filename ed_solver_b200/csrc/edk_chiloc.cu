@@ -313,6 +313,158 @@ __global__ void __launch_bounds__(kChiBlock) chi_terms_kernel(const ChiArgs A)
     }
 }
 
+// The same sums with the Phi kernels split into their one-index parts, which
+// the block computes once into shared memory: per element, phi_ii keeps the
+// inverses of w3 + E_k - E_l, w2 + w3 + E_j - E_l and w2 + E_j - E_k (the
+// last from a (j, k) table when it fits), phi_ji the inverse of w3 + E_k - E_l,
+// and phi_ki, phi_li none.  Same formulas and branches as phi_*.
+struct Hoist {
+    Cx *J[2], *K[2], *L[2], *JK[2];    // per evaluation: one-index parts, (j, k) table
+    unsigned char *fJ[2], *fK[2], *fL[2];
+};
+
+__global__ void __launch_bounds__(kChiBlock) chi_terms_hoisted_kernel(const ChiArgs A, int use_jk)
+{
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    const int i = blockIdx.x, t = blockIdx.y, f = blockIdx.z;
+    const DevTerm T = A.terms[t];
+    const int dj = A.dim[T.sj], dk = A.dim[T.sk], dl = A.dim[T.sl];
+    const double *Ej = A.E + A.eoff[T.sj], *Ek = A.E + A.eoff[T.sk], *El = A.E + A.eoff[T.sl];
+    const double Ei = A.E[A.eoff[S_I] + i];
+    const Cx w[3] = {Cx{A.w[6 * f], A.w[6 * f + 1]}, Cx{A.w[6 * f + 2], A.w[6 * f + 3]},
+                     Cx{A.w[6 * f + 4], A.w[6 * f + 5]}};
+    const double beta = A.beta, eps = A.eps;
+    // shared layout: per evaluation J[dj], K[dk], L[dl], JK[dj*dk] (if use_jk), then the flags
+    Hoist H{};
+    Cx *p = reinterpret_cast<Cx *>(sm_raw);
+    for (int e = 0; e < T.nphi; ++e) {
+        H.J[e] = p; p += dj;
+        H.K[e] = p; p += dk;
+        H.L[e] = p; p += dl;
+        H.JK[e] = p; p += use_jk ? dj * dk : 0;
+    }
+    unsigned char *fp = reinterpret_cast<unsigned char *>(p);
+    for (int e = 0; e < T.nphi; ++e) {
+        H.fJ[e] = fp; fp += dj;
+        H.fK[e] = fp; fp += dk;
+        H.fL[e] = fp; fp += dl;
+    }
+    for (int e = 0; e < T.nphi; ++e) {
+        const Cx W1 = w[T.perm[e][0]], W2 = w[T.perm[e][1]], W3 = w[T.perm[e][2]];
+        const Cx Ws23 = W2 + W3, Ws123 = W1 + W2 + W3, Ws12 = W1 + W2;
+        const int kind = T.kind[e];
+        for (int x = threadIdx.x; x < dj; x += blockDim.x) {
+            if (kind == P_II) H.J[e][x] = inv(W1 + (Ei - Ej[x]));
+            else if (kind == P_JI) H.J[e][x] = inv(W1 + Ej[x] - Ei);
+            else if (kind == P_KI) H.J[e][x] = inv(W2 + Ej[x] - Ei);
+            else {
+                const Cx z = Ws23 + Ej[x] - Ei;
+                H.fJ[e][x] = cabs_(z) > eps;
+                H.J[e][x] = inv(z);
+            }
+        }
+        for (int x = threadIdx.x; x < dk; x += blockDim.x) {
+            if (kind == P_II) {
+                const Cx y = Ws12 + (Ei - Ek[x]);
+                H.K[e][x] = cabs_(y) > eps ? -inv(y) : cx(beta);
+            } else if (kind == P_JI) {
+                H.K[e][x] = inv(W2 + Ei - Ek[x]);
+            } else if (kind == P_KI) {
+                const Cx y = Ws12 + Ek[x] - Ei;
+                H.fK[e][x] = cabs_(y) > eps;
+                H.K[e][x] = inv(y);
+            } else {
+                H.K[e][x] = inv(W3 + Ek[x] - Ei);
+            }
+        }
+        for (int x = threadIdx.x; x < dl; x += blockDim.x) {
+            if (kind == P_II) {
+                H.L[e][x] = inv(Ws123 + Ei - El[x]);
+            } else if (kind == P_JI) {
+                const Cx z = Ws23 + Ei - El[x];
+                H.fL[e][x] = cabs_(z) > eps;
+                H.L[e][x] = inv(z);
+            } else if (kind == P_KI) {
+                H.L[e][x] = -inv(W3 + Ei - El[x]);
+            } else {
+                H.L[e][x] = inv(Ws123 + El[x] - Ei);
+            }
+        }
+        if (use_jk && kind == P_II)
+            for (int x = threadIdx.x; x < dj * dk; x += blockDim.x) {
+                const int jj = x / dk, kk = x % dk;
+                H.JK[e][x] = inv(W2 + Ej[jj] - Ek[kk]);
+            }
+    }
+    __syncthreads();
+    int64_t cf[4][4];                  // address coefficients of i, j, k, l per factor
+    const double *M[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        M[q] = A.C + A.moff[T.mat[q]];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) cf[q][v] = (T.row[q] == v ? T.ld[q] : 0) + (T.col[q] == v ? 1 : 0);
+    }
+    const int64_t n = (int64_t)dj * dk * dl;
+    Cx acc = cx(0.0);
+    for (int64_t e = threadIdx.x; e < n; e += blockDim.x) {
+        const int l = (int)(e % dl);
+        const int k = (int)((e / dl) % dk);
+        const int j = (int)(e / ((int64_t)dl * dk));
+        double fac = 1.0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) fac *= __ldg(M[q] + cf[q][0] * i + cf[q][1] * j + cf[q][2] * k + cf[q][3] * l);
+        if (fac == 0.0) continue;
+        Cx c = cx(0.0);
+        for (int ev = 0; ev < T.nphi; ++ev) {
+            const Cx W2 = w[T.perm[ev][1]], W3 = w[T.perm[ev][2]];
+            Cx r;
+            switch (T.kind[ev]) {
+            case P_II: {
+                const Cx a = inv(W3 + (Ek[k] - El[l]));
+                const Cx z = W2 + W3 + (Ej[j] - El[l]);
+                const Cx b = H.J[ev][j];
+                const Cx tt = cabs_(z) > eps ? inv(z) * (b - H.L[ev][l]) : b * b;
+                const Cx cjk = use_jk ? H.JK[ev][j * dk + k] : inv(W2 + Ej[j] - Ek[k]);
+                r = a * (tt - cjk * (b + H.K[ev][k]));
+                break;
+            }
+            case P_JI: {
+                const Cx a = inv(W3 + (Ek[k] - El[l]));
+                const Cx b = H.J[ev][j];
+                const Cx tt = H.fL[ev][l] ? H.L[ev][l] * b : b * b - b * beta;
+                r = a * (tt - H.K[ev][k] * b);
+                break;
+            }
+            case P_KI:
+                r = H.fK[ev][k] ? H.L[ev][l] * H.K[ev][k] * H.J[ev][j] : cx(0.0);
+                break;
+            default:
+                r = H.fJ[ev][j] ? -(H.K[ev][k] * H.J[ev][j] * H.L[ev][l]) : cx(0.0);
+                break;
+            }
+            c = c + r * (double)T.sgn[ev];
+        }
+        acc = acc + c * (fac * (double)T.total);
+    }
+    __shared__ double red[2][kChiBlock / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        acc.re += __shfl_down_sync(0xffffffffu, acc.re, o);
+        acc.im += __shfl_down_sync(0xffffffffu, acc.im, o);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) { red[0][warp] = acc.re; red[1][warp] = acc.im; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double re = 0.0, im = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) { re += red[0][q]; im += red[1][q]; }
+        double *pp = A.part + (((int64_t)f * A.nterm + t) * A.ni + i) * 2;
+        pp[0] = re;
+        pp[1] = im;
+    }
+}
+
 // out[f] = sum_i boltz_i sum_t part[f][t][i] for the terms of one op, in order.
 __global__ void chi_reduce_kernel(const ChiArgs A, const double *boltz, int op, double *out)
 {
@@ -350,8 +502,18 @@ cudaError_t put(DevMem &m, const T *src, size_t count, cudaStream_t st)
 
 }  // namespace
 
+// 1: always the plain per-element kernel (for A/B checks of the split one)
+static int chiloc_plain_kernel = 0;
+
 extern "C" {
 cudaStream_t edk_internal_stream(edk_ctx *ctx);
+
+int edk_chiloc_set_kernel(int plain)
+{
+    chiloc_plain_kernel = plain ? 1 : 0;
+    return EDK_OK;
+}
+
 int edk_internal_fail(edk_ctx *ctx, int code, const char *msg);
 void edk_internal_add_launches(edk_ctx *ctx, int64_t n);
 void edk_internal_count(edk_ctx *ctx, int64_t h2d, int64_t d2h);
@@ -436,13 +598,31 @@ int edk_chiloc(edk_ctx *ctx, int32_t op_mask, double beta, double Z, double gs_e
     A.w = static_cast<const double *>(dW.p);
     A.part = static_cast<double *>(dP.p);
     if (nterm > 0) {
+        // shared memory of the split kernel: the largest term's one-index parts
+        // (and (j, k) tables when they fit)
+        size_t smem_1d = 0, smem_jk = 0;
+        for (const DevTerm &d : terms) {
+            const size_t dj = A.dim[d.sj], dk = A.dim[d.sk], dl = A.dim[d.sl];
+            const size_t one = (size_t)d.nphi * ((dj + dk + dl) * (sizeof(Cx) + 1));
+            smem_1d = std::max(smem_1d, one + 16);
+            smem_jk = std::max(smem_jk, one + (size_t)d.nphi * dj * dk * sizeof(Cx) + 16);
+        }
+        const size_t cap = 96 * 1024;
+        const int use_jk = smem_jk <= cap ? 1 : 0;
+        const size_t smem = use_jk ? smem_jk : smem_1d;
+        const bool split = smem <= cap;
+        if (split && smem > 48 * 1024)
+            cudaFuncSetAttribute(chi_terms_hoisted_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         // grid.z is limited to 65535: frequency triples in chunks
         for (int f0 = 0; f0 < nf; f0 += 65535) {
             ChiArgs Ac = A;
             const int nfc = std::min(65535, nf - f0);
             Ac.w = A.w + (size_t)f0 * 6;
             Ac.part = A.part + (size_t)f0 * nterm * ni * 2;
-            chi_terms_kernel<<<dim3(ni, nterm, nfc), kChiBlock, 0, st>>>(Ac);
+            if (split && !chiloc_plain_kernel)
+                chi_terms_hoisted_kernel<<<dim3(ni, nterm, nfc), kChiBlock, smem, st>>>(Ac, use_jk);
+            else
+                chi_terms_kernel<<<dim3(ni, nterm, nfc), kChiBlock, 0, st>>>(Ac);
             edk_internal_add_launches(ctx, 1);
         }
     } else {

@@ -216,6 +216,7 @@ def lib():
         "edk_sector_bounds_write": (C.c_int, [C.c_char_p, P]),
         "edk_full_ed": (C.c_int, [P, P, P]),
         "edk_chiloc": (C.c_int, [P, I32, D, D, D, D, I32, I32, I32, P, I32, P, P, P]),
+        "edk_chiloc_set_kernel": (C.c_int, [C.c_int]),
         "edk_h_create_sz": (C.c_int, [P, P, C.c_int, P]),
         "edk_h_sz_info": (C.c_int, [P, P, P]),
         "edk_apply_csz": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, P, P,
@@ -710,6 +711,11 @@ def chiloc(ctx: Context, E, M, w, beta: float, Z: float, gs_e: float, sites: int
                                pu.ctypes.data), "edk_chiloc")
     f = lambda a: a[0:2 * nf:2] + 1j * a[1:2 * nf:2]
     return (f(pd) if mask & 1 else None), (f(pu) if mask & 2 else None)
+
+
+def chiloc_set_kernel(plain: bool):
+    """edk_chiloc's kernel: False = the split kernel (default), True = the per-element one."""
+    lib().edk_chiloc_set_kernel(int(bool(plain)))
 
 
 def gs_write(path: str, entries):

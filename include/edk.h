@@ -512,6 +512,11 @@ typedef struct edk_chiloc_sectors {
 int edk_chiloc(edk_ctx *ctx, int32_t op_mask, double beta, double Z, double gs_e, double phi_eps, int32_t sites,
                int32_t nup, int32_t ndn, const edk_chiloc_sectors *s, int32_t nf, const double *w_host,
                double *pdndn_host, double *pupdn_host);
+/* Process-wide kernel choice of edk_chiloc: 0 (default) = the kernel that
+ * computes the one-index parts of the Phi coefficients once per block (when
+ * they fit in 96 KB of shared memory), 1 = the per-element kernel, for A/B
+ * checks. */
+int edk_chiloc_set_kernel(int plain);
 
 #ifdef __cplusplus
 }

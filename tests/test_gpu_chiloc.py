@@ -51,10 +51,17 @@ def _triples(beta):
     ]
 
 
+@pytest.fixture(params=[False, True], ids=["split-kernel", "per-element-kernel"])
+def kernel(request):
+    edk.chiloc_set_kernel(request.param)
+    yield request.param
+    edk.chiloc_set_kernel(False)
+
+
 @pytest.mark.parametrize("nup,ndn", [(1, 1), (0, 0), (SITES, SITES), (0, SITES), (SITES, 0), (1, 2), (2, 1),
                                      (2, 2), (1, SITES - 1)])
 @pytest.mark.parametrize("degenerate", [False, True])
-def test_random_sector_data_against_reference(ctx, nup, ndn, degenerate):
+def test_random_sector_data_against_reference(ctx, kernel, nup, ndn, degenerate):
     _need_ref()
     rng = np.random.default_rng(100 * nup + 10 * ndn + degenerate)
     E, M = _random_inputs(rng, nup, ndn, degenerate)
@@ -80,7 +87,7 @@ def test_full_ed_matches_dense_diagonalisation(ctx):
         assert np.abs(V.T @ V - np.eye(h.dim)).max() < 1e-12
 
 
-def test_physical_vertex_against_reference(ctx):
+def test_physical_vertex_against_reference(ctx, kernel):
     """ns=4 star model, sector (2,2): device full ED + device c+ matrices +
     device chi~ against the oracle's dense ED + c+ matrices + the reference's
     chi_tilde_loc_ (eigenvector signs and degenerate rotations differ between
