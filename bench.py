@@ -517,6 +517,27 @@ def run_chiloc(args):
     ctx.close()
 
 
+def run_chiloc_case(args):
+    """One edk_chiloc call on the first 256 triples of the --chiloc batch (the
+    small case for per-kernel ncu captures)."""
+    import numpy as np
+    import torch
+    from ed_solver_b200 import edk, vertex
+    from ed_solver_b200.model import star_model
+    rng = np.random.default_rng(5)
+    m = star_model(-1.0, 2.0, rng.uniform(-1.0, 1.0, 3), rng.uniform(0.3, 0.6, 3))
+    ctx = edk.Context(0)
+    E, M = vertex.vertex_inputs(ctx, m, 2, 2)
+    Z, gs = vertex.partition(E, 10.0)
+    nu = lambda n: 1j * (2 * n + 1) * np.pi / 10.0
+    w = [(nu(a), nu(b), -nu(b) if (a + b + c) % 3 == 0 else nu(c))
+         for a in range(-8, 8) for b in range(-8, 8) for c in range(-8, 8)][:256]
+    edk.chiloc(ctx, E, M, w, 10.0, Z, gs, m.ns, 2, 2)
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel_case": "chiloc ns4 (2,2) 256 triples"}), flush=True)
+    ctx.close()
+
+
 def run_sz_case(args):
     """Three FP64 H*v launches of the ns = 14 half-filled Nambu sector (0.64 GB
     of vectors): the small case for per-kernel ncu captures of the Nambu kernel."""
@@ -551,7 +572,11 @@ def main():
     ap.add_argument("--sz", action="store_true", help="time H*v and fused steps of Nambu (Sz) sectors")
     ap.add_argument("--sz-case", action="store_true", help="three Nambu H*v launches (profiling case)")
     ap.add_argument("--chiloc", action="store_true", help="time the local vertex against the reference kernel")
+    ap.add_argument("--chiloc-case", action="store_true", help="one local-vertex call (profiling case)")
     args = ap.parse_args()
+    if args.chiloc_case:
+        run_chiloc_case(args)
+        return
     if args.chiloc:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         run_chiloc(args)
