@@ -194,6 +194,15 @@ __device__ __forceinline__ Cx inv(Cx b)
     return Cx{r / d, -1.0 / d};
 }
 __device__ __forceinline__ double cabs_(Cx a) { return hypot(a.re, a.im); }
+// 1 / b through one reciprocal of |b|^2 (the split kernel's denominators are
+// O(1) to O(1e3): no scaling needed)
+__device__ __forceinline__ Cx inv_fast(Cx b)
+{
+    const double d = __drcp_rn(b.re * b.re + b.im * b.im);
+    return Cx{b.re * d, -b.im * d};
+}
+// |z| > eps without the square root
+__device__ __forceinline__ bool above(Cx z, double eps2) { return z.re * z.re + z.im * z.im > eps2; }
 
 // Fourier transform of <T c c c c> without the Boltzmann factor for the four
 // orderings (the PhiM functions of Chiloc_Wenhu_version3.cpp:29-105); the
@@ -314,7 +323,8 @@ __global__ void __launch_bounds__(kChiBlock) chi_terms_kernel(const ChiArgs A)
 }
 
 // The same sums with the Phi kernels split into their one-index parts, which
-// the block computes once into shared memory: per element, phi_ii keeps the
+// the block computes once into shared memory (complex inverses through one
+// reciprocal, the |z| > PHI_EPS tests on |z|^2): per element, phi_ii keeps the
 // inverses of w3 + E_k - E_l, w2 + w3 + E_j - E_l and w2 + E_j - E_k (the
 // last from a (j, k) table when it fits), phi_ji the inverse of w3 + E_k - E_l,
 // and phi_ki, phi_li none.  Same formulas and branches as phi_*.
@@ -323,7 +333,7 @@ struct Hoist {
     unsigned char *fJ[2], *fK[2], *fL[2];
 };
 
-__global__ void __launch_bounds__(kChiBlock) chi_terms_hoisted_kernel(const ChiArgs A, int use_jk)
+__global__ void __launch_bounds__(kChiBlock, 3) chi_terms_hoisted_kernel(const ChiArgs A, int use_jk)
 {
     extern __shared__ __align__(16) unsigned char sm_raw[];
     const int i = blockIdx.x, t = blockIdx.y, f = blockIdx.z;
@@ -333,7 +343,7 @@ __global__ void __launch_bounds__(kChiBlock) chi_terms_hoisted_kernel(const ChiA
     const double Ei = A.E[A.eoff[S_I] + i];
     const Cx w[3] = {Cx{A.w[6 * f], A.w[6 * f + 1]}, Cx{A.w[6 * f + 2], A.w[6 * f + 3]},
                      Cx{A.w[6 * f + 4], A.w[6 * f + 5]}};
-    const double beta = A.beta, eps = A.eps;
+    const double beta = A.beta, eps2 = A.eps * A.eps;
     // shared layout: per evaluation J[dj], K[dk], L[dl], JK[dj*dk] (if use_jk), then the flags
     Hoist H{};
     Cx *p = reinterpret_cast<Cx *>(sm_raw);
@@ -354,56 +364,57 @@ __global__ void __launch_bounds__(kChiBlock) chi_terms_hoisted_kernel(const ChiA
         const Cx Ws23 = W2 + W3, Ws123 = W1 + W2 + W3, Ws12 = W1 + W2;
         const int kind = T.kind[e];
         for (int x = threadIdx.x; x < dj; x += blockDim.x) {
-            if (kind == P_II) H.J[e][x] = inv(W1 + (Ei - Ej[x]));
-            else if (kind == P_JI) H.J[e][x] = inv(W1 + Ej[x] - Ei);
-            else if (kind == P_KI) H.J[e][x] = inv(W2 + Ej[x] - Ei);
+            if (kind == P_II) H.J[e][x] = inv_fast(W1 + (Ei - Ej[x]));
+            else if (kind == P_JI) H.J[e][x] = inv_fast(W1 + Ej[x] - Ei);
+            else if (kind == P_KI) H.J[e][x] = inv_fast(W2 + Ej[x] - Ei);
             else {
                 const Cx z = Ws23 + Ej[x] - Ei;
-                H.fJ[e][x] = cabs_(z) > eps;
-                H.J[e][x] = inv(z);
+                H.fJ[e][x] = above(z, eps2);
+                H.J[e][x] = inv_fast(z);
             }
         }
         for (int x = threadIdx.x; x < dk; x += blockDim.x) {
             if (kind == P_II) {
                 const Cx y = Ws12 + (Ei - Ek[x]);
-                H.K[e][x] = cabs_(y) > eps ? -inv(y) : cx(beta);
+                H.K[e][x] = above(y, eps2) ? -inv_fast(y) : cx(beta);
             } else if (kind == P_JI) {
-                H.K[e][x] = inv(W2 + Ei - Ek[x]);
+                H.K[e][x] = inv_fast(W2 + Ei - Ek[x]);
             } else if (kind == P_KI) {
                 const Cx y = Ws12 + Ek[x] - Ei;
-                H.fK[e][x] = cabs_(y) > eps;
-                H.K[e][x] = inv(y);
+                H.fK[e][x] = above(y, eps2);
+                H.K[e][x] = inv_fast(y);
             } else {
-                H.K[e][x] = inv(W3 + Ek[x] - Ei);
+                H.K[e][x] = inv_fast(W3 + Ek[x] - Ei);
             }
         }
         for (int x = threadIdx.x; x < dl; x += blockDim.x) {
             if (kind == P_II) {
-                H.L[e][x] = inv(Ws123 + Ei - El[x]);
+                H.L[e][x] = inv_fast(Ws123 + Ei - El[x]);
             } else if (kind == P_JI) {
                 const Cx z = Ws23 + Ei - El[x];
-                H.fL[e][x] = cabs_(z) > eps;
-                H.L[e][x] = inv(z);
+                H.fL[e][x] = above(z, eps2);
+                H.L[e][x] = inv_fast(z);
             } else if (kind == P_KI) {
-                H.L[e][x] = -inv(W3 + Ei - El[x]);
+                H.L[e][x] = -inv_fast(W3 + Ei - El[x]);
             } else {
-                H.L[e][x] = inv(Ws123 + El[x] - Ei);
+                H.L[e][x] = inv_fast(Ws123 + El[x] - Ei);
             }
         }
         if (use_jk && kind == P_II)
             for (int x = threadIdx.x; x < dj * dk; x += blockDim.x) {
                 const int jj = x / dk, kk = x % dk;
-                H.JK[e][x] = inv(W2 + Ej[jj] - Ek[kk]);
+                H.JK[e][x] = inv_fast(W2 + Ej[jj] - Ek[kk]);
             }
     }
     __syncthreads();
-    int64_t cf[4][4];                  // address coefficients of i, j, k, l per factor
+    int cf[4][3];                      // address coefficients of j, k, l per factor (i folded in M)
     const double *M[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        M[q] = A.C + A.moff[T.mat[q]];
+        const int ci = (T.row[q] == VI ? T.ld[q] : 0) + (T.col[q] == VI ? 1 : 0);
+        M[q] = A.C + A.moff[T.mat[q]] + (int64_t)ci * i;
 #pragma unroll
-        for (int v = 0; v < 4; ++v) cf[q][v] = (T.row[q] == v ? T.ld[q] : 0) + (T.col[q] == v ? 1 : 0);
+        for (int v = 1; v < 4; ++v) cf[q][v - 1] = (T.row[q] == v ? T.ld[q] : 0) + (T.col[q] == v ? 1 : 0);
     }
     const int64_t n = (int64_t)dj * dk * dl;
     Cx acc = cx(0.0);
@@ -413,7 +424,7 @@ __global__ void __launch_bounds__(kChiBlock) chi_terms_hoisted_kernel(const ChiA
         const int j = (int)(e / ((int64_t)dl * dk));
         double fac = 1.0;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) fac *= __ldg(M[q] + cf[q][0] * i + cf[q][1] * j + cf[q][2] * k + cf[q][3] * l);
+        for (int q = 0; q < 4; ++q) fac *= __ldg(M[q] + (cf[q][0] * j + cf[q][1] * k + cf[q][2] * l));
         if (fac == 0.0) continue;
         Cx c = cx(0.0);
         for (int ev = 0; ev < T.nphi; ++ev) {
@@ -421,16 +432,16 @@ __global__ void __launch_bounds__(kChiBlock) chi_terms_hoisted_kernel(const ChiA
             Cx r;
             switch (T.kind[ev]) {
             case P_II: {
-                const Cx a = inv(W3 + (Ek[k] - El[l]));
+                const Cx a = inv_fast(W3 + (Ek[k] - El[l]));
                 const Cx z = W2 + W3 + (Ej[j] - El[l]);
                 const Cx b = H.J[ev][j];
-                const Cx tt = cabs_(z) > eps ? inv(z) * (b - H.L[ev][l]) : b * b;
-                const Cx cjk = use_jk ? H.JK[ev][j * dk + k] : inv(W2 + Ej[j] - Ek[k]);
+                const Cx tt = above(z, eps2) ? inv_fast(z) * (b - H.L[ev][l]) : b * b;
+                const Cx cjk = use_jk ? H.JK[ev][j * dk + k] : inv_fast(W2 + Ej[j] - Ek[k]);
                 r = a * (tt - cjk * (b + H.K[ev][k]));
                 break;
             }
             case P_JI: {
-                const Cx a = inv(W3 + (Ek[k] - El[l]));
+                const Cx a = inv_fast(W3 + (Ek[k] - El[l]));
                 const Cx b = H.J[ev][j];
                 const Cx tt = H.fL[ev][l] ? H.L[ev][l] * b : b * b - b * beta;
                 r = a * (tt - H.K[ev][k] * b);
