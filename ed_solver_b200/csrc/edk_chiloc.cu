@@ -329,14 +329,11 @@ __global__ void __launch_bounds__(kChiBlock) chi_terms_kernel(const ChiArgs A)
 // last from a (j, k) table when it fits), phi_ji the inverse of w3 + E_k - E_l,
 // and phi_ki, phi_li none.  Same formulas and branches as phi_*.
 struct Hoist {
-    Cx *J[2], *K[2], *L[2];            // per evaluation: one-index parts
-    Cx *JK[2], *KL[2], *JL[2];         // two-index tables (when they fit)
-    unsigned char *fJ[2], *fK[2], *fL[2], *fJL[2];
+    Cx *J[2], *K[2], *L[2], *JK[2];    // per evaluation: one-index parts, (j, k) table
+    unsigned char *fJ[2], *fK[2], *fL[2];
 };
 
-// tables: bit 0 = the (j, k) table of phi_ii; bit 1 = the (k, l) and (j, l)
-// tables of phi_ii and phi_ji
-__global__ void __launch_bounds__(kChiBlock, 3) chi_terms_hoisted_kernel(const ChiArgs A, int tables)
+__global__ void __launch_bounds__(kChiBlock, 3) chi_terms_hoisted_kernel(const ChiArgs A, int use_jk)
 {
     extern __shared__ __align__(16) unsigned char sm_raw[];
     const int i = blockIdx.x, t = blockIdx.y, f = blockIdx.z;
@@ -347,7 +344,7 @@ __global__ void __launch_bounds__(kChiBlock, 3) chi_terms_hoisted_kernel(const C
     const Cx w[3] = {Cx{A.w[6 * f], A.w[6 * f + 1]}, Cx{A.w[6 * f + 2], A.w[6 * f + 3]},
                      Cx{A.w[6 * f + 4], A.w[6 * f + 5]}};
     const double beta = A.beta, eps2 = A.eps * A.eps;
-    const bool use_jk = tables & 1, use_2d = tables & 2;
+    // shared layout: per evaluation J[dj], K[dk], L[dl], JK[dj*dk] (if use_jk), then the flags
     Hoist H{};
     Cx *p = reinterpret_cast<Cx *>(sm_raw);
     for (int e = 0; e < T.nphi; ++e) {
@@ -355,15 +352,12 @@ __global__ void __launch_bounds__(kChiBlock, 3) chi_terms_hoisted_kernel(const C
         H.K[e] = p; p += dk;
         H.L[e] = p; p += dl;
         H.JK[e] = p; p += use_jk ? dj * dk : 0;
-        H.KL[e] = p; p += use_2d ? dk * dl : 0;
-        H.JL[e] = p; p += use_2d ? dj * dl : 0;
     }
     unsigned char *fp = reinterpret_cast<unsigned char *>(p);
     for (int e = 0; e < T.nphi; ++e) {
         H.fJ[e] = fp; fp += dj;
         H.fK[e] = fp; fp += dk;
         H.fL[e] = fp; fp += dl;
-        H.fJL[e] = fp; fp += use_2d ? dj * dl : 0;
     }
     for (int e = 0; e < T.nphi; ++e) {
         const Cx W1 = w[T.perm[e][0]], W2 = w[T.perm[e][1]], W3 = w[T.perm[e][2]];
@@ -407,16 +401,9 @@ __global__ void __launch_bounds__(kChiBlock, 3) chi_terms_hoisted_kernel(const C
             }
         }
         if (use_jk && kind == P_II)
-            for (int x = threadIdx.x; x < dj * dk; x += blockDim.x)
-                H.JK[e][x] = inv_fast(W2 + Ej[x / dk] - Ek[x % dk]);
-        if (use_2d && (kind == P_II || kind == P_JI))
-            for (int x = threadIdx.x; x < dk * dl; x += blockDim.x)
-                H.KL[e][x] = inv_fast(W3 + (Ek[x / dl] - El[x % dl]));
-        if (use_2d && kind == P_II)
-            for (int x = threadIdx.x; x < dj * dl; x += blockDim.x) {
-                const Cx z = Ws23 + (Ej[x / dl] - El[x % dl]);
-                H.fJL[e][x] = above(z, eps2);
-                H.JL[e][x] = inv_fast(z);
+            for (int x = threadIdx.x; x < dj * dk; x += blockDim.x) {
+                const int jj = x / dk, kk = x % dk;
+                H.JK[e][x] = inv_fast(W2 + Ej[jj] - Ek[kk]);
             }
     }
     __syncthreads();
@@ -445,21 +432,16 @@ __global__ void __launch_bounds__(kChiBlock, 3) chi_terms_hoisted_kernel(const C
             Cx r;
             switch (T.kind[ev]) {
             case P_II: {
-                const Cx a = use_2d ? H.KL[ev][k * dl + l] : inv_fast(W3 + (Ek[k] - El[l]));
+                const Cx a = inv_fast(W3 + (Ek[k] - El[l]));
+                const Cx z = W2 + W3 + (Ej[j] - El[l]);
                 const Cx b = H.J[ev][j];
-                Cx tt;
-                if (use_2d) {
-                    tt = H.fJL[ev][j * dl + l] ? H.JL[ev][j * dl + l] * (b - H.L[ev][l]) : b * b;
-                } else {
-                    const Cx z = W2 + W3 + (Ej[j] - El[l]);
-                    tt = above(z, eps2) ? inv_fast(z) * (b - H.L[ev][l]) : b * b;
-                }
+                const Cx tt = above(z, eps2) ? inv_fast(z) * (b - H.L[ev][l]) : b * b;
                 const Cx cjk = use_jk ? H.JK[ev][j * dk + k] : inv_fast(W2 + Ej[j] - Ek[k]);
                 r = a * (tt - cjk * (b + H.K[ev][k]));
                 break;
             }
             case P_JI: {
-                const Cx a = use_2d ? H.KL[ev][k * dl + l] : inv_fast(W3 + (Ek[k] - El[l]));
+                const Cx a = inv_fast(W3 + (Ek[k] - El[l]));
                 const Cx b = H.J[ev][j];
                 const Cx tt = H.fL[ev][l] ? H.L[ev][l] * b : b * b - b * beta;
                 r = a * (tt - H.K[ev][k] * b);
@@ -629,19 +611,16 @@ int edk_chiloc(edk_ctx *ctx, int32_t op_mask, double beta, double Z, double gs_e
     if (nterm > 0) {
         // shared memory of the split kernel: the largest term's one-index parts
         // (and (j, k) tables when they fit)
-        size_t smem_1d = 0, smem_jk = 0, smem_2d = 0;
+        size_t smem_1d = 0, smem_jk = 0;
         for (const DevTerm &d : terms) {
             const size_t dj = A.dim[d.sj], dk = A.dim[d.sk], dl = A.dim[d.sl];
             const size_t one = (size_t)d.nphi * ((dj + dk + dl) * (sizeof(Cx) + 1));
-            const size_t jk = (size_t)d.nphi * dj * dk * sizeof(Cx);
-            const size_t two = (size_t)d.nphi * ((dk * dl + dj * dl) * sizeof(Cx) + dj * dl);
             smem_1d = std::max(smem_1d, one + 16);
-            smem_jk = std::max(smem_jk, one + jk + 16);
-            smem_2d = std::max(smem_2d, one + jk + two + 16);
+            smem_jk = std::max(smem_jk, one + (size_t)d.nphi * dj * dk * sizeof(Cx) + 16);
         }
         const size_t cap = 96 * 1024;
-        const int tables = smem_2d <= cap ? 3 : smem_jk <= cap ? 1 : 0;
-        const size_t smem = tables == 3 ? smem_2d : tables == 1 ? smem_jk : smem_1d;
+        const int use_jk = smem_jk <= cap ? 1 : 0;
+        const size_t smem = use_jk ? smem_jk : smem_1d;
         const bool split = smem <= cap;
         if (split && smem > 48 * 1024)
             cudaFuncSetAttribute(chi_terms_hoisted_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -652,7 +631,7 @@ int edk_chiloc(edk_ctx *ctx, int32_t op_mask, double beta, double Z, double gs_e
             Ac.w = A.w + (size_t)f0 * 6;
             Ac.part = A.part + (size_t)f0 * nterm * ni * 2;
             if (split && !chiloc_plain_kernel)
-                chi_terms_hoisted_kernel<<<dim3(ni, nterm, nfc), kChiBlock, smem, st>>>(Ac, tables);
+                chi_terms_hoisted_kernel<<<dim3(ni, nterm, nfc), kChiBlock, smem, st>>>(Ac, use_jk);
             else
                 chi_terms_kernel<<<dim3(ni, nterm, nfc), kChiBlock, 0, st>>>(Ac);
             edk_internal_add_launches(ctx, 1);
