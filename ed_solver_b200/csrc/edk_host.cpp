@@ -1033,6 +1033,41 @@ int edk_apply_csz(edk_h *src, int dtype, int site, int spin, int dagger, int pro
     return rc;
 }
 
+int edk_apply_cnambu(edk_h *src, int dtype, int orb, int dagger, int orb2, int sign2, const void *in_dev,
+                     void *out_dev, int64_t *out_dim, int32_t *out_npart)
+{
+    if (!src || !in_dev || !out_dev || (dtype != EDK_F64 && dtype != EDK_F32)) return EDK_ERR_INVALID;
+    edk_ctx *c = src->ctx;
+    if (!src->sz) return c->fail(EDK_ERR_INVALID, "edk_apply_cnambu needs a Nambu sector (edk_h_create_sz)");
+    const SzDev &S = sz_dev(src->sz);
+    const int ns = S.ns, nc = S.nc;
+    if (orb < 0 || orb >= 2 * nc || orb2 >= 2 * nc || orb2 == orb)
+        return c->fail(EDK_ERR_INVALID, "Nambu orbital outside [0, 2nc) (or orb2 == orb)");
+    const int npt = src->npart + (dagger ? 1 : -1);
+    if (npt < 0 || npt > 2 * ns) return c->fail(EDK_ERR_INVALID, "target Nambu sector outside [0, 2 ns]");
+    std::string err;
+    const SzSectorDev *tgt = nullptr;
+    int rc = sz_sector(src->sz, npt, c->stream, &tgt, &err);
+    if (rc) return c->fail(rc, "%s", err.c_str());
+    // IMPiorb of the Nambu AIM2 (quantum_algebra_Anderson_Impurity_class2.f90:88-93)
+    auto bit = [&](int o) { return 1u << (o < nc ? S.nb + o : ns + S.nb + (o - nc)); };
+    SzOp ops[2];
+    ops[0].bit = bit(orb);
+    ops[0].create = dagger ? 1 : 0;
+    int nop = 1;
+    if (orb2 >= 0) {
+        ops[1].bit = bit(orb2);
+        ops[1].create = dagger ? 1 : 0;
+        ops[1].sgn = sign2 < 0 ? -1 : 1;
+        nop = 2;
+    }
+    if (out_dim) *out_dim = tgt->dim;
+    if (out_npart) *out_npart = npt;
+    rc = c->cuda(launch_sz_apply_c(dtype, S, *tgt, nop, ops, in_dev, out_dev, c->num_sms, c->stream), "apply_cnambu");
+    c->launches++;
+    return rc;
+}
+
 int edk_h_destroy(edk_h *h)
 {
     if (!h) return EDK_OK;

@@ -218,6 +218,7 @@ def lib():
         "edk_chiloc": (C.c_int, [P, I32, D, D, D, D, I32, I32, I32, P, I32, P, P, P]),
         "edk_chiloc_set_kernel": (C.c_int, [C.c_int]),
         "edk_h_create_sz": (C.c_int, [P, P, C.c_int, P]),
+        "edk_apply_cnambu": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, P, P, P]),
         "edk_h_sz_info": (C.c_int, [P, P, P]),
         "edk_apply_csz": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, P, P,
                                     P]),
@@ -639,6 +640,19 @@ class HamiltonianSz(Hamiltonian):
         self.ctx.check(lib().edk_apply_csz(self.h, _dtype_code(vec.dtype), site, spin, int(bool(dagger)),
                                            int(bool(projected)), site2, sign2, _ptr(vec), _ptr(out),
                                            C.byref(od), C.byref(on)), "edk_apply_csz")
+        return out, on.value
+
+    def apply_b(self, vec, orb, dagger, orb2=-1, sign2=1):
+        """apply_Csz on Nambu impurity orbitals (orb < nc: up, orb >= nc: hole), optionally
+        + sign2 * the same on orb2 -> (tensor in the target sector, npart')."""
+        import torch
+        npt = self.npart + (1 if dagger else -1)
+        if not 0 <= npt <= 2 * self.model.ns:
+            raise ValueError("target sector outside the Hilbert space")
+        out = torch.empty(binom(2 * self.model.ns, npt), dtype=vec.dtype, device=vec.device)
+        od, on = C.c_int64(), C.c_int32()
+        self.ctx.check(lib().edk_apply_cnambu(self.h, _dtype_code(vec.dtype), orb, int(bool(dagger)), orb2, sign2,
+                                              _ptr(vec), _ptr(out), C.byref(od), C.byref(on)), "edk_apply_cnambu")
         return out, on.value
 
 

@@ -138,3 +138,91 @@ def green_impurity(hc: HCache, gs, beta: float, nw: int, nitergreen: int, spin: 
             a, b = min(i, j), max(i, j)
             out[(i, j)] = 0.5 * (raw[(a, b)] - raw[(a, a)] - raw[(b, b)])
     return out
+
+
+# ---------------------------------------------------------------------------
+# Nambu (Sz) sectors: the superconducting branch of get_eigen_energies and
+# compute_greenAA (AIM%bath%SUPER, force_sz_basis)
+# ---------------------------------------------------------------------------
+
+class HCacheSz:
+    """One device Nambu Hamiltonian per sector (npart) kept alive across calls."""
+
+    def __init__(self, ctx: edk.Context, model):
+        self.ctx, self.model = ctx, model
+        self._h: Dict[int, edk.HamiltonianSz] = {}
+
+    def get(self, npart: int) -> edk.HamiltonianSz:
+        if npart not in self._h:
+            self._h[npart] = edk.HamiltonianSz(self.ctx, self.model, npart)
+        return self._h[npart]
+
+    def close(self):
+        for h in self._h.values():
+            h.close()
+        self._h.clear()
+
+
+def ground_states_sz(hc: HCacheSz, nparts, beta: float, demax0: float, neigen=1, nitermax=1000,
+                     tolerance=1e-12, dtype="f64"):
+    """Sector scan over Nambu sectors and the global window.  Energies stay
+    those of the Nambu operator (solve_AIM shifts them back before get_GS and
+    the Green functions, solver.f90:87-94); the physical E0 is e0 + shift (the
+    same shift for every sector, so window and weights do not change)."""
+    import torch
+    demax = demax0 / beta
+    found = []
+    for npart in nparts:
+        h = hc.get(npart)
+        if h.dim == 0:
+            continue
+        if h.dim <= FULL_ED_SWITCH:
+            w, v = np.linalg.eigh(_dense(h))
+            j = min(h.dim, neigen)
+            keep = [0] + [i for i in range(1, j) if w[i] <= w[0] + demax]
+            dev = f"cuda:{h.ctx.device}"
+            states = [dict(E=float(w[i]), psi=torch.tensor(v[:, i], device=dev)) for i in keep]
+        else:
+            r = h.lanczos_e0(dtype=dtype, nitermax=nitermax, neigen=neigen, tolerance=tolerance, demax=demax)
+            states = [dict(E=float(r["E"][k]), psi=h.lanczos_gs(r["vecp"][k], dtype=dtype)) for k in range(len(r["E"]))]
+        es = min(s["E"] for s in states)
+        found += [dict(npart=npart, **s) for s in states if s["E"] <= es + demax]
+    e0 = min(f["E"] for f in found)
+    gs = [f for f in found if f["E"] <= e0 + demax]
+    z = sum(math.exp(-beta * (f["E"] - e0)) for f in gs)
+    for f in gs:
+        f["boltz"] = math.exp(-beta * (f["E"] - e0)) / z
+    shift = hc.get(gs[0]["npart"]).energy_shift
+    return gs, e0, z, shift
+
+
+def green_nambu(hc: HCacheSz, gs, beta: float, nw: int, nitergreen: int, orbs=None, cutoff_dynamic=1e-8):
+    """G_ab(i w_n) over Nambu impurity orbitals (compute_greenAA on the Nambu
+    AIM2): a, b in [0, 2nc), a < nc the up orbital, a >= nc the hole orbital
+    (so G_{0,nc} is the anomalous function of site 0).  Particle chains from
+    b+_a|psi>, hole chains from b_a|psi>; off-diagonal elements from the
+    symmetric combination b_a + b_b (green_class_compute_symmetric_combination.f90:39-138):
+    G_ab = (G_{a+b} - G_aa - G_bb) / 2.  Returns {(a, b): G}."""
+    nc = hc.model.nc
+    if orbs is None:
+        orbs = list(range(2 * nc))
+    wn = matsubara(beta, nw)
+    pairs = [(a, a) for a in orbs] + [(a, b) for i, a in enumerate(orbs) for b in orbs[i + 1:]]
+    raw = {p: np.zeros(nw, complex) for p in pairs}
+    ns2 = 2 * hc.model.ns
+    for st in gs:
+        h_src = hc.get(st["npart"])
+        for iph in (1, 2):
+            dagger = iph == 1
+            npt = st["npart"] + (1 if dagger else -1)
+            if not 0 <= npt <= ns2:
+                continue
+            h_t = hc.get(npt)
+            for (a, b) in pairs:
+                v, _ = h_src.apply_b(st["psi"], a, dagger, orb2=(b if b != a else -1), sign2=1)
+                G, _, _, _ = h_t.green_chain(v, nitergreen, st["E"], iph, wn, cutoff_dynamic)
+                raw[(a, b)] += st["boltz"] * G
+    out = {}
+    for (a, b) in pairs:
+        out[(a, b)] = raw[(a, b)] if a == b else 0.5 * (raw[(a, b)] - raw[(a, a)] - raw[(b, b)])
+    return out

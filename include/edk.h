@@ -475,6 +475,14 @@ int edk_h_sz_info(const edk_h *h, int32_t *npart, double *energy_shift);
  * the returned *out_npart. */
 int edk_apply_csz(edk_h *src, int dtype, int site, int spin, int dagger, int projected, int site2, int sign2,
                   const void *in_dev, void *out_dev, int64_t *out_dim, int32_t *out_npart);
+/* apply_Csz (apply_C.f90:273-333) on Nambu impurity orbitals: b+_orb
+ * (dagger = 1) or b_orb, orb in [0, 2nc) (orb < nc: the up orbital of site
+ * orb; orb >= nc: the hole orbital of site orb - nc), plus sign2 times the
+ * same operator on orb2 when orb2 >= 0 (the symmetric combinations of
+ * green_class_compute_symmetric_combination.f90:39-138 in the Nambu basis,
+ * e.g. b+_up + b+_hole for the anomalous part).  Target sector npart +/- 1. */
+int edk_apply_cnambu(edk_h *src, int dtype, int orb, int dagger, int orb2, int sign2, const void *in_dev,
+                     void *out_dev, int64_t *out_dim, int32_t *out_npart);
 
 /* ED_diago (ED_ARPACK.f90:590-715): every eigenpair of a sector by dense
  * diagonalisation of the FP64 matrix that H*v gives on the unit vectors
