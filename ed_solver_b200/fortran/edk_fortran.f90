@@ -171,6 +171,17 @@ module edk_fortran
       real(c_double) :: pdndn(*), pupdn(*)
     end function
 
+    ! apply_Csz on Nambu impurity orbitals (0-based orb < 2nc), + sign2 * the same on orb2 >= 0
+    integer(c_int) function edk_apply_cnambu(src, dtype, orb, dagger, orb2, sign2, vin, vout, out_dim, out_npart) &
+        bind(C, name="edk_apply_cnambu")
+      import :: c_int, c_ptr, c_int32_t, c_int64_t
+      type(c_ptr), value :: src
+      integer(c_int), value :: dtype, orb, dagger, orb2, sign2
+      type(c_ptr), value :: vin, vout
+      integer(c_int64_t) :: out_dim
+      integer(c_int32_t) :: out_npart
+    end function
+
     ! GS.raw checkpoints and ed.sector_bound_file (host-only)
     integer(c_int) function edk_gs_write(path, nentries, entries, pool) bind(C, name="edk_gs_write")
       import :: c_int, c_char, c_int32_t, c_double, edk_gs_entry
