@@ -202,6 +202,50 @@ int ctx_init(edk_ctx *c)
 // ---------------------------------------------------------------------------
 // sector Hamiltonian
 // ---------------------------------------------------------------------------
+// Krylov vectors kept between pass 1 and pass 2 (edk_lanczos_opts.keep_basis):
+// v_1, v_2, ... in chunks of kBasisChunk vectors, allocated stream-ordered as
+// pass 1 reaches them.
+constexpr int kBasisChunk = 8;
+struct Basis {
+    int dtype = -1;
+    int64_t dim = 0;
+    int cap = 0;                 // vectors allowed by the memory budget
+    int nvec = 0;                // valid vectors after pass 1
+    bool valid = false;
+    const void *start = nullptr; // identity of the pass-1 start (start_dev, host ran_tab)
+    const double *tab = nullptr;
+    cudaStream_t st = nullptr;
+    std::vector<void *> chunks;
+    size_t vec_bytes() const { return (size_t)dim * (dtype == EDK_F64 ? 8 : 4); }
+    // slots start on 256-byte boundaries, like separate allocations
+    size_t stride() const { return (vec_bytes() + 255) & ~(size_t)255; }
+    void *slot(int q) const
+    {
+        return static_cast<char *>(chunks[(size_t)q / kBasisChunk]) + (size_t)(q % kBasisChunk) * stride();
+    }
+    // makes slot q usable; false when the budget or an allocation says no
+    bool ensure(int q)
+    {
+        if (q >= cap) return false;
+        while ((int)chunks.size() * kBasisChunk <= q) {
+            void *p = nullptr;
+            if (cudaMallocAsync(&p, stride() * kBasisChunk, st) != cudaSuccess) {
+                (void)cudaGetLastError();
+                return false;
+            }
+            chunks.push_back(p);
+        }
+        return true;
+    }
+    void release(cudaStream_t s)
+    {
+        for (void *p : chunks) cudaFreeAsync(p, s);
+        chunks.clear();
+        valid = false;
+        nvec = cap = 0;
+    }
+};
+
 struct edk_h {
     edk_ctx *ctx = nullptr;
     ModelHost model;
@@ -231,10 +275,18 @@ struct edk_h {
     // Nambu (Sz) sector: its tables replace the (N_up, N_dn) ones
     SzHost *sz = nullptr;
     int npart = -1;
+    Basis basis;
     edk_h() = default;
     edk_h(const edk_h &) = delete;
     edk_h &operator=(const edk_h &) = delete;
-    ~edk_h() { if (sz) sz_destroy(sz); }
+    ~edk_h()
+    {
+        if (!basis.chunks.empty()) {
+            basis.release(ctx->stream);
+            cudaStreamSynchronize(ctx->stream);
+        }
+        if (sz) sz_destroy(sz);
+    }
 };
 
 namespace {
@@ -430,6 +482,8 @@ struct Krylov {
     cudaGraphExec_t gexec = nullptr;
     int gk0 = -1;
     bool graph_off = false;
+    // stored-basis mode: v_{q+1} lives in basis slot q (no buffer rotation, no graphs)
+    Basis *basis = nullptr;
     ~Krylov() { if (gexec) cudaGraphExecDestroy(gexec); }
 };
 
@@ -442,7 +496,9 @@ int krylov_start(Krylov &K, const void *start_dev, const double *ran_tab_dev, do
     rc = c->cuda(cudaMemsetAsync(c->flags.p, 0, sizeof(int) * 16, c->stream), "memset flags");
     if (rc) return rc;
     const int grid = c->reduce_grid;
-    rc = c->cuda(launch_start_vector(K.dtype, h->dim, ran_tab_dev, start_dev, K.w[K.ivk],
+    if (K.basis && !K.basis->ensure(0)) K.basis = nullptr;
+    void *v1 = K.basis ? K.basis->slot(0) : K.w[K.ivk];
+    rc = c->cuda(launch_start_vector(K.dtype, h->dim, ran_tab_dev, start_dev, v1,
                                      c->partials.as<double>(), c->counter.as<unsigned>(),
                                      c->sums.as<double>(), grid, c->stream), "start vector");
     c->launches++;
@@ -454,7 +510,7 @@ int krylov_start(Krylov &K, const void *start_dev, const double *ran_tab_dev, do
     if (rc) return rc;
     if (norm_out) *norm_out = std::sqrt(nrm2);
     if (!(std::sqrt(nrm2) >= K.cutoff)) return c->fail(EDK_ERR_ZERO_START, "start vector has zero norm");
-    rc = c->cuda(launch_scale(K.dtype, h->dim, K.w[K.ivk], c->sums.as<double>(), 0, K.psi, K.psi_coef,
+    rc = c->cuda(launch_scale(K.dtype, h->dim, v1, c->sums.as<double>(), 0, K.psi, K.psi_coef,
                               c->tri_sub.as<double>(), grid, c->stream), "scale");
     c->launches++;
     K.k = 0;
@@ -470,25 +526,44 @@ int krylov_step(Krylov &K)
     a.gamma1 = K.gamma1;
     if (K.k == 0) {
         a.mode = kModeFirst;
-        a.x = K.w[K.ivk];
+        a.x = K.basis ? K.basis->slot(0) : K.w[K.ivk];
         a.y = K.w[K.is];
         int rc = rows(h, K.dtype, a);
         if (rc) return rc;
         K.k = 1;
         return EDK_OK;
     }
+    if (K.basis && !K.basis->ensure(K.k)) {
+        // the budget ends here: carry on with rotating buffers from v_k, v_{k-1}
+        edk_ctx *c = h->ctx;
+        const size_t b = K.basis->vec_bytes();
+        int rc = c->cuda(cudaMemcpyAsync(K.w[K.ivk], K.basis->slot(K.k - 1), b, cudaMemcpyDeviceToDevice, c->stream),
+                         "basis fallback");
+        if (!rc && K.k >= 2)
+            rc = c->cuda(cudaMemcpyAsync(K.w[K.ivkm1], K.basis->slot(K.k - 2), b, cudaMemcpyDeviceToDevice,
+                                         c->stream), "basis fallback");
+        if (rc) return rc;
+        K.basis->valid = false;
+        K.basis = nullptr;
+    }
     a.mode = kModeStep;
     a.k = K.k;
     a.x = K.w[K.is];
     a.y = K.w[K.is_out];
-    a.vk = K.w[K.ivk];
-    a.vkm1 = (K.k >= 2) ? K.w[K.ivkm1] : nullptr;
-    a.vout = K.w[K.ivkm1];
+    if (K.basis) {
+        a.vk = K.basis->slot(K.k - 1);
+        a.vkm1 = K.k >= 2 ? K.basis->slot(K.k - 2) : nullptr;
+        a.vout = K.basis->slot(K.k);
+    } else {
+        a.vk = K.w[K.ivk];
+        a.vkm1 = (K.k >= 2) ? K.w[K.ivkm1] : nullptr;
+        a.vout = K.w[K.ivkm1];
+    }
     a.psi = K.psi;
     a.psi_coef = K.psi_coef;
     int rc = rows(h, K.dtype, a);
     if (rc) return rc;
-    std::swap(K.ivk, K.ivkm1);      // v_{k+1} now in the old v_{k-1} slot
+    if (!K.basis) std::swap(K.ivk, K.ivkm1);      // v_{k+1} now in the old v_{k-1} slot
     std::swap(K.is, K.is_out);
     K.k += 1;
     return EDK_OK;
@@ -502,7 +577,7 @@ int krylov_run(Krylov &K, int target)
 {
     edk_ctx *c = K.h->ctx;
     while (K.k < target) {
-        const bool eligible = c->graphs && !K.graph_off && K.k >= 2 && target - K.k >= 2;
+        const bool eligible = c->graphs && !K.graph_off && !K.basis && K.k >= 2 && target - K.k >= 2;
         if (eligible && !K.gexec) {
             // capture two steps with the device step counter, then restore the host state
             const Krylov save_state{K.h, K.dtype, {}, K.ivk, K.ivkm1, K.is, K.is_out, K.k};
@@ -1145,6 +1220,24 @@ int edk_lanczos_e0(edk_h *h, const edk_lanczos_opts *o, edk_lanczos_result *r)
     K.cutoff = o->cutoff_min_lanczos_vec > 0 ? o->cutoff_min_lanczos_vec : 1e-25;
     const double *tab = ran_tab_for(c, o->ran_tab, &rc);
     if (rc) return rc;
+    Basis &B = h->basis;
+    if (!B.chunks.empty()) {
+        B.release(c->stream);
+        cudaStreamSynchronize(c->stream);     // the freed chunks count as free below
+    }
+    if (o->keep_basis) {
+        // leave 1/16 of the device (at least 4 GB) to everything else
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) { (void)cudaGetLastError(); free_b = 0; }
+        const size_t reserve = std::max<size_t>((size_t)4 << 30, total_b / 16);
+        B.dtype = o->dtype;
+        B.dim = h->dim;
+        B.st = c->stream;
+        const size_t avail = free_b > reserve ? free_b - reserve : 0;
+        const int64_t fit = (int64_t)(avail / (B.stride() * kBasisChunk)) * kBasisChunk;
+        B.cap = (int)std::min<int64_t>(fit, (int64_t)niter_max + 1 + kBasisChunk);
+        if (B.cap >= 2 * kBasisChunk) K.basis = &B;
+    }
     if ((rc = krylov_start(K, o->start_dev, tab, nullptr))) return rc;
     const int every = std::max(1, o->check_every);
     std::vector<double> last(ne, 1e300), valp(ne), rdist(ne);
@@ -1235,6 +1328,14 @@ int edk_lanczos_e0(edk_h *h, const edk_lanczos_opts *o, edk_lanczos_result *r)
         std::memcpy(r->vecp + (size_t)kept * n, v.data(), sizeof(double) * n);
         ++kept;
     }
+    if (K.basis) {
+        B.valid = true;
+        B.nvec = K.k;
+        B.start = o->start_dev;
+        B.tab = o->ran_tab;
+    } else if (!B.chunks.empty()) {
+        B.release(c->stream);
+    }
     r->nkept = kept;
     r->niter = n;
     r->status = status;
@@ -1256,17 +1357,30 @@ int edk_lanczos_gs(edk_h *h, const edk_lanczos_opts *o, int32_t niter, const dou
     cf.push_back(0.0);
     if ((rc = c->cuda(cudaMemcpyAsync(c->coef.p, cf.data(), sizeof(double) * cf.size(),
                                       cudaMemcpyHostToDevice, c->stream), "h2d coef"))) return rc;
-    K.psi = psi_dev;
-    K.psi_coef = c->coef.as<double>();
     const double *tab = ran_tab_for(c, o->ran_tab, &rc);
     if (rc) return rc;
-    if ((rc = krylov_start(K, o->start_dev, tab, nullptr))) return rc;
-    // iterations 1..niter-1 produce v_2..v_niter (the last H*v is not needed
-    // by the eigenvector but keeps one kernel for every step)
-    if ((rc = krylov_run(K, niter))) return rc;
-    if (niter == 1) {
-        // nothing beyond psi = coef[0] v1
+    Basis &B = h->basis;
+    const bool stored = o->keep_basis && B.valid && B.dtype == o->dtype && B.dim == h->dim && B.nvec >= niter &&
+                        B.start == o->start_dev && B.tab == o->ran_tab;
+    DevBuf dptr;   // outlives the final stream synchronisation
+    if (stored) {
+        // psi = sum_q coef[q] v_{q+1} from the vectors pass 1 kept
+        std::vector<const void *> ptrs(niter);
+        for (int q = 0; q < niter; ++q) ptrs[q] = B.slot(q);
+        if ((rc = c->cuda(upload(dptr, ptrs, c->stream), "upload basis pointers"))) return rc;
+        rc = c->cuda(launch_combine(o->dtype, h->dim, dptr.as<const void *const>(), c->coef.as<double>(), niter,
+                                    psi_dev, c->reduce_grid, c->stream), "combine basis");
+        c->launches++;
+        if (rc) return rc;
+    } else {
+        K.psi = psi_dev;
+        K.psi_coef = c->coef.as<double>();
+        if ((rc = krylov_start(K, o->start_dev, tab, nullptr))) return rc;
+        // iterations 1..niter-1 produce v_2..v_niter (the last H*v is not needed
+        // by the eigenvector but keeps one kernel for every step)
+        if ((rc = krylov_run(K, niter))) return rc;
     }
+    if (!B.chunks.empty() && o->keep_basis == 1) B.release(c->stream);
     // normalise psi
     if ((rc = c->cuda(launch_norm2(o->dtype, h->dim, psi_dev, c->partials.as<double>(),
                                    c->counter.as<unsigned>(), c->sums.as<double>() + 8, c->reduce_grid,

@@ -217,6 +217,9 @@ cudaError_t launch_scale(int dtype, int64_t n, void *v, const double *sums, int 
                          cudaStream_t st);
 cudaError_t launch_norm2(int dtype, int64_t n, const void *v, double *partials, unsigned *counter,
                          double *sums_out, int grid, cudaStream_t st);
+// psi = sum_q coef[q] v_q over nv stored vectors (vecs_dev: device array of pointers)
+cudaError_t launch_combine(int dtype, int64_t n, const void *const *vecs_dev, const double *coef_dev, int nv,
+                           void *psi, int grid, cudaStream_t st);
 cudaError_t launch_convert(int from_dtype, int to_dtype, int64_t n, const void *in, void *out,
                            cudaStream_t st);
 cudaError_t launch_apply_c(int dtype, int spin, int64_t dother, int64_t dup_src, int64_t dup_tgt,

@@ -358,6 +358,20 @@ __global__ void scale_kernel(int64_t n, T *v, const double *sums, int which, T *
     }
 }
 
+// psi = sum_q coef[q] v_q over stored Krylov vectors, accumulated in the
+// order the fused steps of a recomputing pass 2 use: psi = coef[0] v_0, then
+// psi += coef[q] v_q for q = 1, 2, ... (each stored in the element type).
+template <typename T>
+__global__ void combine_kernel(int64_t n, const T *const *vecs, const double *coef, int nv, T *psi)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        T p = (T)(coef[0] * (double)vecs[0][i]);
+        for (int q = 1; q < nv; ++q) p = (T)((double)p + coef[q] * (double)__ldg(vecs[q] + i));
+        psi[i] = p;
+    }
+}
+
 template <typename A, typename B>
 __global__ void convert_kernel(int64_t n, const A *in, B *out)
 {
@@ -581,6 +595,16 @@ cudaError_t launch_start_vector(int dtype, int64_t n, const double *tab, const v
     else
         start_kernel<float><<<grid, 256, 0, st>>>(n, tab, (const float *)user, (float *)v,
                                                   partials, counter, sums);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_combine(int dtype, int64_t n, const void *const *vecs_dev, const double *coef_dev, int nv,
+                           void *psi, int grid, cudaStream_t st)
+{
+    if (dtype == EDK_F64)
+        combine_kernel<double><<<grid, 256, 0, st>>>(n, (const double *const *)vecs_dev, coef_dev, nv, (double *)psi);
+    else
+        combine_kernel<float><<<grid, 256, 0, st>>>(n, (const float *const *)vecs_dev, coef_dev, nv, (float *)psi);
     return cudaGetLastError();
 }
 

@@ -53,7 +53,8 @@ class _LanczosOpts(C.Structure):
     _fields_ = [("nitermax", C.c_int32), ("neigen", C.c_int32), ("tolerance", C.c_double),
                 ("demax", C.c_double), ("cutoff_min_lanczos_vec", C.c_double), ("dtype", C.c_int32),
                 ("check_every", C.c_int32), ("ran_tab", C.c_void_p), ("start_dev", C.c_void_p),
-                ("use_target", C.c_int32), ("target", C.c_double), ("residual_tol", C.c_double)]
+                ("use_target", C.c_int32), ("target", C.c_double), ("residual_tol", C.c_double),
+                ("keep_basis", C.c_int32)]
 
 
 class _LanczosResult(C.Structure):
@@ -453,20 +454,22 @@ class Hamiltonian:
 
     # ---- Lanczos -------------------------------------------------------
     def _opts(self, dtype, nitermax, neigen, tolerance, demax, cutoff, check_every, ran_tab, start,
-              target=None, residual_tol=0.0):
+              target=None, residual_tol=0.0, keep_basis=False):
         self._tab = None if ran_tab is None else np.ascontiguousarray(ran_tab, np.float64)
         return _LanczosOpts(int(nitermax), int(neigen), float(tolerance), float(demax), float(cutoff),
                             _dtype_code(dtype), int(check_every),
                             None if self._tab is None else self._tab.ctypes.data,
                             None if start is None else _ptr(start),
                             0 if target is None else 1, 0.0 if target is None else float(target),
-                            float(residual_tol))
+                            float(residual_tol), 1 if keep_basis else 0)
 
     def lanczos_e0(self, dtype="f64", nitermax=1000, neigen=1, tolerance=1e-12, demax=1e300,
-                   cutoff=1e-25, check_every=8, ran_tab=None, start=None, target=None, residual_tol=0.0):
-        """Pass 1 (Lanczos_fast_diagonalize). Returns a dict."""
+                   cutoff=1e-25, check_every=8, ran_tab=None, start=None, target=None, residual_tol=0.0,
+                   keep_basis=False):
+        """Pass 1 (Lanczos_fast_diagonalize). Returns a dict.  keep_basis: keep
+        the Krylov vectors on the device for a following lanczos_gs(keep_basis=True)."""
         o = self._opts(dtype, nitermax, neigen, tolerance, demax, cutoff, check_every, ran_tab, start, target,
-                       residual_tol)
+                       residual_tol, keep_basis)
         cap = min(self.dim, nitermax) + 2
         diag = np.zeros(cap)
         sub = np.zeros(cap)
@@ -479,11 +482,13 @@ class Hamiltonian:
                     diag=diag[:n].copy(), subdiag=sub[:n + 1].copy(),
                     vecp=vecp[:k * n].reshape(k, n).copy())
 
-    def lanczos_gs(self, coef, dtype="f64", ran_tab=None, start=None, cutoff=1e-25):
-        """Pass 2 (Lanczos_get_GS_sector): normalised eigenvector as a device tensor."""
+    def lanczos_gs(self, coef, dtype="f64", ran_tab=None, start=None, cutoff=1e-25, keep_basis=False):
+        """Pass 2 (Lanczos_get_GS_sector): normalised eigenvector as a device tensor.
+        keep_basis: form it from the vectors a lanczos_e0(keep_basis=True) with
+        the same start kept (recomputing the recurrence when there are none)."""
         import torch
         code = _dtype_code(dtype)
-        o = self._opts(code, 1, 1, 0.0, 0.0, cutoff, 1, ran_tab, start)
+        o = self._opts(code, 1, 1, 0.0, 0.0, cutoff, 1, ran_tab, start, keep_basis=keep_basis)
         coef = np.ascontiguousarray(coef, np.float64)
         psi = torch.zeros(self.dim, dtype=_torch_dtype(code), device=f"cuda:{self.ctx.device}")
         self.ctx.check(lib().edk_lanczos_gs(self.h, C.byref(o), len(coef), coef.ctypes.data, _ptr(psi)),

@@ -49,6 +49,7 @@ module edk_fortran
     type(c_ptr) :: ran_tab, start_dev
     integer(c_int32_t) :: use_target
     real(c_double) :: target, residual_tol
+    integer(c_int32_t) :: keep_basis
   end type
 
   ! parameter of the adjoint: kind EDK_PARAM_EC=0, EB=1, VBC=2, U=3 (0-based i, j);

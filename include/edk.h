@@ -153,6 +153,18 @@ typedef struct edk_lanczos_opts {
     double residual_tol;         /* > 0: also require the Ritz residual beta_{k+1}|y_k| below
                                     this (an eigenvector criterion; the reference stops on the
                                     eigenvalue change alone) */
+    int32_t keep_basis;          /* != 0 in pass 1: it writes its Krylov vectors into device memory
+                                    kept on the Hamiltonian (as far as free memory allows, leaving
+                                    1/16 of the device and at least 4 GB; pass 1 then runs without
+                                    graph replay).  != 0 in pass 2 with the same start_dev and
+                                    ran_tab pointers: psi is formed from the kept vectors in one
+                                    pass instead of recomputing the recurrence (which it does when
+                                    none are kept or too few); 1 releases them afterwards, 2 keeps
+                                    them for another eigenvector of the same chain.  The next pass
+                                    1 and edk_h_destroy release them too.  0: pass 2 recomputes
+                                    (the reference's way).  Every pass 1 allocates the vectors
+                                    afresh, which costs more than the H*v steps it saves on short
+                                    chains over large sectors: edk_solve leaves it off. */
 } edk_lanczos_opts;
 
 typedef struct edk_lanczos_result {
