@@ -118,6 +118,10 @@ struct edk_ctx {
     DevBuf b_hams, b_items, b_queue, b_alpha, b_beta, b_done, b_work;
     struct BatchShape { int block, R, per_sm; };
     std::vector<std::pair<std::string, BatchShape>> batch_tuned;
+    // fast-kernel launch shape timed per sector shape (element type, dim_up,
+    // dim_dn, table widths, impurity sites): a rebuilt Hamiltonian of the same
+    // shape (a new bath, a cleared cache) reuses it instead of timing again
+    std::vector<std::pair<std::string, FastShape>> fast_by_shape;
     cudaEvent_t get_event() {
         if (!event_pool.empty()) { cudaEvent_t e = event_pool.back(); event_pool.pop_back(); return e; }
         cudaEvent_t e = nullptr;
@@ -391,6 +395,16 @@ int fast_shape_for(edk_h *h, int dtype, const RowArgs &a, FastShape &out)
         return EDK_OK;
     }
     if (h->fast_tuned[dtype]) { out = h->fast_shape[dtype]; return EDK_OK; }
+    char key[160];
+    std::snprintf(key, sizeof key, "%d:%lld:%lld:%d:%d:%d", dtype, (long long)h->H.dup, (long long)h->H.ddn,
+                  h->H.up.ell_k, h->H.dn_kmax, h->H.nc);
+    if (c->kernel_path == 0)
+        for (const auto &kv : c->fast_by_shape)
+            if (kv.first == key) {
+                out = h->fast_shape[dtype] = kv.second;
+                h->fast_tuned[dtype] = true;
+                return EDK_OK;
+            }
     const int n = fast_shapes(h->H, eb, c->num_sms, cand, 12);
     if (n == 0) return c->fail(EDK_ERR_INVALID, "fast row kernel: no launch shape");
     out = cand[0];
@@ -419,6 +433,7 @@ int fast_shape_for(edk_h *h, int dtype, const RowArgs &a, FastShape &out)
     if (rc) return rc;
     h->fast_shape[dtype] = out;
     h->fast_tuned[dtype] = true;
+    c->fast_by_shape.push_back({key, out});
     return EDK_OK;
 }
 

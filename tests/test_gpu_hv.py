@@ -157,3 +157,30 @@ def test_every_fast_kernel_launch_shape_is_exact(ctx):
                 assert np.abs(yf - y32).max() <= 1.2e-7 * np.abs(y32).max(), (sec, i)
         finally:
             ctx.set_kernel_path(0)
+
+
+def test_launch_shape_timed_once_per_sector_shape():
+    """The fast kernel's launch shape is timed on the first H*v of a sector
+    shape; a second Hamiltonian of the same shape in the same context reuses
+    it (one launch per H*v) and gives the same bits."""
+    import torch
+    c = edk.Context(0)
+    try:
+        m = workload("c3").model
+        x = torch.tensor(np.random.default_rng(3).normal(size=3432 * 3432), device="cuda")
+        h1 = edk.Hamiltonian(c, m, 7, 7)
+        n0 = c.launches
+        y1 = h1.hmult(x)
+        tuned = c.launches - n0
+        assert tuned > 1                    # the feasible shapes were timed
+        h2 = edk.Hamiltonian(c, m, 7, 7)
+        n1 = c.launches
+        y2 = h2.hmult(x)
+        assert c.launches - n1 == 1
+        assert torch.equal(y1, y2)
+        h3 = edk.Hamiltonian(c, m, 7, 6)    # another shape: timed again
+        n2 = c.launches
+        h3.hmult(torch.zeros(h3.dim, dtype=torch.float64, device="cuda"))
+        assert c.launches - n2 > 1
+    finally:
+        c.close()
