@@ -122,6 +122,37 @@ struct edk_ctx {
     // dim_dn, table widths, impurity sites): a rebuilt Hamiltonian of the same
     // shape (a new bath, a cleared cache) reuses it instead of timing again
     std::vector<std::pair<std::string, FastShape>> fast_by_shape;
+    // stream-ordered pool of the Krylov vectors kept between the Lanczos passes
+    // (keep_basis); it keeps freed chunks, up to 5/8 of the device, so later
+    // passes reuse them without mapping new device memory
+    cudaMemPool_t basis_pool = nullptr;
+    cudaMemPool_t get_basis_pool() {
+        if (basis_pool) return basis_pool;
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        if (cudaMemPoolCreate(&basis_pool, &props) != cudaSuccess) {
+            (void)cudaGetLastError();
+            basis_pool = nullptr;
+            return nullptr;
+        }
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) { (void)cudaGetLastError(); total_b = 0; }
+        uint64_t keep = (uint64_t)(total_b / 8 * 5);
+        cudaMemPoolSetAttribute(basis_pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        return basis_pool;
+    }
+    // bytes the basis pool holds but no basis uses
+    size_t basis_pool_idle() const {
+        if (!basis_pool) return 0;
+        uint64_t reserved = 0, used = 0;
+        if (cudaMemPoolGetAttribute(basis_pool, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess ||
+            cudaMemPoolGetAttribute(basis_pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess)
+            return 0;
+        return reserved > used ? (size_t)(reserved - used) : 0;
+    }
     cudaEvent_t get_event() {
         if (!event_pool.empty()) { cudaEvent_t e = event_pool.back(); event_pool.pop_back(); return e; }
         cudaEvent_t e = nullptr;
@@ -147,6 +178,7 @@ struct edk_ctx {
         if (pin_tri) cudaFreeHost(pin_tri);
         if (pin_ev) cudaEventDestroy(pin_ev);
         for (auto e : event_pool) cudaEventDestroy(e);
+        if (basis_pool) cudaMemPoolDestroy(basis_pool);
     }
 
     int fail(int code, const char *fmt, ...) {
@@ -207,9 +239,12 @@ int ctx_init(edk_ctx *c)
 // sector Hamiltonian
 // ---------------------------------------------------------------------------
 // Krylov vectors kept between pass 1 and pass 2 (edk_lanczos_opts.keep_basis):
-// v_1, v_2, ... in chunks of kBasisChunk vectors, allocated stream-ordered as
-// pass 1 reaches them.
-constexpr int kBasisChunk = 8;
+// v_1, v_2, ... in chunks allocated from the context's pool as pass 1 reaches
+// them.  Large sectors use chunks of kBasisChunkBytes (as many vectors as fit;
+// one vector when it is larger), so the pool hands a freed chunk to the next
+// pass whatever its sector and element type; a chain that needs less than one
+// such chunk gets one chunk of its own size.
+constexpr size_t kBasisChunkBytes = (size_t)4 << 30;
 struct Basis {
     int dtype = -1;
     int64_t dim = 0;
@@ -219,21 +254,26 @@ struct Basis {
     const void *start = nullptr; // identity of the pass-1 start (start_dev, host ran_tab)
     const double *tab = nullptr;
     cudaStream_t st = nullptr;
+    cudaMemPool_t pool = nullptr;
     std::vector<void *> chunks;
     size_t vec_bytes() const { return (size_t)dim * (dtype == EDK_F64 ? 8 : 4); }
     // slots start on 256-byte boundaries, like separate allocations
     size_t stride() const { return (vec_bytes() + 255) & ~(size_t)255; }
+    size_t chunk = 0;            // bytes per chunk, a multiple of stride()
+    int per_chunk() const { return (int)(chunk / stride()); }
+    size_t chunk_bytes() const { return chunk; }
     void *slot(int q) const
     {
-        return static_cast<char *>(chunks[(size_t)q / kBasisChunk]) + (size_t)(q % kBasisChunk) * stride();
+        const int pc = per_chunk();
+        return static_cast<char *>(chunks[(size_t)q / pc]) + (size_t)(q % pc) * stride();
     }
     // makes slot q usable; false when the budget or an allocation says no
     bool ensure(int q)
     {
-        if (q >= cap) return false;
-        while ((int)chunks.size() * kBasisChunk <= q) {
+        if (q >= cap || !pool) return false;
+        while ((int64_t)chunks.size() * per_chunk() <= q) {
             void *p = nullptr;
-            if (cudaMallocAsync(&p, stride() * kBasisChunk, st) != cudaSuccess) {
+            if (cudaMallocFromPoolAsync(&p, chunk_bytes(), pool, st) != cudaSuccess) {
                 (void)cudaGetLastError();
                 return false;
             }
@@ -1240,18 +1280,23 @@ int edk_lanczos_e0(edk_h *h, const edk_lanczos_opts *o, edk_lanczos_result *r)
         B.release(c->stream);
         cudaStreamSynchronize(c->stream);     // the freed chunks count as free below
     }
-    if (o->keep_basis) {
-        // leave 1/16 of the device (at least 4 GB) to everything else
+    if (o->keep_basis && (B.pool = c->get_basis_pool())) {
+        // leave 1/16 of the device (at least 4 GB) to everything else; the
+        // pool's idle chunks count as free
         size_t free_b = 0, total_b = 0;
         if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) { (void)cudaGetLastError(); free_b = 0; }
+        free_b += c->basis_pool_idle();
         const size_t reserve = std::max<size_t>((size_t)4 << 30, total_b / 16);
         B.dtype = o->dtype;
         B.dim = h->dim;
         B.st = c->stream;
+        const size_t s = B.stride();
+        const size_t whole = s * ((size_t)niter_max + 1);
+        B.chunk = s >= kBasisChunkBytes ? s : std::min(whole, kBasisChunkBytes / s * s);
         const size_t avail = free_b > reserve ? free_b - reserve : 0;
-        const int64_t fit = (int64_t)(avail / (B.stride() * kBasisChunk)) * kBasisChunk;
-        B.cap = (int)std::min<int64_t>(fit, (int64_t)niter_max + 1 + kBasisChunk);
-        if (B.cap >= 2 * kBasisChunk) K.basis = &B;
+        const int64_t fit = (int64_t)(avail / B.chunk_bytes()) * B.per_chunk();
+        B.cap = (int)std::min<int64_t>(fit, (int64_t)niter_max + 1 + B.per_chunk());
+        if (B.cap >= 2) K.basis = &B;
     }
     if ((rc = krylov_start(K, o->start_dev, tab, nullptr))) return rc;
     const int every = std::max(1, o->check_every);

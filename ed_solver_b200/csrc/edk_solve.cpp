@@ -258,6 +258,7 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
             lo.check_every = o->check_every > 0 ? o->check_every : 8;
             lo.ran_tab = o->ran_tab;
             lo.residual_tol = sdt == EDK_F64 ? o->residual_tol : 0.0;
+            lo.keep_basis = o->recompute_pass2 ? 0 : 1;   // pass 2 from pass 1's vectors
             edk_lanczos_result lr{};
             lr.diag = diag.data();
             lr.subdiag = sub.data();
@@ -270,8 +271,9 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
                 stt->converged = lr.converged[k];
                 stt->psi = DBuf((size_t)dim * ebytes);
                 if (!stt->psi.p) return edk_internal_fail(ctx, EDK_ERR_NOMEM, "state vector");
+                if (lo.keep_basis) lo.keep_basis = k + 1 < lr.nkept ? 2 : 1;
                 if ((rc = edk_lanczos_gs(h, &lo, lr.niter, lr.vecp + (size_t)k * lr.niter, stt->psi.p))) return rc;
-                lanczos_steps += lr.niter;
+                lanczos_steps += lr.niter;      // the reference's count: pass 2 reruns the recurrence
                 if (sdt == EDK_F32) {
                     // FP64 refinement restart from the FP32 eigenvector
                     DBuf p64((size_t)dim * 8);
@@ -285,6 +287,7 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
                     ro.use_target = 1;
                     ro.target = stt->E;
                     ro.check_every = 4;
+                    ro.keep_basis = o->recompute_pass2 ? 0 : 1;
                     ro.residual_tol = o->residual_tol > 0.0 ? o->residual_tol : 1e-9 * std::max(1.0, std::fabs(stt->E));
                     edk_lanczos_result rr{};
                     rr.diag = diag.data();

@@ -70,7 +70,8 @@ class _SolveOpts(C.Structure):
                 ("nitergreen", C.c_int32), ("nw", C.c_int32), ("spin_mask", C.c_int32), ("npairs", C.c_int32),
                 ("pairs", C.c_void_p), ("cutoff_dynamic", C.c_double), ("ran_tab", C.c_void_p),
                 ("residual_tol", C.c_double), ("green_mode", C.c_int32), ("gs_in", C.c_char_p),
-                ("gs_out", C.c_char_p), ("sector_bound_file", C.c_char_p), ("iwindow", C.c_int32)]
+                ("gs_out", C.c_char_p), ("sector_bound_file", C.c_char_p), ("iwindow", C.c_int32),
+                ("recompute_pass2", C.c_int32)]
 
 
 class _ChilocSectors(C.Structure):
@@ -795,8 +796,10 @@ def sector_bounds_write(path: str, nup, ndn, sz=(1000, -1000)):
 def solve(ctx: Context, model: AIMModel, sectors, beta: float, nw: int, dtype="f64", neigen=1,
           nitermax=1000, tolerance=1e-12, tolerance_lowprec=1e-6, demax0=5.0, nitergreen=200,
           spins=(0, 1), pairs=None, cutoff_dynamic=1e-8, check_every=8, ran_tab=None, residual_tol=0.0,
-          green_mode=0, gs_in=None, gs_out=None, sector_bound_file=None, iwindow=1):
+          green_mode=0, gs_in=None, gs_out=None, sector_bound_file=None, iwindow=1, recompute_pass2=False):
     """One impurity solve through the C-ABI (edk_solve): host inputs, host outputs.
+    recompute_pass2: rerun the Lanczos recurrence in pass 2 (the reference's way)
+    instead of forming the eigenvectors from the Krylov vectors pass 1 kept.
 
     Returns dict(e0, z, residual, nstates, lanczos_steps, green_steps, G (2, npairs, nw) complex,
     docc (nc,), energies, sectors, e0_lowprec).
@@ -812,7 +815,8 @@ def solve(ctx: Context, model: AIMModel, sectors, beta: float, nw: int, dtype="f
                    int(nw), int(mask), len(pr) // 2, pr.ctypes.data, float(cutoff_dynamic),
                    None if tab is None else tab.ctypes.data, float(residual_tol), int(green_mode),
                    None if gs_in is None else gs_in.encode(), None if gs_out is None else gs_out.encode(),
-                   None if sector_bound_file is None else sector_bound_file.encode(), int(iwindow))
+                   None if sector_bound_file is None else sector_bound_file.encode(), int(iwindow),
+                   1 if recompute_pass2 else 0)
     G = np.zeros((2, len(pr) // 2, nw, 2))
     docc = np.zeros(model.nc)
     en = np.zeros(64)

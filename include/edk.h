@@ -156,15 +156,17 @@ typedef struct edk_lanczos_opts {
     int32_t keep_basis;          /* != 0 in pass 1: it writes its Krylov vectors into device memory
                                     kept on the Hamiltonian (as far as free memory allows, leaving
                                     1/16 of the device and at least 4 GB; pass 1 then runs without
-                                    graph replay).  != 0 in pass 2 with the same start_dev and
+                                    graph replay).  The memory comes from a pool owned by the
+                                    context, which keeps released chunks (up to 5/8 of the device)
+                                    for the next pass and returns them when the context is
+                                    destroyed.  != 0 in pass 2 with the same start_dev and
                                     ran_tab pointers: psi is formed from the kept vectors in one
                                     pass instead of recomputing the recurrence (which it does when
                                     none are kept or too few); 1 releases them afterwards, 2 keeps
                                     them for another eigenvector of the same chain.  The next pass
                                     1 and edk_h_destroy release them too.  0: pass 2 recomputes
-                                    (the reference's way).  Every pass 1 allocates the vectors
-                                    afresh, which costs more than the H*v steps it saves on short
-                                    chains over large sectors: edk_solve leaves it off. */
+                                    (the reference's way).  edk_solve sets it unless
+                                    edk_solve_opts.recompute_pass2 is set. */
 } edk_lanczos_opts;
 
 typedef struct edk_lanczos_result {
@@ -392,6 +394,10 @@ typedef struct edk_solve_opts {
                                     (solver.h:107-137), and the bounds of the states found are
                                     written back to it (get_new_bounds, solver.h:374-415) */
     int32_t iwindow;             /* window around the bounds (reference default 1) */
+    int32_t recompute_pass2;     /* 0: each Lanczos pass 1 keeps its Krylov vectors on the device
+                                    (edk_lanczos_opts.keep_basis) and pass 2 forms the eigenvector
+                                    from them; 1: pass 2 reruns the recurrence (the reference's
+                                    Lanczos_get_GS_sector) */
 } edk_solve_opts;
 
 typedef struct edk_solve_result {
@@ -399,7 +405,8 @@ typedef struct edk_solve_result {
     double e0_lowprec;           /* mixed: lowest FP32 eigenvalue before refinement */
     double residual;             /* |H psi0 - E0 psi0| / |psi0| with the FP64 matvec */
     int32_t nstates;             /* eigenstates in the Boltzmann window */
-    int32_t lanczos_steps;       /* H*v applications of the eigen part */
+    int32_t lanczos_steps;       /* Lanczos steps of the eigen part as the reference counts them
+                                    (pass 2 included, also when it is formed from kept vectors) */
     int32_t green_steps;         /* H*v applications of the Green part */
     double *G;                   /* host [2][npairs][nw][2] (spin, pair, w, re/im) or NULL */
     double *docc;                /* host [nc] or NULL */
