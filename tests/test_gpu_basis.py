@@ -73,3 +73,17 @@ def test_stored_basis_nambu(ctx):
     ref = h.lanczos_gs(r0["vecp"][0]).cpu().numpy()
     got = h.lanczos_gs(r1["vecp"][0], keep_basis=True).cpu().numpy()
     assert np.abs(got - ref).max() < 1e-13
+
+
+@pytest.mark.parametrize("dtype,tol", [("f64", 1e-12), ("f32", 1e-6)])
+def test_solve_pass2_from_kept_vectors_matches_recompute(ctx, dtype, tol):
+    """edk_solve with pass 2 formed from the kept Krylov vectors (the default)
+    and with the reference's recomputing pass 2 give the same E0 and G."""
+    from ed_solver_b200.model import workload as wl
+    w = wl("c1")
+    kw = dict(dtype=dtype, nitermax=w.nitermax, nitergreen=60)
+    a = edk.solve(ctx, w.model, w.sectors, w.beta, 64, **kw)
+    b = edk.solve(ctx, w.model, w.sectors, w.beta, 64, recompute_pass2=True, **kw)
+    assert abs(a["e0"] - b["e0"]) <= tol * abs(b["e0"])
+    assert np.abs(a["G"] - b["G"]).max() <= tol * np.abs(b["G"]).max()
+    assert a["lanczos_steps"] == b["lanczos_steps"]
