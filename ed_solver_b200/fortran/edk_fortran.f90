@@ -70,6 +70,54 @@ module edk_fortran
     integer(c_int32_t) :: stored_vectors
   end type
 
+  ! block Lanczos options (edk_block_lanczos)
+  type, bind(C) :: edk_block_opts
+    integer(c_int32_t) :: block, nitermax, neigen
+    real(c_double) :: tolerance
+    integer(c_int32_t) :: check_every
+    type(c_ptr) :: ran_tab
+  end type
+
+  ! one chain of a batched Green-function launch (edk_green_batch)
+  type, bind(C) :: edk_chain
+    type(c_ptr) :: target, start_dev
+    real(c_double) :: e0
+    integer(c_int32_t) :: iph
+    real(c_double) :: weight
+    integer(c_int32_t) :: out
+  end type
+
+  type, bind(C) :: edk_batch_stats
+    integer(c_int64_t) :: steps
+    integer(c_int32_t) :: chains
+    real(c_double) :: kernel_ms
+    integer(c_int32_t) :: block, rows, blocks_per_sm, tuned_shapes
+  end type
+
+  ! one impurity solve (edk_solve): options and results
+  type, bind(C) :: edk_solve_opts
+    integer(c_int32_t) :: dtype, nsectors
+    type(c_ptr) :: sectors
+    integer(c_int32_t) :: neigen, nitermax
+    real(c_double) :: tolerance, tolerance_lowprec
+    integer(c_int32_t) :: check_every
+    real(c_double) :: beta, demax0
+    integer(c_int32_t) :: nitergreen, nw, spin_mask, npairs
+    type(c_ptr) :: pairs
+    real(c_double) :: cutoff_dynamic
+    type(c_ptr) :: ran_tab
+    real(c_double) :: residual_tol
+    integer(c_int32_t) :: green_mode
+    type(c_ptr) :: gs_in, gs_out, sector_bound_file
+    integer(c_int32_t) :: iwindow, recompute_pass2
+  end type
+
+  type, bind(C) :: edk_solve_result
+    real(c_double) :: e0, z, e0_lowprec, residual
+    integer(c_int32_t) :: nstates, lanczos_steps, green_steps
+    type(c_ptr) :: G, docc, energies, state_sectors
+  end type
+
   type, bind(C) :: edk_lanczos_result
     integer(c_int32_t) :: nkept, niter, status
     real(c_double) :: E(64)
@@ -268,6 +316,170 @@ module edk_fortran
       type(edk_param), intent(in) :: params(*)
       real(c_double), intent(out) :: grad(*), G(*)
       type(edk_grad_stats), intent(out) :: stats
+    end function
+
+    ! ---- context utilities ----
+    integer(c_int) function edk_ctx_set_stream(ctx, stream) bind(C, name="edk_ctx_set_stream")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx, stream
+    end function
+    type(c_ptr) function edk_ctx_last_error(ctx) bind(C, name="edk_ctx_last_error")
+      import :: c_ptr
+      type(c_ptr), value :: ctx
+    end function
+    integer(c_int64_t) function edk_ctx_launch_count(ctx) bind(C, name="edk_ctx_launch_count")
+      import :: c_int64_t, c_ptr
+      type(c_ptr), value :: ctx
+    end function
+    integer(c_int) function edk_ctx_timing(ctx, enable) bind(C, name="edk_ctx_timing")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: enable
+    end function
+    integer(c_int) function edk_ctx_set_kernel_path(ctx, path) bind(C, name="edk_ctx_set_kernel_path")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: path
+    end function
+    integer(c_int) function edk_ctx_set_graphs(ctx, enable) bind(C, name="edk_ctx_set_graphs")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: enable
+    end function
+    integer(c_int) function edk_ctx_timing_report(ctx, which, launches, total_ms) &
+        bind(C, name="edk_ctx_timing_report")
+      import :: c_int, c_ptr, c_int64_t, c_double
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: which
+      integer(c_int64_t) :: launches
+      real(c_double) :: total_ms
+    end function
+    integer(c_int) function edk_ctx_timing_elements(ctx, which, elements) bind(C, name="edk_ctx_timing_elements")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: which
+      real(c_double) :: elements
+    end function
+    integer(c_int) function edk_ctx_transfer_bytes(ctx, h2d, d2h) bind(C, name="edk_ctx_transfer_bytes")
+      import :: c_int, c_ptr, c_int64_t
+      type(c_ptr), value :: ctx
+      integer(c_int64_t) :: h2d, d2h
+    end function
+    integer(c_int) function edk_ctx_clear_cache(ctx) bind(C, name="edk_ctx_clear_cache")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+    end function
+
+    ! ---- basis and tables (host-only) ----
+    integer(c_int64_t) function edk_binom(n, k) bind(C, name="edk_binom")
+      import :: c_int64_t, c_int
+      integer(c_int), value :: n, k
+    end function
+    ! states as unsigned 64-bit patterns, read through integer(c_int64_t)
+    integer(c_int) function edk_basis(ns, npart, states) bind(C, name="edk_basis")
+      import :: c_int, c_int64_t
+      integer(c_int), value :: ns, npart
+      integer(c_int64_t) :: states(*)
+    end function
+    integer(c_int) function edk_rank_table(ns, rank) bind(C, name="edk_rank_table")
+      import :: c_int, c_int32_t
+      integer(c_int), value :: ns
+      integer(c_int32_t) :: rank(*)
+    end function
+    integer(c_int) function edk_default_ran_tab(tab) bind(C, name="edk_default_ran_tab")
+      import :: c_int, c_double
+      real(c_double) :: tab(10001)
+    end function
+    ! arrays may be c_null_ptr for the size query
+    integer(c_int) function edk_build_table(m, spin, npart, dim, nnz, ptr, tgt, val, diag) &
+        bind(C, name="edk_build_table")
+      import :: c_int, c_ptr, c_int64_t, edk_model
+      type(edk_model), intent(in) :: m
+      integer(c_int), value :: spin, npart
+      integer(c_int64_t) :: dim, nnz
+      type(c_ptr), value :: ptr, tgt, val, diag
+    end function
+    integer(c_int) function edk_h_table(h, spin, nnz, ptr, tgt, val, diag) bind(C, name="edk_h_table")
+      import :: c_int, c_ptr, c_int64_t
+      type(c_ptr), value :: h
+      integer(c_int), value :: spin
+      integer(c_int64_t) :: nnz
+      type(c_ptr), value :: ptr, tgt, val, diag
+    end function
+
+    ! ---- vectors and observables ----
+    integer(c_int) function edk_convert(ctx, from_dtype, to_dtype, n, vin, vout) bind(C, name="edk_convert")
+      import :: c_int, c_ptr, c_int64_t
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: from_dtype, to_dtype
+      integer(c_int64_t), value :: n
+      type(c_ptr), value :: vin, vout
+    end function
+    integer(c_int) function edk_residual(h, psi, e, res_norm, psi_norm) bind(C, name="edk_residual")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h, psi
+      real(c_double), value :: e
+      real(c_double) :: res_norm, psi_norm
+    end function
+    integer(c_int) function edk_double_occ(h, dtype, psi, site, docc, norm2) bind(C, name="edk_double_occ")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h, psi
+      integer(c_int), value :: dtype, site
+      real(c_double) :: docc, norm2
+    end function
+
+    ! ---- continued fractions (invert_zmtridiag, matrices_tridiag.f90:163-198) ----
+    integer(c_int) function edk_cf_eval(ctx, nchain, ld, n, diag, subdiag, e, ph, scale, nw, wn, G) &
+        bind(C, name="edk_cf_eval")
+      import :: c_int, c_ptr, c_int32_t, c_double
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: nchain, ld, nw
+      integer(c_int32_t), intent(in) :: n(*)
+      real(c_double), intent(in) :: diag(*), subdiag(*), e(*), ph(*), scale(*), wn(*)
+      real(c_double), intent(out) :: G(*)
+    end function
+    ! the same without device allocation (static device scratch; no counterpart in the reference)
+    integer(c_int) function edk_cf_eval_noalloc(ctx, nchain, ld, n, diag, subdiag, e, ph, scale, nw, wn, G) &
+        bind(C, name="edk_cf_eval_noalloc")
+      import :: c_int, c_ptr, c_int32_t, c_double
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: nchain, ld, nw
+      integer(c_int32_t), intent(in) :: n(*)
+      real(c_double), intent(in) :: diag(*), subdiag(*), e(*), ph(*), scale(*), wn(*)
+      real(c_double), intent(out) :: G(*)
+    end function
+
+    ! ---- block Lanczos, batched chains, the solve driver ----
+    integer(c_int) function edk_block_lanczos(h, opts, E, vecs, niter, converged) bind(C, name="edk_block_lanczos")
+      import :: c_int, c_ptr, c_int32_t, c_double, edk_block_opts
+      type(c_ptr), value :: h
+      type(edk_block_opts), intent(in) :: opts
+      real(c_double) :: E(*)
+      type(c_ptr), value :: vecs
+      integer(c_int32_t) :: niter, converged
+    end function
+    integer(c_int) function edk_green_batch(ctx, dtype, nchain, chains, nitergreen, nw, wn, cutoff_dynamic, &
+        nout, G, mode, stats) bind(C, name="edk_green_batch")
+      import :: c_int, c_ptr, c_int32_t, c_double, edk_chain, edk_batch_stats
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: dtype
+      integer(c_int32_t), value :: nchain, nitergreen, nw, nout, mode
+      type(edk_chain), intent(in) :: chains(*)
+      real(c_double), intent(in) :: wn(*)
+      real(c_double), value :: cutoff_dynamic
+      real(c_double) :: G(*)
+      type(edk_batch_stats) :: stats
+    end function
+    integer(c_int) function edk_solve(ctx, m, o, r) bind(C, name="edk_solve")
+      import :: c_int, c_ptr, edk_model, edk_solve_opts, edk_solve_result
+      type(c_ptr), value :: ctx
+      type(edk_model), intent(in) :: m
+      type(edk_solve_opts), intent(in) :: o
+      type(edk_solve_result), intent(inout) :: r
+    end function
+    integer(c_int) function edk_chiloc_set_kernel(plain) bind(C, name="edk_chiloc_set_kernel")
+      import :: c_int
+      integer(c_int), value :: plain
     end function
   end interface
 
