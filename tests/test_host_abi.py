@@ -31,6 +31,14 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_fortran_module_binds_every_declared_symbol():
+    """The ISO_C_BINDING module names every entry point of include/*.h (and
+    nothing else) in its bind(C) interfaces."""
+    f90 = open(os.path.join(ROOT, "ed_solver_b200", "fortran", "edk_fortran.f90")).read()
+    bound = set(re.findall(r'bind\(C,\s*name="(edk_\w+)"\)', f90))
+    assert bound == declared_symbols(), (declared_symbols() - bound, bound - declared_symbols())
+
+
 def test_basis_and_rank_bit_exact():
     for ns in (1, 4, 8, 11, 16):
         for np_ in range(ns + 1):
