@@ -76,8 +76,9 @@ int64_t edk_ctx_launch_count(const edk_ctx *ctx);
  * FP32), the number of launches and their summed device time in ms. */
 int edk_ctx_timing(edk_ctx *ctx, int enable);
 /* Row-kernel selection: 0 = the fastest kernel whose preconditions hold
- * (default; the fast kernel's launch shape is timed once per sector and
- * element type), 1 = always the generic kernel (for A/B checks), 2 or 3 = the
+ * (default; the fast kernel's launch shape is timed once per sector shape
+ * and element type, and the context keeps the choice for later Hamiltonians of
+ * the same shape), 1 = always the generic kernel (for A/B checks), 2 or 3 = the
  * fast kernel where its preconditions hold with its default launch shape,
  * 16+i (i < 12) = the fast kernel with its i-th feasible launch shape (modulo
  * their number), for measurements. */
