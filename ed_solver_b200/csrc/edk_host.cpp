@@ -89,6 +89,7 @@ struct edk_ctx {
     // Krylov workspace shared by all sector Hamiltonians of this context:
     // v_{k-1}, v_k, s, s', scratch (per element type), grown on demand
     DevBuf work[2][5];
+    size_t work_limit = 0;   // > 0: the largest Krylov workspace a pass may allocate (bytes)
     size_t tri_cap = 0;
     int reduce_grid = 0;
     bool graphs = true;      // replay pairs of fused Lanczos steps as a CUDA graph
@@ -253,6 +254,11 @@ struct Basis {
     bool valid = false;
     const void *start = nullptr; // identity of the pass-1 start (start_dev, host ran_tab)
     const double *tab = nullptr;
+    // contents of the pass-1 start: |start_dev| (as the start kernel summed it)
+    // and the sum of the host ran_tab entries; pass 2 compares them before it
+    // uses the kept vectors
+    double start_norm = -1.0;
+    double tab_sum = 0.0;
     cudaStream_t st = nullptr;
     cudaMemPool_t pool = nullptr;
     std::vector<void *> chunks;
@@ -397,6 +403,10 @@ int check_model(edk_ctx *c, const edk_model *m)
 int work_ptrs(edk_h *h, int dtype, void *(&w)[5])
 {
     const size_t es = dtype == EDK_F64 ? 8 : 4;
+    const size_t limit = h->ctx->work_limit;
+    if (limit > 0 && 5 * es * (size_t)h->dim > limit)
+        return h->ctx->fail(EDK_ERR_NOMEM, "Krylov workspace of %zu bytes exceeds the context's limit of %zu bytes",
+                            5 * es * (size_t)h->dim, limit);
     for (int i = 0; i < 5; ++i) {
         int rc = h->ctx->cuda(h->ctx->work[dtype][i].ensure(es * (size_t)h->dim), "alloc Krylov workspace");
         if (rc) return rc;
@@ -564,6 +574,7 @@ int krylov_start(Krylov &K, const void *start_dev, const double *ran_tab_dev, do
     rc = c->cuda(cudaStreamSynchronize(c->stream), "sync");
     if (rc) return rc;
     if (norm_out) *norm_out = std::sqrt(nrm2);
+    if (!std::isfinite(nrm2)) return c->fail(EDK_ERR_NOT_FINITE, "start vector has a non-finite element");
     if (!(std::sqrt(nrm2) >= K.cutoff)) return c->fail(EDK_ERR_ZERO_START, "start vector has zero norm");
     rc = c->cuda(launch_scale(K.dtype, h->dim, v1, c->sums.as<double>(), 0, K.psi, K.psi_coef,
                               c->tri_sub.as<double>(), grid, c->stream), "scale");
@@ -791,6 +802,15 @@ int tri_wait(edk_ctx *c, int n, TriHost &t)
     return EDK_OK;
 }
 
+// Order-dependent sum of a caller's ran_tab (10001 entries), 0 for none.
+double host_tab_sum(const double *tab)
+{
+    if (!tab) return 0.0;
+    double s = 0.0;
+    for (int i = 0; i < 10001; ++i) s = s * 0.9999999 + tab[i];
+    return s;
+}
+
 const double *ran_tab_for(edk_ctx *c, const double *user_tab, int *rc)
 {
     *rc = EDK_OK;
@@ -903,6 +923,8 @@ int64_t edk_ctx_launch_count(const edk_ctx *ctx) { return ctx ? ctx->launches : 
 
 cudaStream_t edk_internal_stream(edk_ctx *ctx) { return ctx->stream; }
 
+int edk_internal_ctx_device(const edk_ctx *ctx) { return ctx->device; }
+
 int edk_internal_fail(edk_ctx *ctx, int code, const char *msg) { return ctx->fail(code, "%s", msg); }
 
 edk_ctx *edk_internal_h_ctx(edk_h *h) { return h->ctx; }
@@ -979,6 +1001,22 @@ int edk_ctx_transfer_bytes(const edk_ctx *ctx, int64_t *h2d, int64_t *d2h)
     if (h2d) *h2d = ctx->h2d_bytes;
     if (d2h) *d2h = ctx->d2h_bytes;
     return EDK_OK;
+}
+
+int edk_ctx_set_workspace_limit(edk_ctx *ctx, int64_t bytes)
+{
+    if (!ctx || bytes < 0) return EDK_ERR_INVALID;
+    ctx->work_limit = (size_t)bytes;
+    return EDK_OK;
+}
+
+int edk_ctx_trim(edk_ctx *ctx)
+{
+    if (!ctx) return EDK_ERR_INVALID;
+    if (!ctx->basis_pool) return EDK_OK;
+    int rc = ctx->cuda(cudaStreamSynchronize(ctx->stream), "sync");
+    if (rc) return rc;
+    return ctx->cuda(cudaMemPoolTrimTo(ctx->basis_pool, 0), "cudaMemPoolTrimTo");
 }
 
 int edk_ctx_clear_cache(edk_ctx *ctx)
@@ -1298,7 +1336,8 @@ int edk_lanczos_e0(edk_h *h, const edk_lanczos_opts *o, edk_lanczos_result *r)
         B.cap = (int)std::min<int64_t>(fit, (int64_t)niter_max + 1 + B.per_chunk());
         if (B.cap >= 2) K.basis = &B;
     }
-    if ((rc = krylov_start(K, o->start_dev, tab, nullptr))) return rc;
+    double start_norm = -1.0;
+    if ((rc = krylov_start(K, o->start_dev, tab, &start_norm))) return rc;
     const int every = std::max(1, o->check_every);
     std::vector<double> last(ne, 1e300), valp(ne), rdist(ne);
     std::vector<int> conv(ne, 0);
@@ -1393,6 +1432,8 @@ int edk_lanczos_e0(edk_h *h, const edk_lanczos_opts *o, edk_lanczos_result *r)
         B.nvec = K.k;
         B.start = o->start_dev;
         B.tab = o->ran_tab;
+        B.start_norm = start_norm;
+        B.tab_sum = host_tab_sum(o->ran_tab);
     } else if (!B.chunks.empty()) {
         B.release(c->stream);
     }
@@ -1420,8 +1461,22 @@ int edk_lanczos_gs(edk_h *h, const edk_lanczos_opts *o, int32_t niter, const dou
     const double *tab = ran_tab_for(c, o->ran_tab, &rc);
     if (rc) return rc;
     Basis &B = h->basis;
-    const bool stored = o->keep_basis && B.valid && B.dtype == o->dtype && B.dim == h->dim && B.nvec >= niter &&
-                        B.start == o->start_dev && B.tab == o->ran_tab;
+    bool stored = o->keep_basis && B.valid && B.dtype == o->dtype && B.dim == h->dim && B.nvec >= niter &&
+                  B.start == o->start_dev && B.tab == o->ran_tab && B.tab_sum == host_tab_sum(o->ran_tab);
+    if (stored && o->start_dev) {
+        // the same pointer must still hold the same start vector: compare its norm
+        // with the one pass 1 summed (same grid and order, so equal to rounding)
+        double n2 = 0.0;
+        rc = c->cuda(launch_norm2(o->dtype, h->dim, o->start_dev, c->partials.as<double>(), c->counter.as<unsigned>(),
+                                  c->sums.as<double>() + 12, c->reduce_grid, c->stream), "norm2 start");
+        c->launches++;
+        if (!rc) rc = c->cuda(cudaMemcpyAsync(&n2, c->sums.as<double>() + 12, sizeof(double), cudaMemcpyDeviceToHost,
+                                              c->stream), "d2h");
+        if (!rc) rc = c->cuda(cudaStreamSynchronize(c->stream), "sync");
+        if (rc) return rc;
+        const double n1 = B.start_norm;
+        if (!(std::fabs(std::sqrt(n2) - n1) <= 1e-12 * n1)) stored = false;
+    }
     DevBuf dptr;   // outlives the final stream synchronisation
     if (stored) {
         // psi = sum_q coef[q] v_{q+1} from the vectors pass 1 kept

@@ -4,12 +4,14 @@
 // All device memory the call needs -- copies of the host inputs, the output
 // and the zero-denominator flag -- lives in one file-scope static device array
 // (kScratchBytes per device, created with the module), cut into 256-byte
-// aligned regions per call.  The array's address is resolved once per device
-// with cudaGetSymbolAddress, with that device current, by the first call made
-// on it; that first call should come before any stream capture.  Every call on
-// a device shares the one array: the flag, which must start at zero, is
-// cleared at the start of each call, and calls whose GPU work overlaps race on
-// the array.  No cudaMalloc, cudaFree or allocating library routine is called.
+// aligned regions per call.  Each call runs with the context's device current
+// (the caller's current device is restored before it returns), so the array,
+// the stream and the copies always belong to one device.  The array's address
+// is resolved once per device with cudaGetSymbolAddress, with that device
+// current, by the first call made on it; that first call should come before
+// any stream capture.  Every call on a device shares the one array: the flag,
+// which must start at zero, is cleared at the start of each call, and calls
+// whose GPU work overlaps race on the array.  No cudaMalloc, cudaFree or allocating library routine is called.
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
@@ -20,6 +22,7 @@
 extern "C" {
 cudaStream_t edk_internal_stream(edk_ctx *ctx);
 int edk_internal_fail(edk_ctx *ctx, int code, const char *msg);
+int edk_internal_ctx_device(const edk_ctx *ctx);
 }
 
 namespace {
@@ -35,13 +38,32 @@ void *g_scratch_ptr[kMaxDevices] = {};
 
 size_t round_up(size_t b) { return (b + kAlign - 1) / kAlign * kAlign; }
 
+// Makes the context's device current for the lifetime of the guard and puts
+// the caller's current device back afterwards.
+struct DeviceGuard {
+    int prev = -1;
+    bool switched = false;
+    cudaError_t enter(int dev)
+    {
+        cudaError_t e = cudaGetDevice(&prev);
+        if (e != cudaSuccess) return e;
+        if (prev == dev) return cudaSuccess;
+        e = cudaSetDevice(dev);
+        switched = e == cudaSuccess;
+        return e;
+    }
+    ~DeviceGuard()
+    {
+        if (switched) cudaSetDevice(prev);
+    }
+};
+
 // Once per device, with that device current: the device address of g_scratch.
-int scratch_of_current_device(edk_ctx *ctx, unsigned char **out)
+int scratch_of_device(edk_ctx *ctx, int dev, unsigned char **out)
 {
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices)
-        return edk_internal_fail(ctx, EDK_ERR_CUDA, "edk_cf_eval_noalloc: no usable current device");
+    if (dev < 0 || dev >= kMaxDevices)
+        return edk_internal_fail(ctx, EDK_ERR_CUDA, "edk_cf_eval_noalloc: device ordinal outside the table");
+    cudaError_t e;
     std::lock_guard<std::mutex> lock(g_setup_mutex);
     if (!g_scratch_ptr[dev]) {
         void *p = nullptr;
@@ -89,8 +111,15 @@ extern "C" int edk_cf_eval_noalloc(edk_ctx *ctx, int32_t nchain, int32_t ld, con
                  nchain, ld, nw, need, kScratchBytes);
         return edk_internal_fail(ctx, EDK_ERR_INVALID, msg);
     }
+    // the context's device, not whichever device the caller left current
+    const int dev = edk_internal_ctx_device(ctx);
+    DeviceGuard guard;
+    if (guard.enter(dev) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return edk_internal_fail(ctx, EDK_ERR_CUDA, "edk_cf_eval_noalloc: cannot make the context's device current");
+    }
     unsigned char *base = nullptr;
-    int rc = scratch_of_current_device(ctx, &base);
+    int rc = scratch_of_device(ctx, dev, &base);
     if (rc) return rc;
     unsigned char *q = base;
     auto take = [&](size_t bytes) { unsigned char *p = q; q += bytes; return p; };

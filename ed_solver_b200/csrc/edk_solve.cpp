@@ -47,6 +47,10 @@ struct DBuf {
 constexpr int64_t kLowprecMinDim = (int64_t)1 << 20;
 // Longest row the batched kernel stages in shared memory (FP64 elements).
 constexpr int64_t kBatchMaxDup = 96 * 1024 / 8;
+// Sectors of at most this many states are diagonalised densely (ED_diago),
+// and with edk_solve_opts.reference_small_sectors their Green functions are
+// Lehmann sums (FULL_ED_SWITCH, Global_Variables.f90:23).
+constexpr int64_t kFullEdSwitch = 40;
 
 struct State {
     int nup, ndn;
@@ -121,8 +125,9 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
     cudaStream_t st = edk_internal_stream(ctx);
     const double demax = o->demax0 / o->beta;
     int rc;
+    const int64_t lowprec_min = o->lowprec_min_dim > 0 ? o->lowprec_min_dim : kLowprecMinDim;
     auto sector_dtype = [&](int64_t dim) {
-        return (o->dtype == EDK_F32 && dim >= kLowprecMinDim) ? EDK_F32 : EDK_F64;
+        return (o->dtype == EDK_F32 && dim >= lowprec_min) ? EDK_F32 : EDK_F64;
     };
 
     // sector Hamiltonians are kept on the context, keyed by the model's bytes and the sector
@@ -217,7 +222,7 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
         edk_h_dims(h, &dim, nullptr, nullptr);
         if (dim == 0) continue;
         std::vector<std::unique_ptr<State>> found;
-        if (dim <= 40) {
+        if (dim <= kFullEdSwitch) {
             // dense H from Hmult__ on unit vectors, FP64
             DBuf ecol((size_t)dim * 8), hcol((size_t)dim * dim * 8);
             std::vector<double> unit(dim, 0.0), Hd((size_t)dim * dim);
@@ -265,6 +270,10 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
             lr.vecp = vecp.data();
             if ((rc = edk_lanczos_e0(h, &lo, &lr))) return rc;
             lanczos_steps += lr.niter;
+            // every state of the sector is formed from pass 1's kept vectors
+            // before any FP64 refinement runs: a refinement is a Lanczos run of
+            // its own, which would release that basis and reuse the pass-1
+            // coefficient buffers
             for (int k = 0; k < lr.nkept; ++k) {
                 auto stt = std::make_unique<State>();
                 stt->nup = nu; stt->ndn = nd; stt->E = lr.E[k]; stt->E_pass1 = lr.E[k]; stt->dtype = sdt;
@@ -274,9 +283,15 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
                 if (lo.keep_basis) lo.keep_basis = k + 1 < lr.nkept ? 2 : 1;
                 if ((rc = edk_lanczos_gs(h, &lo, lr.niter, lr.vecp + (size_t)k * lr.niter, stt->psi.p))) return rc;
                 lanczos_steps += lr.niter;      // the reference's count: pass 2 reruns the recurrence
-                if (sdt == EDK_F32) {
-                    // FP64 refinement restart from the FP32 eigenvector
+                found.push_back(std::move(stt));
+            }
+            if (sdt == EDK_F32) {
+                // FP64 refinement restart from each FP32 eigenvector, with its
+                // own tridiagonal and coefficient buffers
+                std::vector<double> rdiag(cap), rsub(cap), rvecp(cap);
+                for (auto &stt : found) {
                     DBuf p64((size_t)dim * 8);
+                    if (!p64.p) return edk_internal_fail(ctx, EDK_ERR_NOMEM, "refinement vector");
                     if ((rc = edk_convert(ctx, EDK_F32, EDK_F64, dim, stt->psi.p, p64.p))) return rc;
                     edk_lanczos_opts ro = lo;
                     ro.dtype = EDK_F64;
@@ -290,12 +305,13 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
                     ro.keep_basis = o->recompute_pass2 ? 0 : 1;
                     ro.residual_tol = o->residual_tol > 0.0 ? o->residual_tol : 1e-9 * std::max(1.0, std::fabs(stt->E));
                     edk_lanczos_result rr{};
-                    rr.diag = diag.data();
-                    rr.subdiag = sub.data();
-                    rr.vecp = vecp.data();
+                    rr.diag = rdiag.data();
+                    rr.subdiag = rsub.data();
+                    rr.vecp = rvecp.data();
                     if ((rc = edk_lanczos_e0(h, &ro, &rr))) return rc;
                     lanczos_steps += rr.niter;
                     DBuf q64((size_t)dim * 8);
+                    if (!q64.p) return edk_internal_fail(ctx, EDK_ERR_NOMEM, "refinement vector");
                     if ((rc = edk_lanczos_gs(h, &ro, rr.niter, rr.vecp, q64.p))) return rc;
                     lanczos_steps += rr.niter;
                     stt->E = rr.E[0];
@@ -303,7 +319,6 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
                     if ((rc = edk_convert(ctx, EDK_F64, EDK_F32, dim, q64.p, stt->psi.p))) return rc;
                     stt->dtype = EDK_F32;
                 }
-                found.push_back(std::move(stt));
             }
         }
         if (!found.empty()) {
@@ -430,6 +445,23 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
         }
         std::vector<double> raw((size_t)combos.size() * nw * 2);
         std::vector<double> Gc((size_t)2 * nw);
+        // host copies of the window's states in sectors of at most kFullEdSwitch
+        // states (FP64: those sectors are diagonalised densely), for the Lehmann branch
+        std::map<const State *, std::vector<double>> small_psi;
+        auto host_psi = [&](const State *s, int64_t dim, const std::vector<double> **out) -> int {
+            auto it = small_psi.find(s);
+            if (it == small_psi.end()) {
+                std::vector<double> v((size_t)dim);
+                if (s->dtype != EDK_F64) return edk_internal_fail(ctx, EDK_ERR_INVALID, "small sector state not FP64");
+                if (cudaMemcpyAsync(v.data(), s->psi.p, (size_t)dim * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                    cudaStreamSynchronize(st) != cudaSuccess)
+                    return edk_internal_fail(ctx, EDK_ERR_CUDA, "state download");
+                edk_internal_count(ctx, 0, dim * 8);
+                it = small_psi.emplace(s, std::move(v)).first;
+            }
+            *out = &it->second;
+            return EDK_OK;
+        };
         for (int spin = 0; spin < 2; ++spin) {
             if (!((o->spin_mask >> spin) & 1)) continue;
             std::fill(raw.begin(), raw.end(), 0.0);
@@ -468,6 +500,47 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
                     if ((rc = psi_in(gdt, &psi))) return rc;
                     int64_t tdup = 0;
                     edk_h_dims(ht, nullptr, &tdup, nullptr);
+                    if (o->reference_small_sectors && tdim <= kFullEdSwitch) {
+                        // compute_dynamic_full_ed (green_class_compute_dynamic.f90:77-165): with
+                        // phi = A|psi> unnormalised, dyn(iw) = sum over the window's states |n>
+                        // of the target sector of |<n|phi>|^2 / (iw - ph (E_n - E_psi)), and 0
+                        // when |phi|^2 < cutoff_dynamic or no state of that sector is kept
+                        const void *psi64 = nullptr;
+                        if ((rc = psi_in(EDK_F64, &psi64))) return rc;
+                        DBuf phi((size_t)tdim * 8);
+                        std::vector<double> ph((size_t)tdim);
+                        for (size_t q = 0; q < combos.size(); ++q) {
+                            const int i = combos[q].first, j = combos[q].second;
+                            int64_t od = 0;
+                            if ((rc = edk_apply_c(hs_src, EDK_F64, i, spin, iph == 1, i == j ? -1 : j, 1, psi64,
+                                                  phi.p, &od)))
+                                return rc;
+                            if (cudaMemcpyAsync(ph.data(), phi.p, (size_t)tdim * 8, cudaMemcpyDeviceToHost, st) !=
+                                    cudaSuccess ||
+                                cudaStreamSynchronize(st) != cudaSuccess)
+                                return edk_internal_fail(ctx, EDK_ERR_CUDA, "Lehmann branch download");
+                            edk_internal_count(ctx, 0, tdim * 8);
+                            double n2 = 0.0;
+                            for (int64_t t = 0; t < tdim; ++t) n2 += ph[t] * ph[t];
+                            if (n2 < o->cutoff_dynamic) continue;
+                            const double sgn = iph == 1 ? 1.0 : -1.0;
+                            for (auto &n : gs) {
+                                if (n->nup != tnu || n->ndn != tnd) continue;
+                                const std::vector<double> *vn = nullptr;
+                                if ((rc = host_psi(n.get(), tdim, &vn))) return rc;
+                                double ov = 0.0;
+                                for (int64_t t = 0; t < tdim; ++t) ov += (*vn)[t] * ph[t];
+                                const double amp = ov * ov, de = sgn * (n->E - s->E);
+                                for (int w = 0; w < nw; ++w) {
+                                    // amp / (i wn - de)
+                                    const double den = wn[w] * wn[w] + de * de;
+                                    raw[q * 2 * nw + 2 * w] += s->boltz * amp * (-de) / den;
+                                    raw[q * 2 * nw + 2 * w + 1] += s->boltz * amp * (-wn[w]) / den;
+                                }
+                            }
+                        }
+                        continue;
+                    }
                     if (o->green_mode == 0 && gdt == EDK_F64 && tdim < kLowprecMinDim && tdup <= kBatchMaxDup) {
                         for (size_t q = 0; q < combos.size(); ++q) {
                             const int i = combos[q].first, j = combos[q].second;

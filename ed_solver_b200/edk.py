@@ -71,7 +71,8 @@ class _SolveOpts(C.Structure):
                 ("pairs", C.c_void_p), ("cutoff_dynamic", C.c_double), ("ran_tab", C.c_void_p),
                 ("residual_tol", C.c_double), ("green_mode", C.c_int32), ("gs_in", C.c_char_p),
                 ("gs_out", C.c_char_p), ("sector_bound_file", C.c_char_p), ("iwindow", C.c_int32),
-                ("recompute_pass2", C.c_int32)]
+                ("recompute_pass2", C.c_int32), ("reference_small_sectors", C.c_int32),
+                ("lowprec_min_dim", C.c_int64)]
 
 
 class _ChilocSectors(C.Structure):
@@ -191,6 +192,8 @@ def lib():
         "edk_ctx_timing_elements": (C.c_int, [P, C.c_int, P]),
         "edk_ctx_transfer_bytes": (C.c_int, [P, P, P]),
         "edk_ctx_clear_cache": (C.c_int, [P]),
+        "edk_ctx_trim": (C.c_int, [P]),
+        "edk_ctx_set_workspace_limit": (C.c_int, [P, C.c_int64]),
         "edk_ctx_timing_report": (C.c_int, [P, C.c_int, P, P]),
         "edk_h_create": (C.c_int, [P, P, C.c_int, C.c_int, P]),
         "edk_h_destroy": (C.c_int, [P]),
@@ -367,6 +370,14 @@ class Context:
 
     def clear_cache(self):
         self.check(lib().edk_ctx_clear_cache(self.h), "clear_cache")
+
+    def set_workspace_limit(self, nbytes: int):
+        """Caps the Krylov workspace; a pass needing more fails with EDK_ERR_NOMEM (0: no cap)."""
+        self.check(lib().edk_ctx_set_workspace_limit(self.h, int(nbytes)), "set_workspace_limit")
+
+    def trim(self):
+        """Returns the device memory the Krylov-basis pool keeps in reserve."""
+        self.check(lib().edk_ctx_trim(self.h), "trim")
 
     def close(self):
         if getattr(self, "h", None):
@@ -796,10 +807,16 @@ def sector_bounds_write(path: str, nup, ndn, sz=(1000, -1000)):
 def solve(ctx: Context, model: AIMModel, sectors, beta: float, nw: int, dtype="f64", neigen=1,
           nitermax=1000, tolerance=1e-12, tolerance_lowprec=1e-6, demax0=5.0, nitergreen=200,
           spins=(0, 1), pairs=None, cutoff_dynamic=1e-8, check_every=8, ran_tab=None, residual_tol=0.0,
-          green_mode=0, gs_in=None, gs_out=None, sector_bound_file=None, iwindow=1, recompute_pass2=False):
+          green_mode=0, gs_in=None, gs_out=None, sector_bound_file=None, iwindow=1, recompute_pass2=False,
+          reference_small_sectors=False, lowprec_min_dim=0):
     """One impurity solve through the C-ABI (edk_solve): host inputs, host outputs.
     recompute_pass2: rerun the Lanczos recurrence in pass 2 (the reference's way)
     instead of forming the eigenvectors from the Krylov vectors pass 1 kept.
+    reference_small_sectors: target sectors of at most 40 states take the
+    reference's Lehmann sum over the eigenstates kept in the window
+    (compute_dynamic_full_ed) instead of an exact continued fraction.
+    lowprec_min_dim: in mixed precision, the smallest sector that runs FP32
+    vectors (0: 2^20).
 
     Returns dict(e0, z, residual, nstates, lanczos_steps, green_steps, G (2, npairs, nw) complex,
     docc (nc,), energies, sectors, e0_lowprec).
@@ -816,7 +833,7 @@ def solve(ctx: Context, model: AIMModel, sectors, beta: float, nw: int, dtype="f
                    None if tab is None else tab.ctypes.data, float(residual_tol), int(green_mode),
                    None if gs_in is None else gs_in.encode(), None if gs_out is None else gs_out.encode(),
                    None if sector_bound_file is None else sector_bound_file.encode(), int(iwindow),
-                   1 if recompute_pass2 else 0)
+                   1 if recompute_pass2 else 0, 1 if reference_small_sectors else 0, int(lowprec_min_dim))
     G = np.zeros((2, len(pr) // 2, nw, 2))
     docc = np.zeros(model.nc)
     en = np.zeros(64)

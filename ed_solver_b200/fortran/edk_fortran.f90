@@ -109,7 +109,8 @@ module edk_fortran
     real(c_double) :: residual_tol
     integer(c_int32_t) :: green_mode
     type(c_ptr) :: gs_in, gs_out, sector_bound_file
-    integer(c_int32_t) :: iwindow, recompute_pass2
+    integer(c_int32_t) :: iwindow, recompute_pass2, reference_small_sectors
+    integer(c_int64_t) :: lowprec_min_dim
   end type
 
   type, bind(C) :: edk_solve_result
@@ -368,6 +369,15 @@ module edk_fortran
     integer(c_int) function edk_ctx_clear_cache(ctx) bind(C, name="edk_ctx_clear_cache")
       import :: c_int, c_ptr
       type(c_ptr), value :: ctx
+    end function
+    integer(c_int) function edk_ctx_trim(ctx) bind(C, name="edk_ctx_trim")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+    end function
+    integer(c_int) function edk_ctx_set_workspace_limit(ctx, bytes) bind(C, name="edk_ctx_set_workspace_limit")
+      import :: c_int, c_ptr, c_int64_t
+      type(c_ptr), value :: ctx
+      integer(c_int64_t), value :: bytes
     end function
 
     ! ---- basis and tables (host-only) ----

@@ -36,7 +36,8 @@ extern "C" {
 #define EDK_ERR_CF_ZERO_DEN    6   /* zero denominator in the continued fraction
                                       (matrices_tridiag.f90:176-190) */
 #define EDK_ERR_TIMEOUT        7   /* a bounded device-side wait gave up */
-#define EDK_ERR_NOT_FINITE     8   /* NaN/Inf met in a Krylov coefficient */
+#define EDK_ERR_NOT_FINITE     8   /* NaN/Inf met in a Krylov coefficient or in the
+                                      start vector */
 #define EDK_ERR_UNSUPPORTED    9
 
 /* ---- element types ----------------------------------------------------- */
@@ -98,6 +99,17 @@ int edk_ctx_transfer_bytes(const edk_ctx *ctx, int64_t *h2d, int64_t *d2h);
 /* Destroys the sector Hamiltonians edk_solve keeps on the context between
  * calls (they are reused when the same model and sector come back). */
 int edk_ctx_clear_cache(edk_ctx *ctx);
+/* Hands the device memory that the context's Krylov-basis pool keeps in
+ * reserve (released bases, up to 5/8 of the device) back to the driver, so
+ * that other allocators can use it.  The next pass that keeps its basis maps
+ * memory again.  Nothing else is freed. */
+int edk_ctx_trim(edk_ctx *ctx);
+/* Caps the Krylov workspace (five vectors of the sector's size per element
+ * type, shared by the context's passes): a pass that would need more than
+ * `bytes` returns EDK_ERR_NOMEM before allocating; 0 removes the cap.  Where
+ * the reference would die in an allocation, a caller with a memory budget
+ * gets a status instead. */
+int edk_ctx_set_workspace_limit(edk_ctx *ctx, int64_t bytes);
 
 /* ---- basis (quantum_fermion_hilbert_class.f90:346-421) ----------------- */
 int64_t edk_binom(int n, int k);
@@ -167,7 +179,11 @@ typedef struct edk_lanczos_opts {
                                     them for another eigenvector of the same chain.  The next pass
                                     1 and edk_h_destroy release them too.  0: pass 2 recomputes
                                     (the reference's way).  edk_solve sets it unless
-                                    edk_solve_opts.recompute_pass2 is set. */
+                                    edk_solve_opts.recompute_pass2 is set.  The start buffer (or
+                                    the ran_tab array) must hold the same values in pass 2 as in
+                                    pass 1: pass 2 compares the norm of start_dev and a sum of
+                                    ran_tab with pass 1's and recomputes when they differ, which
+                                    catches most but not all changes. */
 } edk_lanczos_opts;
 
 typedef struct edk_lanczos_result {
@@ -229,7 +245,8 @@ int edk_cf_eval(edk_ctx *ctx, int32_t nchain, int32_t ld, const int32_t *n_host,
  * text.  The first call on a device resolves the array's address
  * (cudaGetSymbolAddress, that device current); make it before any stream
  * capture.  All calls on a device share the array and clear its flag first:
- * calls whose GPU work overlaps race.  The context's device must be current. */
+ * calls whose GPU work overlaps race.  The call runs with the context's device
+ * current and puts the caller's current device back before it returns. */
 #define EDK_NOALLOC_SCRATCH_BYTES 4194304
 int edk_cf_eval_noalloc(edk_ctx *ctx, int32_t nchain, int32_t ld, const int32_t *n_host,
                         const double *diag_host, const double *subdiag_host, const double *e_host,
@@ -399,6 +416,14 @@ typedef struct edk_solve_opts {
                                     (edk_lanczos_opts.keep_basis) and pass 2 forms the eigenvector
                                     from them; 1: pass 2 reruns the recurrence (the reference's
                                     Lanczos_get_GS_sector) */
+    int32_t reference_small_sectors;  /* 1: Green functions into target sectors of at most 40
+                                    states (FULL_ED_SWITCH) take the reference's Lehmann branch
+                                    (compute_dynamic_full_ed, green_class_compute_dynamic.f90:44-62,
+                                    77-165): a sum over the eigenstates of that sector kept in the
+                                    Boltzmann window, 0 when none is kept.  0: the continued
+                                    fraction of min(nitergreen, dim) steps, exact for the sector */
+    int64_t lowprec_min_dim;     /* mixed precision: sectors of at least this many states run
+                                    FP32 Krylov vectors; 0 means 2^20 */
 } edk_solve_opts;
 
 typedef struct edk_solve_result {

@@ -664,13 +664,37 @@ def ground_states(model: AIMModel, sectors: Sequence[Tuple[int, int]], beta: flo
     return gs, e0, z
 
 
+def lehmann_small_sector(gs, tsec, v: np.ndarray, e_psi: float, iph: int, wn: np.ndarray,
+                         cutoff_dynamic=1e-8) -> np.ndarray:
+    """compute_dynamic_full_ed (ed_solver/green_class_compute_dynamic.f90:77-165),
+    the branch compute_dynamic takes for target sectors of at most FULL_ED_SWITCH
+    states (:44-62): with v = A|psi> unnormalised, the sum over the states |n> of
+    the target sector that the window kept of |<n|v>|^2 / (i w - ph (E_n - E_psi))
+    (:150-154, fermionic sign -1); zero when |v|^2 < cutoff_dynamic (:116-122) or
+    when no state of that sector is kept (iisector == 0, :143)."""
+    out = np.zeros(len(wn), complex)
+    if float(v @ v) < cutoff_dynamic:
+        return out
+    ph = 1.0 if iph == 1 else -1.0
+    for n in gs:
+        if tuple(n["sector"]) != tuple(tsec):
+            continue
+        amp = float(n["psi"] @ v) ** 2
+        out += amp / (1j * wn - ph * (n["E"] - e_psi))
+    return out
+
+
 def green_impurity(model: AIMModel, gs, beta: float, nw: int, nitergreen: int, spin: int = 0,
-                   pairs: Optional[Sequence[Tuple[int, int]]] = None, cutoff_dynamic=1e-8):
+                   pairs: Optional[Sequence[Tuple[int, int]]] = None, cutoff_dynamic=1e-8,
+                   reference_small_sectors: bool = False):
     """G_ij(i w_n) for impurity orbitals of one spin, the (c, c+) channel of compute_greenAA.
 
     For each state |psi> with weight boltz: particle part with |phi> = (c+_i [+ c+_j])|psi>,
     hole part with (c_i [+ c_j])|psi> (real-H symmetric combination), then
     G_ij = (G_{i+j} - G_ii - G_jj) / 2 for i != j.  Returns dict {(i,j): array(nw)}.
+    reference_small_sectors: target sectors of at most FULL_ED_SWITCH states take
+    the Lehmann branch (lehmann_small_sector) as the reference does; otherwise
+    every target sector runs the continued fraction.
     """
     nc = model.nc
     if pairs is None:
@@ -696,8 +720,11 @@ def green_impurity(model: AIMModel, gs, beta: float, nw: int, nitergreen: int, s
                     v = vi
                 if tsec not in hcache:
                     hcache[tsec] = OracleH(model, *tsec)
-                G, _, _ = green_chain(hcache[tsec], v, nitergreen, st["E"], iph, wn,
-                                      cutoff_dynamic=cutoff_dynamic)
+                if reference_small_sectors and hcache[tsec].dim <= FULL_ED_SWITCH:
+                    G = lehmann_small_sector(gs, tsec, v, st["E"], iph, wn, cutoff_dynamic)
+                else:
+                    G, _, _ = green_chain(hcache[tsec], v, nitergreen, st["E"], iph, wn,
+                                          cutoff_dynamic=cutoff_dynamic)
                 raw[(i, j)] += st["boltz"] * G
     out = {}
     for (i, j) in pairs:

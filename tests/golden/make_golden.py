@@ -16,7 +16,7 @@ import sys
 
 import numpy as np
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ED_SOLVER_REF", "/root/reference")
 g = np.loadtxt(os.path.join(ref, "test", "2b", "bm", "g_bm"))
 beta = 50.0
 n = 200

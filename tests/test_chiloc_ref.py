@@ -8,7 +8,7 @@ import pytest
 import oracle as O
 from ed_solver_b200.model import star_model
 
-REF_SRC = "/root/reference/ed_solver/Chiloc_Wenhu_version3.cpp"
+REF_SRC = os.path.join(os.environ.get("ED_SOLVER_REF", "/root/reference"), "ed_solver", "Chiloc_Wenhu_version3.cpp")
 
 
 def _need_ref():

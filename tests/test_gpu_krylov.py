@@ -153,8 +153,8 @@ def test_reference_golden_through_the_device(ctx):
     assert np.abs(G[(1, 1)] - (g[:, 3] + 1j * g[:, 4])).max() < 2e-8
 
 
-def test_pipelined_kernel_krylov_ns14_against_oracle(ctx):
-    """The ns=14 (7,7) sector (1.18e7 states) runs on the pipelined row kernel:
+def test_fast_row_kernel_krylov_ns14_against_oracle(ctx):
+    """The ns=14 (7,7) sector (1.18e7 states) runs on the fast row kernel:
     Lanczos coefficients, the pass-2 vector (accumulated inside the fused step),
     the c+ map and a Green chain in FP64 against the oracle (1e-9); the FP32
     chain against the FP64 one (1e-5)."""

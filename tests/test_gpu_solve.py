@@ -151,3 +151,87 @@ def test_sector_bound_file_restricts_the_scan(ctx, tmp_path):
     assert b[0] == (min(s[0] for s in kept), max(s[0] for s in kept))
     assert b[1] == (min(s[1] for s in kept), max(s[1] for s in kept))
     assert all(abs(s[0] - nu) <= 1 and abs(s[1] - nd) <= 1 for s in kept)
+
+
+def _model_2b():
+    return star_model(-5.0, 10.0, [0.0, 0.0], [math.sqrt(0.2), math.sqrt(0.3)], orbital_of_bath=[0, 1], nc=2,
+                      Uprime=2.0, J=0.0, cutoff=1e-8)
+
+
+def test_solve_reference_small_sectors_reproduce_g_bm(ctx):
+    """reference_small_sectors on the test/2b deck, where every sector has at
+    most 36 states and the reference's own run took the Lehmann branch with
+    every eigenstate kept (dEmax0=10000, Neigen=500): G11 and G22 of g_bm."""
+    g = np.loadtxt(os.path.join(os.path.dirname(__file__), "golden", "g_bm_2b.txt"))
+    secs = [(a, b) for a in range(5) for b in range(5)]
+    r = edk.solve(ctx, _model_2b(), secs, 50.0, len(g), dtype="f64", neigen=500, tolerance=1e-13, demax0=10000.0,
+                  nitergreen=400, spins=(0,), pairs=[(0, 0), (1, 1)], reference_small_sectors=True)
+    assert r["nstates"] == 256
+    assert np.abs(r["G"][0, 0] - (g[:, 1] + 1j * g[:, 2])).max() < 2e-8
+    assert np.abs(r["G"][0, 1] - (g[:, 3] + 1j * g[:, 4])).max() < 2e-8
+
+
+def test_solve_reference_small_sectors_narrow_window_against_oracle(ctx):
+    """A narrow window (dEmax = 0.5): the Lehmann branch keeps only the target
+    states in the window, so G differs from the exact continued fraction; the
+    device solve equals the oracle's restatement of the branch (1e-10)."""
+    m = _model_2b()
+    secs = [(a, b) for a in range(5) for b in range(5)]
+    kw = dict(neigen=40, tolerance=1e-13, demax0=25.0, nitergreen=400, spins=(0, 1), pairs=[(0, 0), (1, 1), (0, 1)])
+    r = edk.solve(ctx, m, secs, 50.0, 128, dtype="f64", reference_small_sectors=True, **kw)
+    rc = edk.solve(ctx, m, secs, 50.0, 128, dtype="f64", **kw)
+    gs, e0, z = O.ground_states(m, secs, 50.0, 25.0, neigen=40, tolerance=1e-13)
+    for spin in (0, 1):
+        Go = O.green_impurity(m, gs, 50.0, 128, 400, spin=spin, pairs=[(0, 0), (1, 1), (0, 1)],
+                              reference_small_sectors=True)
+        for p, key in enumerate([(0, 0), (1, 1), (0, 1)]):
+            assert np.abs(r["G"][spin, p] - Go[key]).max() < 1e-10
+    assert np.abs(r["G"] - rc["G"]).max() > 1e-3
+
+
+def test_mixed_precision_c2_all_sectors_fp32(ctx):
+    """C2 (ns=10 Kanamori, 121 sectors, 512 points at beta=40) with FP32
+    Krylov vectors in every sector of at least 1000 states (lowprec_min_dim),
+    against the FP64 solve: |dE0/E0| <= 1e-8, |d docc| <= 1e-7 and
+    max|dG| <= 1e-6."""
+    w = workload("c2")
+    kw = dict(nitergreen=w.nitergreen, spins=(0, 1), pairs=[(0, 0), (1, 1), (0, 1)], tolerance=1e-12,
+              residual_tol=1e-10, demax0=w.demax0)
+    r64 = edk.solve(ctx, w.model, w.sectors, w.beta, 512, dtype="f64", **kw)
+    r32 = edk.solve(ctx, w.model, w.sectors, w.beta, 512, dtype="f32", lowprec_min_dim=1000, **kw)
+    de = abs(r32["e0"] - r64["e0"]) / abs(r64["e0"])
+    dd = np.abs(r32["docc"] - r64["docc"]).max()
+    dg = np.abs(r32["G"] - r64["G"]).max()
+    print(f"C2 mixed vs FP64: |dE0/E0| = {de:.3e}, |d docc| = {dd:.3e}, max|dG| = {dg:.3e}")
+    assert r32["e0_lowprec"] != r32["e0"]          # FP32 passes ran and were refined
+    assert de <= 1e-8 and dd <= 1e-7 and dg <= 1e-6
+
+
+def test_mixed_precision_two_states_per_sector(ctx):
+    """Mixed precision with neigen = 2 and a short pass 1: every FP32 state of
+    the sector is formed before any FP64 refinement, and each refinement has
+    its own coefficient buffers, so both states match the FP64 solve."""
+    w = workload("c1")
+    kw = dict(nitergreen=100, spins=(0,), tolerance=1e-12, residual_tol=1e-10, neigen=2, demax0=100.0,
+              nitermax=120, tolerance_lowprec=1e-5)
+    r64 = edk.solve(ctx, w.model, w.sectors, w.beta, 64, dtype="f64", **kw)
+    r32 = edk.solve(ctx, w.model, w.sectors, w.beta, 64, dtype="f32", lowprec_min_dim=1000, **kw)
+    assert r64["nstates"] == 2 and r32["nstates"] == 2
+    assert np.abs(r32["energies"] - r64["energies"]).max() <= 1e-8 * abs(r64["e0"])
+    assert np.abs(r32["G"] - r64["G"]).max() <= 1e-6
+
+
+def test_c1_as_specified(ctx):
+    """C1 as the configuration states it: ground state to |H psi - E psi| < 1e-12
+    (Ritz residual), then G(i w_n) at 1024 Matsubara points, beta = 50, from
+    200-step continued fractions, against the oracle driver."""
+    w = workload("c1")
+    m = w.model
+    r = edk.solve(ctx, m, w.sectors, w.beta, 1024, dtype="f64", nitergreen=200, spins=(0, 1), tolerance=1e-14,
+                  residual_tol=1e-12)
+    assert r["residual"] < 1e-11
+    gso, e0o, zo = O.ground_states(m, w.sectors, w.beta, w.demax0, tolerance=1e-14)
+    assert abs(r["e0"] - e0o) < 1e-12 * abs(e0o)
+    for spin in (0, 1):
+        Go = O.green_impurity(m, gso, w.beta, 1024, 200, spin=spin)[(0, 0)]
+        assert np.abs(r["G"][spin, 0] - Go).max() < 1e-8

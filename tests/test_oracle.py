@@ -92,6 +92,45 @@ def test_reference_golden_g_bm():
     assert np.abs(G[(0, 1)]).max() < 1e-12
 
 
+def _model_2b():
+    return star_model(-5.0, 10.0, [0.0, 0.0], [math.sqrt(0.2), math.sqrt(0.3)], orbital_of_bath=[0, 1], nc=2,
+                      Uprime=2.0, J=0.0, cutoff=1e-8)
+
+
+def test_reference_golden_g_bm_through_the_lehmann_branch():
+    """Every sector of the test/2b model has at most 36 states, so the
+    reference took compute_dynamic_full_ed there.  Its vertex-dump run keeps
+    every eigenstate (dEmax0=10000, Neigen=500, test/2b/test.py:200), where the
+    Lehmann sum is exact: the oracle's restatement of that branch reproduces
+    G11 and G22."""
+    g = np.loadtxt(GOLDEN)
+    m = _model_2b()
+    secs = [(a, b) for a in range(5) for b in range(5)]
+    gs, e0, z = O.ground_states(m, secs, 50.0, 10000.0, neigen=500, tolerance=1e-13)
+    assert len(gs) == 256
+    G = O.green_impurity(m, gs, 50.0, len(g), 400, pairs=[(0, 0), (1, 1), (0, 1)],
+                         reference_small_sectors=True)
+    assert np.abs(G[(0, 0)] - (g[:, 1] + 1j * g[:, 2])).max() < 2e-8
+    assert np.abs(G[(1, 1)] - (g[:, 3] + 1j * g[:, 4])).max() < 2e-8
+
+
+def test_lehmann_branch_differs_from_the_continued_fraction_in_a_narrow_window():
+    """With a narrow window (dEmax = 0.5) the Lehmann branch sums only the
+    target-sector states the window kept, so it is not the exact G the
+    continued fraction gives; zero when no target state is kept."""
+    m = _model_2b()
+    secs = [(a, b) for a in range(5) for b in range(5)]
+    gs, e0, z = O.ground_states(m, secs, 50.0, 25.0, neigen=40, tolerance=1e-13)
+    Gl = O.green_impurity(m, gs, 50.0, 64, 400, reference_small_sectors=True)[(0, 0)]
+    Gc = O.green_impurity(m, gs, 50.0, 64, 400)[(0, 0)]
+    assert np.abs(Gl - Gc).max() > 1e-3
+    kept = {tuple(s["sector"]) for s in gs}
+    wn = matsubara(50.0, 8)
+    v, tsec = O.apply_c(m, *gs[0]["sector"], 0, 0, True, gs[0]["psi"])
+    Gs = O.lehmann_small_sector(gs, tsec, v, gs[0]["E"], 1, wn)
+    assert (tsec in kept) or np.all(Gs == 0)
+
+
 def test_apply_c_is_a_signed_partial_permutation():
     m = _models()[1]
     rng = np.random.default_rng(2)

@@ -62,6 +62,31 @@ def test_noalloc_matches_cf_eval_on_consecutive_calls(nctx):
         assert np.abs(G - G_ref).max() <= TOL * max(1.0, np.abs(G_ref).max())
 
 
+def test_noalloc_allocates_nothing(nctx):
+    """The device's free memory, torch's allocator counters and the current
+    device are the same before and after a call (after a first call has
+    resolved the array's address)."""
+    import torch
+    args = _chains(11, 16, 400)
+    wn = matsubara(25.0, 256)
+    rc0, G0 = _call("edk_cf_eval_noalloc", nctx, *args, wn)
+    assert rc0 == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    stats0 = {k: v for k, v in torch.cuda.memory_stats(0).items() if k.endswith(".allocated") or "segment" in k}
+    dev0 = torch.cuda.current_device()
+    for _ in range(3):
+        rc, G = _call("edk_cf_eval_noalloc", nctx, *args, wn)
+        assert rc == 0
+        assert np.array_equal(G, G0)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    stats1 = {k: v for k, v in torch.cuda.memory_stats(0).items() if k.endswith(".allocated") or "segment" in k}
+    assert free1 == free0
+    assert stats1 == stats0
+    assert torch.cuda.current_device() == dev0
+
+
 def test_noalloc_flag_cleared_between_calls(nctx):
     # a zero denominator sets the flag; the next call starts from a cleared flag
     n = np.array([1], np.int32)
