@@ -32,7 +32,7 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = dict(name="ns16_halffilled_E0_G512", nc=1, nb=15, sector=(8, 8), beta=50.0, nw=512,
                 nitergreen=300, nitermax=1000, tolerance=1e-12, tolerance_lowprec=1e-6,
-                residual_tol=1e-9, spins=(0, 1), pairs=[(0, 0)], demax0=5.0)
+                residual_tol=1e-9, spins=(0, 1), pairs=[(0, 0)], demax0=5.0, fp32_sums=True)
 # H*v applications of one plain FP64 solve of this workload (eigen part + Green part),
 # measured on B200 with the library's start-vector table; used to convert a
 # per-step CPU time into solves/s for the reference arm.
@@ -133,7 +133,36 @@ def _solve(ctx, model, dtype):
     return edk.solve(ctx, model, [w["sector"]], w["beta"], w["nw"], dtype=dtype, neigen=1,
                      nitermax=w["nitermax"], tolerance=w["tolerance"], tolerance_lowprec=w["tolerance_lowprec"],
                      demax0=w["demax0"], nitergreen=w["nitergreen"], spins=w["spins"], pairs=w["pairs"],
-                     residual_tol=w["residual_tol"])
+                     residual_tol=w["residual_tol"], fp32_sums=w["fp32_sums"] and dtype == "f32")
+
+
+def _hv_time(ctx, model, peak, reps=10):
+    """Plain H*v (FP32 in, FP32 out) of the headline sector: mean CUDA-event time
+    of `reps` launches inside the library, algorithmic bytes 2 D 4 B (read x,
+    write y; tables below 0.2 %)."""
+    import torch
+    from ed_solver_b200 import edk
+    h = edk.Hamiltonian(ctx, model, *WORKLOAD["sector"])
+    x = torch.randn(h.dim, dtype=torch.float32, device=f"cuda:{ctx.device}")
+    y = torch.empty_like(x)
+    ctx.set_fp32_sums(WORKLOAD["fp32_sums"])
+    h.hmult(x, out=y)                                 # launch shape timed here
+    h.hmult(x, out=y)
+    torch.cuda.synchronize()
+    ctx.timing(False)
+    ctx.timing(True)
+    for _ in range(reps):
+        h.hmult(x, out=y)
+    torch.cuda.synchronize()
+    n, ms, el = ctx.timing_report(4)
+    ctx.timing(False)
+    ctx.set_fp32_sums(False)
+    t = ms / max(n, 1)
+    gbs = 2.0 * 4.0 * h.dim / (t * 1e-3) / 1e9
+    del x, y
+    h.close()
+    return {"ms_per_hv": t, "achieved_gbs": gbs, "frac": gbs / peak, "launches": n,
+            "fp32_sums": WORKLOAD["fp32_sums"], "algorithmic_bytes": 8.0 * h.dim}
 
 
 def _cpu_step_time(model, nsteps=2):
@@ -224,15 +253,19 @@ def run_ours(args):
         step_bytes = 3.0 * 4.0 * e6                      # read v_k, read v_{k-1}, write w per element (FP32)
         achieved = step_bytes / (t6 * 1e-3) / 1e9 if t6 > 0 else None
         traffic = _traffic_per_launch()
-        # ---- plain FP64 solve: accuracy reference and speed-up ----
+        # ---- plain FP64 solves: accuracy reference and speed-up (same clock, up to 5 solves) ----
         torch.cuda.synchronize()
         e_a, e_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         _solve(ctx, model, "f64")                        # builds FP64 workspace
+        n64 = max(1, min(5, args.steps))
         e_a.record(stream)
-        r64 = _solve(ctx, model, "f64")
+        r64s = [_solve(ctx, model, "f64") for _ in range(n64)]
         e_b.record(stream)
         torch.cuda.synchronize()
-        t64 = e_a.elapsed_time(e_b) * 1e-3
+        r64 = r64s[-1]
+        t64 = e_a.elapsed_time(e_b) * 1e-3 / n64
+        # ---- plain H*v of the (8,8) sector, FP32 (the metric's first half) ----
+        hv = _hv_time(ctx, model, peak)
         steps64 = r64["lanczos_steps"] + r64["green_steps"]
         dG = float(np.abs(res["G"] - r64["G"]).max())
         dE = abs(res["e0"] - r64["e0"]) / abs(r64["e0"])
@@ -272,7 +305,8 @@ def run_ours(args):
                     "h2d_bytes_per_step": (h2d1 - h2d0) // ne2e, "d2h_bytes_per_step": (d2h1 - d2h0) // ne2e},
             "gpu_launches": launches,
             "clocks": clocks,
-            "fp64": {"solve_s": t64, "solves_per_s": 1.0 / t64, "hv_steps": steps64},
+            "fp64": {"solve_s": t64, "solves_per_s": 1.0 / t64, "hv_steps": steps64, "solves_timed": n64},
+            "hv": hv,
             "speedup_mixed_vs_fp64": t64 / (t_max * 1e-3 / args.steps),
             "accuracy_vs_fp64": {"rel_dE0": dE, "max_abs_dG": dG, "residual": res["residual"],
                                  "docc": float(res["docc"][0]), "docc_fp64": float(r64["docc"][0])},
@@ -291,10 +325,15 @@ def run_kernel_case(args):
     from ed_solver_b200 import edk
     ctx = edk.Context(0)
     h = edk.Hamiltonian(ctx, _model(), *WORKLOAD["sector"])
-    ctx.set_kernel_path(16)      # the first feasible launch shape, no per-sector timing launches
+    # one fixed launch shape (--kernel-shape, an index into the sector's list), no timing launches
+    shapes = h.launch_shapes("f32")
+    ctx.set_kernel_path(16 + args.kernel_shape)
+    ctx.set_fp32_sums(args.fp32_sums)
     r = h.lanczos_e0(dtype="f32", nitermax=6, tolerance=0.0, check_every=6)
     torch.cuda.synchronize()
-    print(json.dumps({"kernel_case": "ns16 (8,8) FP32 Lanczos", "dim": h.dim, "niter": r["niter"]}), flush=True)
+    print(json.dumps({"kernel_case": "ns16 (8,8) FP32 Lanczos", "dim": h.dim, "niter": r["niter"],
+                      "shape": shapes[args.kernel_shape % len(shapes)], "fp32_sums": bool(args.fp32_sums)}),
+          flush=True)
     h.close()
     ctx.close()
 
@@ -565,6 +604,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--kernel-case", action="store_true",
                     help="run only six FP32 Lanczos steps of the (8,8) sector (profiling case)")
+    ap.add_argument("--kernel-shape", type=int, default=0,
+                    help="launch shape of the --kernel-case (index into the sector's feasible shapes)")
+    ap.add_argument("--fp32-sums", action="store_true",
+                    help="sum the hop terms of H*v in FP32 in the FP32 passes of large sectors")
     ap.add_argument("--grad", action="store_true",
                     help="time the 32 parameter gradients of E0 + G and check them by central differences")
     ap.add_argument("--grad-fd", type=int, default=4, help="parameters checked by central differences (--grad)")

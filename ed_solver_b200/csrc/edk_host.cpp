@@ -99,6 +99,8 @@ struct edk_ctx {
     double *pin_tri = nullptr;
     size_t pin_cap = 0;
     cudaEvent_t pin_ev = nullptr;
+    int fp32_sums = 0;       // FP32 vectors: sum the hop terms in FP32 (edk_ctx_set_fp32_sums)
+    int64_t fp32_sums_min_dim = (int64_t)1 << 20;
     int kernel_path = 0;     // 0 = fastest applicable row kernel, 1 = generic row kernel only,
                              // 2/3 = the fast kernel where applicable
     // optional event timing of row-kernel launches: (class, start, stop)
@@ -320,8 +322,9 @@ struct edk_h {
     };
     std::vector<std::unique_ptr<CMap>> cmaps;
     // fast-kernel launch shape per element type, chosen by timing on first use
-    FastShape fast_shape[2];
-    bool fast_tuned[2] = {false, false};
+    // (index: element type + 2 * FP32 hop sums)
+    FastShape fast_shape[4];
+    bool fast_tuned[4] = {false, false, false, false};
     // Nambu (Sz) sector: its tables replace the (N_up, N_dn) ones
     SzHost *sz = nullptr;
     int npart = -1;
@@ -432,34 +435,48 @@ RowArgs base_args(edk_h *h)
 // first call with an output vector, every feasible shape is timed (two H*v
 // launches each, the first as warm-up) writing into that vector, which the
 // real launch then overwrites; the fastest is kept on the Hamiltonian.
-int fast_shape_for(edk_h *h, int dtype, const RowArgs &a, FastShape &out)
+constexpr int kMaxShapes = 32;
+
+// aligned: every vector of the call is aligned to twice the element size,
+// which the register-staged kernel (kind 0) needs; without it only the
+// bulk-copy kernel (kind 1) is a candidate, taken untimed and not remembered.
+int fast_shape_for(edk_h *h, int dtype, const RowArgs &a, bool aligned, FastShape &out)
 {
     edk_ctx *c = h->ctx;
     const int eb = dtype == EDK_F64 ? 8 : 4;
-    FastShape cand[12];
+    FastShape cand[kMaxShapes];
+    const int slot = dtype + 2 * a.sum32;
     if (c->kernel_path >= 16) {
         // a fixed candidate, for measurements
-        const int n = fast_shapes(h->H, eb, c->num_sms, cand, 12);
+        const int n = fast_shapes(h->H, eb, c->num_sms, cand, kMaxShapes);
         if (n == 0) return c->fail(EDK_ERR_INVALID, "fast row kernel: no launch shape");
         out = cand[(c->kernel_path - 16) % n];
         return EDK_OK;
     }
-    if (h->fast_tuned[dtype]) { out = h->fast_shape[dtype]; return EDK_OK; }
+    if (h->fast_tuned[slot]) { out = h->fast_shape[slot]; return EDK_OK; }
+    if (!aligned) {
+        const int n = fast_shapes(h->H, eb, c->num_sms, cand, kMaxShapes);
+        for (int i = 0; i < n; ++i)
+            if (!shape_needs_pairs(cand[i].kind)) { out = cand[i]; return EDK_OK; }
+        if (n == 0) return c->fail(EDK_ERR_INVALID, "fast row kernel: no launch shape");
+        out = cand[0];
+        return EDK_OK;
+    }
     char key[160];
-    std::snprintf(key, sizeof key, "%d:%lld:%lld:%d:%d:%d", dtype, (long long)h->H.dup, (long long)h->H.ddn,
-                  h->H.up.ell_k, h->H.dn_kmax, h->H.nc);
+    std::snprintf(key, sizeof key, "%d:%lld:%lld:%d:%d:%d:%d", dtype, (long long)h->H.dup, (long long)h->H.ddn,
+                  h->H.up.ell_k, h->H.dn_kmax, h->H.nc, a.sum32);
     if (c->kernel_path == 0)
         for (const auto &kv : c->fast_by_shape)
             if (kv.first == key) {
-                out = h->fast_shape[dtype] = kv.second;
-                h->fast_tuned[dtype] = true;
+                out = h->fast_shape[slot] = kv.second;
+                h->fast_tuned[slot] = true;
                 return EDK_OK;
             }
-    const int n = fast_shapes(h->H, eb, c->num_sms, cand, 12);
+    const int n = fast_shapes(h->H, eb, c->num_sms, cand, kMaxShapes);
     if (n == 0) return c->fail(EDK_ERR_INVALID, "fast row kernel: no launch shape");
     out = cand[0];
     if (c->kernel_path != 0 || n == 1 || !a.x || !a.y) {
-        if (n == 1 || c->kernel_path != 0) { h->fast_shape[dtype] = out; h->fast_tuned[dtype] = true; }
+        if (n == 1 || c->kernel_path != 0) { h->fast_shape[slot] = out; h->fast_tuned[slot] = true; }
         return EDK_OK;
     }
     RowArgs t = a;
@@ -481,16 +498,19 @@ int fast_shape_for(edk_h *h, int dtype, const RowArgs &a, FastShape &out)
     c->event_pool.push_back(eb_);
     int rc = c->cuda(cudaGetLastError(), "fast row kernel autotune");
     if (rc) return rc;
-    h->fast_shape[dtype] = out;
-    h->fast_tuned[dtype] = true;
+    h->fast_shape[slot] = out;
+    h->fast_tuned[slot] = true;
     c->fast_by_shape.push_back({key, out});
     return EDK_OK;
 }
 
-int rows(edk_h *h, int dtype, const RowArgs &a)
+int rows(edk_h *h, int dtype, const RowArgs &a_in)
 {
     edk_ctx *c = h->ctx;
     const int eb = dtype == EDK_F64 ? 8 : 4;
+    RowArgs a = a_in;
+    // FP32 hop sums where the context allows them (FP32 vectors of large sectors)
+    a.sum32 = dtype == EDK_F32 && c->fp32_sums && h->dim >= c->fp32_sums_min_dim && !h->sz ? 1 : 0;
     LaunchCfg cfg;
     if (!h->sz) {
         cfg = plan_rows(h->H, eb, c->num_sms);
@@ -498,10 +518,14 @@ int rows(edk_h *h, int dtype, const RowArgs &a)
         // aligned to twice the element size
         auto al = [&](const void *p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) % (2 * eb)) == 0; };
         const bool aligned = al(a.x) && al(a.y) && al(a.vk) && al(a.vkm1) && al(a.vout) && al(a.psi);
-        cfg.fast = c->kernel_path != 1 && aligned && fast_rows_ok(h->H, eb);
+        // kinds 0, 2 and 3 need those aligned column pairs; kinds 1 and 4 read
+        // single elements at any alignment
+        FastShape any[kMaxShapes];
+        cfg.fast = c->kernel_path != 1 && fast_rows_ok(h->H, eb) && fast_shapes(h->H, eb, c->num_sms, any, kMaxShapes) > 0;
         if (cfg.fast) {
-            int rc = fast_shape_for(h, dtype, a, cfg.fast_shape);
+            int rc = fast_shape_for(h, dtype, a, aligned, cfg.fast_shape);
             if (rc) return rc;
+            if (shape_needs_pairs(cfg.fast_shape.kind) && !aligned) cfg.fast = false;
         }
     }
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;
@@ -925,6 +949,12 @@ cudaStream_t edk_internal_stream(edk_ctx *ctx) { return ctx->stream; }
 
 int edk_internal_ctx_device(const edk_ctx *ctx) { return ctx->device; }
 
+void edk_internal_fp32_sums(edk_ctx *ctx, int *enable, int64_t *min_dim)
+{
+    *enable = ctx->fp32_sums;
+    *min_dim = ctx->fp32_sums_min_dim;
+}
+
 int edk_internal_fail(edk_ctx *ctx, int code, const char *msg) { return ctx->fail(code, "%s", msg); }
 
 edk_ctx *edk_internal_h_ctx(edk_h *h) { return h->ctx; }
@@ -962,7 +992,7 @@ int edk_ctx_set_graphs(edk_ctx *ctx, int enable)
 
 int edk_ctx_set_kernel_path(edk_ctx *ctx, int path)
 {
-    if (!ctx || path < 0 || (path > 3 && path < 16) || path > 27) return EDK_ERR_INVALID;
+    if (!ctx || path < 0 || (path > 3 && path < 16) || path >= 16 + kMaxShapes) return EDK_ERR_INVALID;
     ctx->kernel_path = path;
     return EDK_OK;
 }
@@ -1007,6 +1037,14 @@ int edk_ctx_set_workspace_limit(edk_ctx *ctx, int64_t bytes)
 {
     if (!ctx || bytes < 0) return EDK_ERR_INVALID;
     ctx->work_limit = (size_t)bytes;
+    return EDK_OK;
+}
+
+int edk_ctx_set_fp32_sums(edk_ctx *ctx, int enable, int64_t min_dim)
+{
+    if (!ctx || min_dim < 0) return EDK_ERR_INVALID;
+    ctx->fp32_sums = enable ? 1 : 0;
+    ctx->fp32_sums_min_dim = min_dim;
     return EDK_OK;
 }
 
@@ -1244,6 +1282,22 @@ int edk_h_destroy(edk_h *h)
     return EDK_OK;
 }
 
+int edk_h_launch_shapes(const edk_h *h, int dtype, int32_t *desc, int32_t cap)
+{
+    if (!h || (dtype != EDK_F64 && dtype != EDK_F32) || cap < 0 || (cap > 0 && !desc)) return -1;
+    if (h->sz) return 0;
+    FastShape cand[kMaxShapes];
+    const int n = fast_shapes(h->H, dtype == EDK_F64 ? 8 : 4, h->ctx->num_sms, cand, kMaxShapes);
+    for (int i = 0; i < n && i < cap; ++i) {
+        desc[5 * i] = cand[i].r;
+        desc[5 * i + 1] = cand[i].kmu;
+        desc[5 * i + 2] = cand[i].kmd;
+        desc[5 * i + 3] = cand[i].variant;
+        desc[5 * i + 4] = cand[i].kind;
+    }
+    return n;
+}
+
 int edk_h_dims(const edk_h *h, int64_t *dim, int64_t *dim_up, int64_t *dim_dn)
 {
     if (!h) return EDK_ERR_INVALID;
@@ -1357,7 +1411,9 @@ int edk_lanczos_e0(edk_h *h, const edk_lanczos_opts *o, edk_lanczos_result *r)
         }
         if ((rc = tri_wait(c, ready, T))) return rc;
         if (queued > ready && (rc = tri_enqueue(c, queued))) return rc;
-        if (T.flags[1]) return c->fail(EDK_ERR_NOT_FINITE, "non-finite Lanczos coefficient");
+        if (T.flags[1] == 2) return c->fail(EDK_ERR_TIMEOUT, "row kernel: a bounded wait for staged rows gave up");
+        if (T.flags[1] == 2) return c->fail(EDK_ERR_TIMEOUT, "row kernel: a bounded wait for staged rows gave up");
+    if (T.flags[1]) return c->fail(EDK_ERR_NOT_FINITE, "non-finite Lanczos coefficient");
         for (int it = checked + 1; it <= ready; ++it) {
             const int m = std::min(ne, it);
             if (o->use_target) {
@@ -1598,6 +1654,7 @@ int edk_green_chain(edk_h *t, int dtype, const void *start_dev, int32_t nitergre
     if ((rc = krylov_run(K, niter))) return rc;
     TriHost T;
     if ((rc = fetch_tri(c, K.k, T))) return rc;
+    if (T.flags[1] == 2) return c->fail(EDK_ERR_TIMEOUT, "row kernel: a bounded wait for staged rows gave up");
     if (T.flags[1]) return c->fail(EDK_ERR_NOT_FINITE, "non-finite Lanczos coefficient");
     int n = niter;
     for (int it = 1; it < niter; ++it)

@@ -81,7 +81,8 @@ struct RowArgs {
     double *partials = nullptr;    // gridDim*4 doubles
     unsigned *counter = nullptr;   // last-block counter
     double *sums_out = nullptr;    // 4 doubles: final sums (deterministic order)
-    int *flags = nullptr;          // [0] breakdown step (0 = none), [1] non-finite
+    int *flags = nullptr;          // [0] breakdown step (0 = none), [1] non-finite (1) or timeout (2)
+    int sum32 = 0;                 // FP32 vectors: hop terms summed in FP32 (bulk-copy kernels)
 };
 
 // Launch shape of the fast row kernel: rows per group, up/down table-width
@@ -91,8 +92,16 @@ struct RowArgs {
 // thread in all).
 // One column per thread (24 resident warps instead of 16) was measured at
 // ns=16 and never beat these two, so it is not instantiated.
+// kind 0: the fast row kernel (edk_rows_fast.cuh); kinds 1 and 2: the same
+// mathematics with rows staged by bulk copies (edk_rows_tma.cuh): 1 = one
+// column per thread with the next column's loads in flight (any alignment,
+// odd rows), 2 = two columns per thread.  Kinds 0 and 2 read column pairs and
+// need vectors aligned to twice the element size and even rows.  Block
+// variants: 0 = 512 threads x 1 block per SM, 1 = 256 x 2, 2 = 128 x 4,
+// 3 = 768 x 1 (kind 2).
+inline bool shape_needs_pairs(int kind) { return kind == 0 || kind == 2; }
 struct FastShape {
-    int r = 0, kmu = 0, kmd = 0, variant = 0;
+    int r = 0, kmu = 0, kmd = 0, variant = 0, kind = 0;
 };
 
 struct LaunchCfg {

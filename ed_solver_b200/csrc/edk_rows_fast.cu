@@ -1,6 +1,7 @@
 // Fast row kernel: FP32 instances, launch-shape enumeration and dispatch.
 // The kernel itself is in edk_rows_fast.cuh.
 #include "edk_rows_fast.cuh"
+#include "edk_rows_tma.cuh"
 
 namespace edk {
 
@@ -21,14 +22,24 @@ int rows_allowed(int eb, int kmd, int *out)
     return 1;
 }
 
+// Rows per group of the bulk-copy kernel (one column per thread, the loads of
+// the next column in registers): two rows while the neighbour loads fit.
+int tma_rows_allowed(int eb, int kmd, int *out)
+{
+    if (eb == 4 && kmd <= 12) { out[0] = 2; out[1] = 1; return 2; }
+    if (eb == 8 && kmd == 4) { out[0] = 2; out[1] = 1; return 2; }
+    out[0] = 1;
+    return 1;
+}
+
 }  // namespace
 
 bool fast_rows_ok(const HamDev &H, int elem_bytes)
 {
     const int kmax = H.up.ell_k > H.dn_kmax ? H.up.ell_k : H.dn_kmax;
     const int64_t rowbytes = H.dup * (int64_t)elem_bytes;
-    return !H.hund && H.nc <= 2 && (H.dup % 2) == 0 && kmax <= 16 && rowbytes <= kMaxSmemBytes &&
-           H.up.packed && H.dup * H.ddn < (int64_t)1 << 31 && H.up.ell_k >= 0;
+    return !H.hund && H.nc <= 2 && kmax <= 16 && rowbytes <= kMaxSmemBytes && H.up.packed &&
+           H.dup * H.ddn < (int64_t)1 << 31 && H.up.ell_k >= 0;
 }
 
 int fast_shapes(const HamDev &H, int elem_bytes, int num_sms, FastShape *out, int cap)
@@ -40,7 +51,8 @@ int fast_shapes(const HamDev &H, int elem_bytes, int num_sms, FastShape *out, in
     int rs[3];
     const int nr = rows_allowed(elem_bytes, kmd, rs);
     int n = 0;
-    for (int variant = 0; variant < 3; ++variant) {
+    // the register-staged kernel reads column pairs: even rows only
+    for (int variant = 0; variant < 3 && (H.dup % 2) == 0; ++variant) {
         // shared memory per block when 1, 2 or 4 blocks share an SM
         const int64_t smem_cap = kMaxSmemBytes / (variant == 0 ? 1 : variant == 1 ? 2 : 4);
         // 128-thread blocks only pay off for short rows
@@ -50,7 +62,30 @@ int fast_shapes(const HamDev &H, int elem_bytes, int num_sms, FastShape *out, in
             if ((int64_t)r * rowbytes > smem_cap) continue;
             // keep every SM busy: no multi-row groups when there are too few rows
             if (r > 1 && (H.ddn + r - 1) / r < num_sms) continue;
-            out[n++] = FastShape{r, kmu, kmd, variant};
+            out[n++] = FastShape{r, kmu, kmd, variant, 0};
+        }
+    }
+    // the bulk-copy kernels: two staged-row buffers of R rows per block
+    const int64_t slotb = (int64_t)tma_slot_elems(H.dup, elem_bytes) * elem_bytes;
+    auto feasible = [&](int r, int variant) {
+        const int64_t smem_cap = kMaxSmemBytes / (variant == 0 ? 1 : variant == 1 ? 2 : 4);
+        if (variant == 2 && H.dup > 4096) return false;
+        if (2 * r * slotb > smem_cap) return false;
+        return !(r > 1 && (H.ddn + r - 1) / r < num_sms);
+    };
+    const int nr2 = tma_rows_allowed(elem_bytes, kmd, rs);
+    for (int variant = 0; variant < 3; ++variant)
+        for (int i = 0; i < nr2 && n < cap; ++i)
+            if (feasible(rs[i], variant)) out[n++] = FastShape{rs[i], kmu, kmd, variant, 1};
+    // kind 2 (instantiated for down-table bounds 8 and 12): variants 0, 1 and
+    // 3 (768 threads, one block per SM)
+    if ((kmd == 8 || kmd == 12) && (H.dup % 2) == 0) {
+        const int rr[2] = {2, 1};
+        for (int i = 0; i < 2; ++i) {
+            const int r = rr[i];
+            if (elem_bytes == 8 && r > 1) continue;
+            for (int variant : {0, 1, 3})
+                if (n < cap && feasible(r, variant == 3 ? 0 : variant)) out[n++] = FastShape{r, kmu, kmd, variant, 2};
         }
     }
     return n;
@@ -59,6 +94,8 @@ int fast_shapes(const HamDev &H, int elem_bytes, int num_sms, FastShape *out, in
 cudaError_t launch_rows_fast(const HamDev &H, int dtype, const RowArgs &a, int num_sms, const FastShape &s,
                              cudaStream_t st)
 {
+    if (s.kind >= 1)
+        return dtype == EDK_F64 ? launch_tma_f64(H, a, num_sms, s, st) : launch_tma_f32(H, a, num_sms, s, st);
     return dtype == EDK_F64 ? launch_fast_f64(H, a, num_sms, s, st) : launch_fast_f32(H, a, num_sms, s, st);
 }
 

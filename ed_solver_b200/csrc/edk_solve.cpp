@@ -45,6 +45,13 @@ struct DBuf {
 // Sectors with fewer states than this run in FP64 even in mixed precision,
 // and their Green chains run batched (one persistent launch for all of them).
 constexpr int64_t kLowprecMinDim = (int64_t)1 << 20;
+// With edk_solve_opts.fp32_sums, FP32 passes of sectors of at least this many
+// states sum their hop terms in FP32.  Smaller sectors keep FP64 sums even when
+// lowprec_min_dim lets them run FP32 vectors: a chain with a pole close to the
+// Fermi level in a sector of a few thousand states loses a factor of about 4
+// in G with FP32 sums, while at 1.2e7 states the error stays at the level of
+// the FP32 storage of the vectors.
+constexpr int64_t kFp32SumsMinDim = (int64_t)1 << 20;
 // Longest row the batched kernel stages in shared memory (FP64 elements).
 constexpr int64_t kBatchMaxDup = 96 * 1024 / 8;
 // Sectors of at most this many states are diagonalised densely (ED_diago),
@@ -74,6 +81,7 @@ cudaStream_t edk_internal_stream(edk_ctx *ctx);
 int edk_internal_fail(edk_ctx *ctx, int code, const char *msg);
 void edk_internal_count(edk_ctx *ctx, int64_t h2d, int64_t d2h);
 edk_ctx *edk_internal_h_ctx(edk_h *h);
+void edk_internal_fp32_sums(edk_ctx *ctx, int *enable, int64_t *min_dim);
 
 int edk_convert(edk_ctx *ctx, int from_dtype, int to_dtype, int64_t n, const void *in_dev, void *out_dev)
 {
@@ -126,6 +134,15 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
     const double demax = o->demax0 / o->beta;
     int rc;
     const int64_t lowprec_min = o->lowprec_min_dim > 0 ? o->lowprec_min_dim : kLowprecMinDim;
+    // the context's FP32-sum setting for the duration of the solve
+    struct SumsGuard {
+        edk_ctx *c;
+        int en = 0;
+        int64_t md = 0;
+        ~SumsGuard() { edk_ctx_set_fp32_sums(c, en, md); }
+    } sums_guard{ctx};
+    edk_internal_fp32_sums(ctx, &sums_guard.en, &sums_guard.md);
+    edk_ctx_set_fp32_sums(ctx, o->dtype == EDK_F32 && o->fp32_sums ? 1 : 0, kFp32SumsMinDim);
     auto sector_dtype = [&](int64_t dim) {
         return (o->dtype == EDK_F32 && dim >= lowprec_min) ? EDK_F32 : EDK_F64;
     };

@@ -72,7 +72,7 @@ class _SolveOpts(C.Structure):
                 ("residual_tol", C.c_double), ("green_mode", C.c_int32), ("gs_in", C.c_char_p),
                 ("gs_out", C.c_char_p), ("sector_bound_file", C.c_char_p), ("iwindow", C.c_int32),
                 ("recompute_pass2", C.c_int32), ("reference_small_sectors", C.c_int32),
-                ("lowprec_min_dim", C.c_int64)]
+                ("lowprec_min_dim", C.c_int64), ("fp32_sums", C.c_int32)]
 
 
 class _ChilocSectors(C.Structure):
@@ -193,6 +193,8 @@ def lib():
         "edk_ctx_transfer_bytes": (C.c_int, [P, P, P]),
         "edk_ctx_clear_cache": (C.c_int, [P]),
         "edk_ctx_trim": (C.c_int, [P]),
+        "edk_ctx_set_fp32_sums": (C.c_int, [P, C.c_int, C.c_int64]),
+        "edk_h_launch_shapes": (C.c_int, [P, C.c_int, P, C.c_int32]),
         "edk_ctx_set_workspace_limit": (C.c_int, [P, C.c_int64]),
         "edk_ctx_timing_report": (C.c_int, [P, C.c_int, P, P]),
         "edk_h_create": (C.c_int, [P, P, C.c_int, C.c_int, P]),
@@ -375,6 +377,10 @@ class Context:
         """Caps the Krylov workspace; a pass needing more fails with EDK_ERR_NOMEM (0: no cap)."""
         self.check(lib().edk_ctx_set_workspace_limit(self.h, int(nbytes)), "set_workspace_limit")
 
+    def set_fp32_sums(self, enable: bool, min_dim: int = 1 << 20):
+        """FP32 vectors of sectors with at least min_dim states: sum the hop terms of H*v in FP32."""
+        self.check(lib().edk_ctx_set_fp32_sums(self.h, int(bool(enable)), int(min_dim)), "set_fp32_sums")
+
     def trim(self):
         """Returns the device memory the Krylov-basis pool keeps in reserve."""
         self.check(lib().edk_ctx_trim(self.h), "trim")
@@ -446,6 +452,17 @@ class Hamiltonian:
         lib().edk_h_table(self.h, spin, C.byref(nnz), ptr.ctypes.data, tgt.ctypes.data,
                           val.ctypes.data, diag.ctypes.data)
         return ptr, tgt[:nnz.value], val[:nnz.value], diag[:d]
+
+    def launch_shapes(self, dtype="f64"):
+        """Feasible launch shapes of the fast row kernels, in the order
+        Context.set_kernel_path(16 + i) selects them: dicts with rows per
+        group, table bounds, block variant and kernel kind."""
+        desc = np.zeros(5 * 32, np.int32)
+        n = lib().edk_h_launch_shapes(self.h, _dtype_code(dtype), desc.ctypes.data, 32)
+        if n < 0:
+            raise EdkError(EDK_ERR_INVALID, "launch_shapes")
+        return [dict(zip(("rows", "kmu", "kmd", "variant", "kind"), map(int, desc[5 * i:5 * i + 5])))
+                for i in range(min(n, 32))]
 
     def hmult(self, x, out=None):
         """Hmult__: y = H x for a device tensor x (float64 or float32)."""
@@ -808,7 +825,7 @@ def solve(ctx: Context, model: AIMModel, sectors, beta: float, nw: int, dtype="f
           nitermax=1000, tolerance=1e-12, tolerance_lowprec=1e-6, demax0=5.0, nitergreen=200,
           spins=(0, 1), pairs=None, cutoff_dynamic=1e-8, check_every=8, ran_tab=None, residual_tol=0.0,
           green_mode=0, gs_in=None, gs_out=None, sector_bound_file=None, iwindow=1, recompute_pass2=False,
-          reference_small_sectors=False, lowprec_min_dim=0):
+          reference_small_sectors=False, lowprec_min_dim=0, fp32_sums=False):
     """One impurity solve through the C-ABI (edk_solve): host inputs, host outputs.
     recompute_pass2: rerun the Lanczos recurrence in pass 2 (the reference's way)
     instead of forming the eigenvectors from the Krylov vectors pass 1 kept.
@@ -817,6 +834,8 @@ def solve(ctx: Context, model: AIMModel, sectors, beta: float, nw: int, dtype="f
     (compute_dynamic_full_ed) instead of an exact continued fraction.
     lowprec_min_dim: in mixed precision, the smallest sector that runs FP32
     vectors (0: 2^20).
+    fp32_sums: in mixed precision, sum the hop terms of H*v in FP32 in sectors
+    of at least 2^20 states (the recurrence, norms and alpha/beta stay FP64).
 
     Returns dict(e0, z, residual, nstates, lanczos_steps, green_steps, G (2, npairs, nw) complex,
     docc (nc,), energies, sectors, e0_lowprec).
@@ -833,7 +852,8 @@ def solve(ctx: Context, model: AIMModel, sectors, beta: float, nw: int, dtype="f
                    None if tab is None else tab.ctypes.data, float(residual_tol), int(green_mode),
                    None if gs_in is None else gs_in.encode(), None if gs_out is None else gs_out.encode(),
                    None if sector_bound_file is None else sector_bound_file.encode(), int(iwindow),
-                   1 if recompute_pass2 else 0, 1 if reference_small_sectors else 0, int(lowprec_min_dim))
+                   1 if recompute_pass2 else 0, 1 if reference_small_sectors else 0, int(lowprec_min_dim),
+                   1 if fp32_sums else 0)
     G = np.zeros((2, len(pr) // 2, nw, 2))
     docc = np.zeros(model.nc)
     en = np.zeros(64)

@@ -111,6 +111,7 @@ module edk_fortran
     type(c_ptr) :: gs_in, gs_out, sector_bound_file
     integer(c_int32_t) :: iwindow, recompute_pass2, reference_small_sectors
     integer(c_int64_t) :: lowprec_min_dim
+    integer(c_int32_t) :: fp32_sums
   end type
 
   type, bind(C) :: edk_solve_result
@@ -369,6 +370,19 @@ module edk_fortran
     integer(c_int) function edk_ctx_clear_cache(ctx) bind(C, name="edk_ctx_clear_cache")
       import :: c_int, c_ptr
       type(c_ptr), value :: ctx
+    end function
+    integer(c_int) function edk_h_launch_shapes(h, dtype, desc, cap) bind(C, name="edk_h_launch_shapes")
+      import :: c_int, c_ptr, c_int32_t
+      type(c_ptr), value :: h
+      integer(c_int), value :: dtype
+      integer(c_int32_t) :: desc(*)
+      integer(c_int32_t), value :: cap
+    end function
+    integer(c_int) function edk_ctx_set_fp32_sums(ctx, enable, min_dim) bind(C, name="edk_ctx_set_fp32_sums")
+      import :: c_int, c_ptr, c_int64_t
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: enable
+      integer(c_int64_t), value :: min_dim
     end function
     integer(c_int) function edk_ctx_trim(ctx) bind(C, name="edk_ctx_trim")
       import :: c_int, c_ptr

@@ -81,7 +81,7 @@ int edk_ctx_timing(edk_ctx *ctx, int enable);
  * and element type, and the context keeps the choice for later Hamiltonians of
  * the same shape), 1 = always the generic kernel (for A/B checks), 2 or 3 = the
  * fast kernel where its preconditions hold with its default launch shape,
- * 16+i (i < 12) = the fast kernel with its i-th feasible launch shape (modulo
+ * 16+i (i < 32) = the fast kernel with its i-th feasible launch shape (modulo
  * their number), for measurements. */
 int edk_ctx_set_kernel_path(edk_ctx *ctx, int path);
 /* 1 (default): Lanczos passes and Green chains replay pairs of fused steps as
@@ -110,6 +110,12 @@ int edk_ctx_trim(edk_ctx *ctx);
  * the reference would die in an allocation, a caller with a memory budget
  * gets a status instead. */
 int edk_ctx_set_workspace_limit(edk_ctx *ctx, int64_t bytes);
+/* FP32 Krylov vectors of sectors with at least min_dim states: enable != 0
+ * sums the up- and down-spin hop terms of H*v in FP32 (the diagonal and
+ * density terms, the Lanczos recurrence and its norms stay FP64), which takes
+ * most FP32 -> FP64 conversions out of the step.  Off by default; edk_solve
+ * sets it for its FP32 passes from edk_solve_opts.fp32_sums. */
+int edk_ctx_set_fp32_sums(edk_ctx *ctx, int enable, int64_t min_dim);
 
 /* ---- basis (quantum_fermion_hilbert_class.f90:346-421) ----------------- */
 int64_t edk_binom(int n, int k);
@@ -134,6 +140,14 @@ int edk_h_create(edk_ctx *ctx, const edk_model *m, int nup, int ndn, edk_h **out
  * the context (the Hamiltonian synchronises on the context's stream). */
 int edk_h_destroy(edk_h *h);
 int edk_h_dims(const edk_h *h, int64_t *dim, int64_t *dim_up, int64_t *dim_dn);
+/* The feasible launch shapes of the fast row kernels for this sector and
+ * element type, in the order edk_ctx_set_kernel_path(ctx, 16 + i) selects
+ * them; returns their number (or -1 on bad arguments) and writes the first
+ * min(number, cap) as 5 ints each: rows per group, up-table bound, down-table
+ * bound, block variant (0: 512 threads, 1: 256 x 2, 2: 128 x 4 per SM) and
+ * kernel kind (0: register-staged rows, 1: rows staged by bulk copies with
+ * the neighbour loads pipelined). */
+int edk_h_launch_shapes(const edk_h *h, int dtype, int32_t *desc, int32_t cap);
 /* Export one spin species' table (tab_HAIM2, HAIM_offdiag_arrays.f90:210-606)
  * as built for the device: CSR row pointer ptr[dim_s+1], 0-based target rank
  * tgt[nnz], value val[nnz], diagonal diag[dim_s].  Any pointer may be NULL;
@@ -424,6 +438,9 @@ typedef struct edk_solve_opts {
                                     fraction of min(nitergreen, dim) steps, exact for the sector */
     int64_t lowprec_min_dim;     /* mixed precision: sectors of at least this many states run
                                     FP32 Krylov vectors; 0 means 2^20 */
+    int32_t fp32_sums;           /* mixed precision: 1 sums the hop terms of H*v in FP32 in the
+                                    FP32 passes of sectors of at least 2^20 states
+                                    (edk_ctx_set_fp32_sums); 0 keeps every sum in FP64 */
 } edk_solve_opts;
 
 typedef struct edk_solve_result {

@@ -67,7 +67,9 @@ def test_eigenvector_start_exhausts_the_krylov_space(ctx, dtype):
     assert r["status"] == edk.EDK_KRYLOV_EXHAUSTED
     assert r["niter"] == 1
     assert r["subdiag"][1] == 0.0
-    assert abs(r["E"][0] - d[i, i]) < 1e-12 * max(1.0, abs(d[i, i]))
+    # FP32 storage rounds the stored vector s = H v to FP32, and alpha is read from it
+    tol = 1e-12 if dtype == "f64" else 1.2e-7
+    assert abs(r["E"][0] - d[i, i]) < tol * max(1.0, abs(d[i, i]))
     _after_ok(ctx)
 
 

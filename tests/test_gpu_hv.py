@@ -135,8 +135,8 @@ def test_hmult_fp32_large_sectors(ctx, kpath, name, sec):
 
 
 def test_every_fast_kernel_launch_shape_is_exact(ctx):
-    """Each feasible launch shape of the fast row kernel (rows per group, block
-    shape, columns per thread) on the ns=14 (7,7) and (8,7) sectors: FP64
+    """Each feasible launch shape of both fast row kernels (rows per group,
+    block shape, kernel kind) on the ns=14 (7,7) and (8,7) sectors: FP64
     bit-exact, FP32 within the output rounding."""
     import torch
     m = workload("c3").model
@@ -149,14 +149,43 @@ def test_every_fast_kernel_launch_shape_is_exact(ctx):
         y32 = ho.hmult(x.astype(np.float32).astype(np.float64))
         xd = torch.tensor(x, device="cuda")
         xf = xd.to(torch.float32)
+        n64, n32 = len(h.launch_shapes("f64")), len(h.launch_shapes("f32"))
+        assert any(sh["kind"] == 1 for sh in h.launch_shapes("f32")), h.launch_shapes("f32")
         try:
-            for i in range(12):
+            for i in range(max(n64, n32)):
                 ctx.set_kernel_path(16 + i)
                 assert np.array_equal(h.hmult(xd).cpu().numpy(), y64), (sec, i)
                 yf = h.hmult(xf).double().cpu().numpy()
                 assert np.abs(yf - y32).max() <= 1.2e-7 * np.abs(y32).max(), (sec, i)
         finally:
             ctx.set_kernel_path(0)
+
+
+def test_fp32_hop_sums_every_launch_shape(ctx):
+    """FP32 hop sums (edk_ctx_set_fp32_sums) at every launch shape on the
+    ns=14 (7,7) and (8,7) sectors: H*v of the FP32-rounded input within
+    2e-6 of the largest element of the oracle's FP64 H*v (eight FP32 products
+    per spin summed in FP32 against the FP64 sums)."""
+    import torch
+    m = workload("c3").model
+    rng = np.random.default_rng(17)
+    ctx.set_fp32_sums(True, 1)
+    try:
+        for sec in [(7, 7), (8, 7)]:
+            h = edk.Hamiltonian(ctx, m, *sec)
+            ho = O.OracleH(m, *sec)
+            x = rng.normal(size=h.dim).astype(np.float32)
+            y = ho.hmult(x.astype(np.float64))
+            xf = torch.tensor(x, device="cuda")
+            n = len(h.launch_shapes("f32"))
+            assert n > 0
+            for i in range(n):
+                ctx.set_kernel_path(16 + i)
+                yf = h.hmult(xf).double().cpu().numpy()
+                assert np.abs(yf - y).max() <= 2e-6 * np.abs(y).max(), (sec, i, h.launch_shapes("f32")[i])
+    finally:
+        ctx.set_kernel_path(0)
+        ctx.set_fp32_sums(False)
 
 
 def test_launch_shape_timed_once_per_sector_shape():
