@@ -319,19 +319,21 @@ def run_ours(args):
 
 
 def run_kernel_case(args):
-    """Six FP32 Lanczos steps of the ns=16 (8,8) sector and nothing else: the
-    small case (3.3 GB of vectors) for per-kernel ncu captures."""
+    """Six FP32 Lanczos steps of one ns=16 sector (--kernel-sector, default
+    (8,8)) and nothing else: the small case (3.3 GB of vectors) for per-kernel
+    ncu captures."""
     import torch
     from ed_solver_b200 import edk
     ctx = edk.Context(0)
-    h = edk.Hamiltonian(ctx, _model(), *WORKLOAD["sector"])
+    sector = tuple(int(v) for v in args.kernel_sector.split(",")) if args.kernel_sector else WORKLOAD["sector"]
+    h = edk.Hamiltonian(ctx, _model(), *sector)
     # one fixed launch shape (--kernel-shape, an index into the sector's list), no timing launches
     shapes = h.launch_shapes("f32")
     ctx.set_kernel_path(16 + args.kernel_shape)
     ctx.set_fp32_sums(args.fp32_sums)
     r = h.lanczos_e0(dtype="f32", nitermax=6, tolerance=0.0, check_every=6)
     torch.cuda.synchronize()
-    print(json.dumps({"kernel_case": "ns16 (8,8) FP32 Lanczos", "dim": h.dim, "niter": r["niter"],
+    print(json.dumps({"kernel_case": f"ns16 {sector} FP32 Lanczos", "dim": h.dim, "niter": r["niter"],
                       "shape": shapes[args.kernel_shape % len(shapes)], "fp32_sums": bool(args.fp32_sums)}),
           flush=True)
     h.close()
@@ -606,6 +608,7 @@ def main():
                     help="run only six FP32 Lanczos steps of the (8,8) sector (profiling case)")
     ap.add_argument("--kernel-shape", type=int, default=0,
                     help="launch shape of the --kernel-case (index into the sector's feasible shapes)")
+    ap.add_argument("--kernel-sector", default=None, help="sector of the --kernel-case, e.g. 9,8")
     ap.add_argument("--fp32-sums", action="store_true",
                     help="sum the hop terms of H*v in FP32 in the FP32 passes of large sectors")
     ap.add_argument("--grad", action="store_true",

@@ -479,12 +479,52 @@ int fast_shape_for(edk_h *h, int dtype, const RowArgs &a, bool aligned, FastShap
         if (n == 1 || c->kernel_path != 0) { h->fast_shape[slot] = out; h->fast_tuned[slot] = true; }
         return EDK_OK;
     }
+    // Candidates are timed as the launch they mostly serve, a fused Lanczos
+    // step, against scratch coefficients, flags and reduction buffers of their
+    // own (so the live Lanczos state is untouched) and a zeroed scratch vector
+    // that stands in for v_k, v_{k-1} and the second output: x is gathered,
+    // the call's y is written (the real launch then overwrites it).  The
+    // flags and the block counter are cleared before every timed launch.
+    // Without room for the scratch vector, H*v mode.
     RowArgs t = a;
     t.mode = kModeHv;
+    DevBuf tv, tstate;
+    const size_t vbytes = (size_t)h->dim * eb;
+    if (tv.ensure(vbytes) == cudaSuccess && tstate.ensure(sizeof(double) * (16 + 4 * (size_t)c->num_sms * 16) + 256) ==
+                                                cudaSuccess) {
+        double *tri = tstate.as<double>();                 // tri_diag [0..7], tri_sub [8..15]
+        double *part = tri + 16;
+        const double init[16] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0};
+        int rc0 = c->cuda(cudaMemcpyAsync(tri, init, sizeof init, cudaMemcpyHostToDevice, c->stream), "tune state");
+        unsigned char *tail = reinterpret_cast<unsigned char *>(part + 4 * (size_t)c->num_sms * 16);
+        if (!rc0) rc0 = c->cuda(cudaMemsetAsync(tail, 0, 256, c->stream), "tune state");
+        if (!rc0) rc0 = c->cuda(cudaMemsetAsync(tv.p, 0, vbytes, c->stream), "tune state");
+        if (!rc0) rc0 = c->cuda(cudaStreamSynchronize(c->stream), "tune state");
+        if (rc0) return rc0;
+        t.mode = kModeStep;
+        t.k = 1;
+        t.kdev = nullptr;
+        t.gamma1 = 0.0;
+        t.cutoff = 1e-300;
+        t.tri_diag = tri;
+        t.tri_sub = tri + 8;
+        t.partials = part;
+        t.counter = reinterpret_cast<unsigned *>(tail);
+        t.sums_out = reinterpret_cast<double *>(tail + 64);
+        t.flags = reinterpret_cast<int *>(tail + 128);
+        t.vk = tv.p;
+        t.vkm1 = tv.p;
+        t.vout = tv.p;
+        t.psi = nullptr;
+        t.psi_coef = nullptr;
+    } else {
+        (void)cudaGetLastError();
+    }
     cudaEvent_t ea = c->get_event(), eb_ = c->get_event();
     float best = 3.0e38f;
     for (int i = 0; i < n; ++i)
         for (int rep = 0; rep < 2; ++rep) {
+            if (t.mode == kModeStep) cudaMemsetAsync(reinterpret_cast<void *>(t.counter), 0, 256, c->stream);
             cudaEventRecord(ea, c->stream);
             cudaError_t e = launch_rows_fast(h->H, dtype, t, c->num_sms, cand[i], c->stream);
             cudaEventRecord(eb_, c->stream);

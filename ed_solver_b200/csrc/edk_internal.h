@@ -98,7 +98,7 @@ struct RowArgs {
 // odd rows), 2 = two columns per thread.  Kinds 0 and 2 read column pairs and
 // need vectors aligned to twice the element size and even rows.  Block
 // variants: 0 = 512 threads x 1 block per SM, 1 = 256 x 2, 2 = 128 x 4,
-// 3 = 768 x 1 (kind 2).
+// 3 = 768 x 1 and 4 = 640 x 1 (kind 2).
 inline bool shape_needs_pairs(int kind) { return kind == 0 || kind == 2; }
 struct FastShape {
     int r = 0, kmu = 0, kmd = 0, variant = 0, kind = 0;

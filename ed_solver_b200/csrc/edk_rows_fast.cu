@@ -77,15 +77,21 @@ int fast_shapes(const HamDev &H, int elem_bytes, int num_sms, FastShape *out, in
     for (int variant = 0; variant < 3; ++variant)
         for (int i = 0; i < nr2 && n < cap; ++i)
             if (feasible(rs[i], variant)) out[n++] = FastShape{rs[i], kmu, kmd, variant, 1};
-    // kind 2 (instantiated for down-table bounds 8 and 12): variants 0, 1 and
-    // 3 (768 threads, one block per SM)
+    // kind 2 (instantiated for down-table bounds 8 and 12, and in FP32 with
+    // one row per group for tables exactly 9 wide): variants 0, 1, 3 (768
+    // threads, one block per SM) and 4 (640 threads, one block per SM)
     if ((kmd == 8 || kmd == 12) && (H.dup % 2) == 0) {
+        const int kmu9 = elem_bytes == 4 && H.up.ell_k == 9 ? 9 : kmu;
+        const int kmd9 = elem_bytes == 4 && H.dn_kmax == 9 ? 9 : kmd;
         const int rr[2] = {2, 1};
         for (int i = 0; i < 2; ++i) {
             const int r = rr[i];
             if (elem_bytes == 8 && r > 1) continue;
-            for (int variant : {0, 1, 3})
-                if (n < cap && feasible(r, variant == 3 ? 0 : variant)) out[n++] = FastShape{r, kmu, kmd, variant, 2};
+            int ku = r == 1 ? kmu9 : kmu, kd = r == 1 ? kmd9 : kmd;
+            // exact-9 instances: (9, 8), (8, 9), (9, 9)
+            if ((ku == 9 && kd == 12) || (kd == 9 && ku == 16)) { ku = kmu; kd = kmd; }
+            for (int variant : {0, 1, 3, 4})
+                if (n < cap && feasible(r, variant >= 3 ? 0 : variant)) out[n++] = FastShape{r, ku, kd, variant, 2};
         }
     }
     return n;

@@ -304,9 +304,11 @@ __global__ void __launch_bounds__(NTHR, MINB) row_tma_kernel(const HamDev H, con
                 d32[r][e] = 0.f;
             }
         // up-spin hops from the staged rows: one table entry serves the R rows
+        // (a table exactly KMU wide runs the unrolled loop without tests)
+        const int kend = K == KMU ? KMU : K;
 #pragma unroll
         for (int k = 0; k < KMU; ++k) {
-            if (k >= K) break;
+            if (K != KMU && k >= kend) break;
 #pragma unroll
             for (int e = 0; e < CPT; ++e) {
                 const uint32_t t = L.ent[k][e] & 0xFFFFFFu;

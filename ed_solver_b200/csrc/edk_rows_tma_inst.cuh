@@ -14,7 +14,8 @@
     if (s.kind == KIND && s.r == R && s.kmu == KMU && s.kmd == KMD)                                          \
         return s.variant == 0   ? launch_tma_t<T, R, KMU, KMD, 512, 1, CPT, PIPE, S>(H, a, num_sms, st)      \
                : s.variant == 1 ? launch_tma_t<T, R, KMU, KMD, 256, 2, CPT, PIPE, S>(H, a, num_sms, st)      \
-                                : launch_tma_t<T, R, KMU, KMD, 768, 1, CPT, PIPE, S>(H, a, num_sms, st);
+               : s.variant == 3 ? launch_tma_t<T, R, KMU, KMD, 768, 1, CPT, PIPE, S>(H, a, num_sms, st)      \
+                                : launch_tma_t<T, R, KMU, KMD, 640, 1, CPT, PIPE, S>(H, a, num_sms, st);
 // kind 2 (two columns per thread): rows per group 2 or 1
 #define EDK_TMA_MORE(T, KMU, KMD, S)                                                                         \
     EDK_TMA_KIND(T, 2, KMU, KMD, S, 2, 2, false)                                                             \
@@ -29,4 +30,6 @@
     EDK_TMA_KIND1(float, 1, 8, 12, S) EDK_TMA_KIND1(float, 1, 16, 12, S)                                     \
     EDK_TMA_KIND1(float, 1, 8, 16, S) EDK_TMA_KIND1(float, 1, 16, 16, S)                                     \
     EDK_TMA_MORE(float, 8, 8, S) EDK_TMA_MORE(float, 16, 8, S)                                               \
-    EDK_TMA_MORE(float, 8, 12, S) EDK_TMA_MORE(float, 16, 12, S)
+    EDK_TMA_MORE(float, 8, 12, S) EDK_TMA_MORE(float, 16, 12, S)                                             \
+    EDK_TMA_KIND(float, 1, 9, 8, S, 2, 2, false) EDK_TMA_KIND(float, 1, 8, 9, S, 2, 2, false)                \
+    EDK_TMA_KIND(float, 1, 9, 9, S, 2, 2, false)

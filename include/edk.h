@@ -144,7 +144,7 @@ int edk_h_dims(const edk_h *h, int64_t *dim, int64_t *dim_up, int64_t *dim_dn);
  * element type, in the order edk_ctx_set_kernel_path(ctx, 16 + i) selects
  * them; returns their number (or -1 on bad arguments) and writes the first
  * min(number, cap) as 5 ints each: rows per group, up-table bound, down-table
- * bound, block variant (0: 512 threads, 1: 256 x 2, 2: 128 x 4 per SM) and
+ * bound, block variant (0: 512 threads, 1: 256 x 2, 2: 128 x 4, 3: 768, 4: 640 per SM) and
  * kernel kind (0: register-staged rows, 1: rows staged by bulk copies with
  * the neighbour loads pipelined). */
 int edk_h_launch_shapes(const edk_h *h, int dtype, int32_t *desc, int32_t cap);
