@@ -1279,6 +1279,46 @@ int edk_apply_csz(edk_h *src, int dtype, int site, int spin, int dagger, int pro
     return rc;
 }
 
+int edk_apply_csz_ab(edk_h *src, int dtype, int site, int proj, int site2, int proj2, int spin, int dagger,
+                     const void *in_dev, void *out_dev, int64_t *out_dim, int32_t *out_npart)
+{
+    if (!src || !in_dev || !out_dev || spin < 0 || spin > 1 || (dtype != EDK_F64 && dtype != EDK_F32))
+        return EDK_ERR_INVALID;
+    edk_ctx *c = src->ctx;
+    if (!src->sz) return c->fail(EDK_ERR_INVALID, "edk_apply_csz_ab needs a Nambu sector (edk_h_create_sz)");
+    const SzDev &S = sz_dev(src->sz);
+    if (site < 0 || site >= S.nc || site2 < 0 || site2 >= S.nc)
+        return c->fail(EDK_ERR_INVALID, "site outside the impurity");
+    const int ns = S.ns;
+    const int create = spin == 0 ? (dagger != 0) : (dagger == 0);
+    const int npt = src->npart + (create ? 1 : -1);
+    if (npt < 0 || npt > 2 * ns) return c->fail(EDK_ERR_INVALID, "target Nambu sector outside [0, 2 ns]");
+    std::string err;
+    const SzSectorDev *tgt = nullptr;
+    int rc = sz_sector(src->sz, npt, c->stream, &tgt, &err);
+    if (rc) return c->fail(rc, "%s", err.c_str());
+    // the two operators of symmetric_combineAB (green_class_compute_symmetric_combination.f90:155-262),
+    // each c[+] of apply_Csz_updo or, projected, of apply_Csz_N_updo (apply_C.f90:404-483)
+    auto op = [&](int st_site, int projected) {
+        SzOp o;
+        const int up_bit = S.nb + st_site, hole_bit = ns + S.nb + st_site;
+        o.bit = 1u << (spin == 0 ? up_bit : hole_bit);
+        o.create = create;
+        o.sgn = 1;
+        if (projected) {
+            o.pmask = 1u << (spin == 0 ? hole_bit : up_bit);
+            o.pwant = spin == 0 ? 0u : o.pmask;
+        }
+        return o;
+    };
+    SzOp ops[2] = {op(site, proj), op(site2, proj2)};
+    if (out_dim) *out_dim = tgt->dim;
+    if (out_npart) *out_npart = npt;
+    rc = c->cuda(launch_sz_apply_c(dtype, S, *tgt, 2, ops, in_dev, out_dev, c->num_sms, c->stream), "apply_csz_ab");
+    c->launches++;
+    return rc;
+}
+
 int edk_apply_cnambu(edk_h *src, int dtype, int orb, int dagger, int orb2, int sign2, const void *in_dev,
                      void *out_dev, int64_t *out_dim, int32_t *out_npart)
 {

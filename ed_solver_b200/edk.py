@@ -227,6 +227,8 @@ def lib():
         "edk_h_create_sz": (C.c_int, [P, P, C.c_int, P]),
         "edk_apply_cnambu": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, P, P, P]),
         "edk_h_sz_info": (C.c_int, [P, P, P]),
+        "edk_apply_csz_ab": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, P, P,
+                                       P]),
         "edk_apply_csz": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, P, P,
                                     P]),
     }
@@ -674,6 +676,22 @@ class HamiltonianSz(Hamiltonian):
         self.ctx.check(lib().edk_apply_csz(self.h, _dtype_code(vec.dtype), site, spin, int(bool(dagger)),
                                            int(bool(projected)), site2, sign2, _ptr(vec), _ptr(out),
                                            C.byref(od), C.byref(on)), "edk_apply_csz")
+        return out, on.value
+
+    def apply_c_ab(self, vec, site, proj, site2, proj2, spin, dagger):
+        """symmetric_combineAB's start vector: (A_site + B_site2)|vec>, each the
+        c[+] of apply_Csz_updo or, projected, of apply_Csz_N_updo (site2 may equal
+        site) -> (tensor in the target sector, npart')."""
+        import torch
+        create = bool(dagger) if spin == 0 else not dagger
+        npt = self.npart + (1 if create else -1)
+        if not 0 <= npt <= 2 * self.model.ns:
+            raise ValueError("target sector outside the Hilbert space")
+        out = torch.empty(binom(2 * self.model.ns, npt), dtype=vec.dtype, device=vec.device)
+        od, on = C.c_int64(), C.c_int32()
+        self.ctx.check(lib().edk_apply_csz_ab(self.h, _dtype_code(vec.dtype), site, int(bool(proj)), site2,
+                                              int(bool(proj2)), spin, int(bool(dagger)), _ptr(vec), _ptr(out),
+                                              C.byref(od), C.byref(on)), "edk_apply_csz_ab")
         return out, on.value
 
     def apply_b(self, vec, orb, dagger, orb2=-1, sign2=1):

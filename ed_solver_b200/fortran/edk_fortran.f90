@@ -278,6 +278,15 @@ module edk_fortran
       real(c_double) :: energy_shift
     end function
     ! apply_Csz_updo / apply_Csz_N_updo (apply_C.f90:344-483)
+    integer(c_int) function edk_apply_csz_ab(src, dtype, site, proj, site2, proj2, spin, dagger, vin, vout, &
+        out_dim, out_npart) bind(C, name="edk_apply_csz_ab")
+      import :: c_int, c_ptr, c_int32_t, c_int64_t
+      type(c_ptr), value :: src
+      integer(c_int), value :: dtype, site, proj, site2, proj2, spin, dagger
+      type(c_ptr), value :: vin, vout
+      integer(c_int64_t) :: out_dim
+      integer(c_int32_t) :: out_npart
+    end function
     integer(c_int) function edk_apply_csz(src, dtype, site, spin, dagger, projected, site2, sign2, vin, vout, &
         out_dim, out_npart) bind(C, name="edk_apply_csz")
       import :: c_int, c_ptr, c_int32_t, c_int64_t

@@ -226,3 +226,44 @@ def green_nambu(hc: HCacheSz, gs, beta: float, nw: int, nitergreen: int, orbs=No
     for (a, b) in pairs:
         out[(a, b)] = raw[(a, b)] if a == b else 0.5 * (raw[(a, b)] - raw[(a, a)] - raw[(b, b)])
     return out
+
+
+def green_ab_nambu(hc: HCacheSz, gs, beta: float, nw: int, nitergreen: int, spin: int = 0, sites=None,
+                   proj_a: bool = True, proj_b: bool = False, cutoff_dynamic=1e-8):
+    """compute_greenAB (green_class_computeAB.f90:23-212) in the Nambu basis for
+    two impurity operators of one spin: A = c (projected: apply_Csz_N_updo,
+    apply_C.f90:404-483) and B = c (apply_Csz_updo).  With A projected and B
+    plain this is the GNF channel of correlations_dyn_stat.h:96.  For every
+    state |psi> (weight boltz): particle chains from (A+_i + B+_j)|psi> and hole
+    chains from (A_i + B_j)|psi> (symmetric_combineAB,
+    green_class_compute_symmetric_combination.f90:155-262, real H), then
+    G_AB(i, j) = (G_{A_i+B_j} - G_{A_i A_i} - G_{B_j B_j}) / 2
+    (reshuffle_vecAB, green_class_compute_symmetric_combination_AB.h:50-69).
+    Returns {(i, j): G} over the impurity sites."""
+    nc = hc.model.nc
+    if sites is None:
+        sites = list(range(nc))
+    wn = matsubara(beta, nw)
+    keys = [("ab", i, j) for i in sites for j in sites] + [("aa", i, i) for i in sites] + \
+           [("bb", j, j) for j in sites]
+    raw = {k: np.zeros(nw, complex) for k in keys}
+    ns2 = 2 * hc.model.ns
+    for st in gs:
+        h_src = hc.get(st["npart"])
+        for iph in (1, 2):
+            dagger = iph == 1
+            create = dagger if spin == 0 else not dagger
+            npt = st["npart"] + (1 if create else -1)
+            if not 0 <= npt <= ns2:
+                continue
+            h_t = hc.get(npt)
+            for (kind, i, j) in keys:
+                pa, pb = {"ab": (proj_a, proj_b), "aa": (proj_a, proj_a), "bb": (proj_b, proj_b)}[kind]
+                if kind == "ab":
+                    v, _ = h_src.apply_c_ab(st["psi"], i, pa, j, pb, spin, dagger)
+                else:
+                    v, _ = h_src.apply_c(st["psi"], i, spin, dagger, projected=pa)
+                G, _, _, _ = h_t.green_chain(v, nitergreen, st["E"], iph, wn, cutoff_dynamic)
+                raw[(kind, i, j)] += st["boltz"] * G
+    return {(i, j): 0.5 * (raw[("ab", i, j)] - raw[("aa", i, i)] - raw[("bb", j, j)])
+            for i in sites for j in sites}

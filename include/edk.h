@@ -535,6 +535,16 @@ int edk_h_sz_info(const edk_h *h, int32_t *npart, double *energy_shift);
  * overwritten) lives in the sector npart +/- 1: binom(2ns, npart +/- 1)
  * elements, returned in out_dim; its Hamiltonian is edk_h_create_sz with
  * the returned *out_npart. */
+/* The start vector of symmetric_combineAB (green_class_compute_symmetric_combination.f90:155-262)
+ * for the A/B Green functions of the Nambu basis, e.g. GNF with A = the
+ * projected c of apply_Csz_N_updo and B = c (correlations_dyn_stat.h:96):
+ * out = A_site |in> + B_site2 |in>, with A and B each the operator of
+ * edk_apply_csz on that site (same spin and dagger) and `proj`/`proj2`
+ * selecting apply_Csz_N_updo for it; site2 may equal site.  The reference
+ * reaches this channel only in the Nambu basis: its n c operator stops in
+ * the (N_up, N_dn) basis (apply_C.f90:135-148). */
+int edk_apply_csz_ab(edk_h *src, int dtype, int site, int proj, int site2, int proj2, int spin, int dagger,
+                     const void *in_dev, void *out_dev, int64_t *out_dim, int32_t *out_npart);
 int edk_apply_csz(edk_h *src, int dtype, int site, int spin, int dagger, int projected, int site2, int sign2,
                   const void *in_dev, void *out_dev, int64_t *out_dim, int32_t *out_npart);
 /* apply_Csz (apply_C.f90:273-333) on Nambu impurity orbitals: b+_orb

@@ -487,6 +487,48 @@ class OracleSz:
         return out, npt
 
 
+def green_ab_nambu(model, gs, beta: float, nw: int, nitergreen: int, spin: int = 0, sites=None,
+                   proj_a: bool = True, proj_b: bool = False, cutoff_dynamic=1e-8):
+    """compute_greenAB in the Nambu basis (ed_solver/green_class_computeAB.f90:23-212)
+    for A = c of one spin, projected (apply_Csz_N_updo, ed_solver/apply_C.f90:404-483)
+    or not (apply_Csz_updo), and B likewise: chains from the symmetric
+    combinations (A+_i + B+_j)|psi> (particle) and (A_i + B_j)|psi> (hole) of
+    symmetric_combineAB (ed_solver/green_class_compute_symmetric_combination.f90:155-262,
+    real H), and G_AB(i,j) = (G_{A_i+B_j} - G_{A_iA_i} - G_{B_jB_j}) / 2
+    (reshuffle_vecAB, ed_solver/green_class_compute_symmetric_combination_AB.h:50-69).
+    gs: list of dict(npart, E, psi, boltz).  Returns {(i, j): G}."""
+    nc = model.nc
+    sites = list(range(nc)) if sites is None else list(sites)
+    wn = matsubara(beta, nw)
+    keys = [("ab", i, j) for i in sites for j in sites] + [("aa", i, i) for i in sites] + \
+           [("bb", j, j) for j in sites]
+    raw = {k: np.zeros(nw, complex) for k in keys}
+    cache = {}
+
+    def H(n):
+        if n not in cache:
+            cache[n] = OracleSz(model, n)
+        return cache[n]
+
+    for st in gs:
+        hs = H(st["npart"])
+        psi = np.asarray(st["psi"], np.float64)
+        for iph in (1, 2):
+            dagger = iph == 1
+            create = dagger if spin == 0 else not dagger
+            npt = st["npart"] + (1 if create else -1)
+            if not 0 <= npt <= 2 * model.ns:
+                continue
+            for (kind, i, j) in keys:
+                pa, pb = {"ab": (proj_a, proj_b), "aa": (proj_a, proj_a), "bb": (proj_b, proj_b)}[kind]
+                v, _ = hs.apply_c(psi, i, spin, dagger, projected=pa)
+                if kind == "ab":
+                    v = v + hs.apply_c(psi, j, spin, dagger, projected=pb)[0]
+                G, _, _ = green_chain(H(npt), v, nitergreen, st["E"], iph, wn, cutoff_dynamic=cutoff_dynamic)
+                raw[(kind, i, j)] += st["boltz"] * G
+    return {(i, j): 0.5 * (raw[("ab", i, j)] - raw[("aa", i, i)] - raw[("bb", j, j)]) for i in sites for j in sites}
+
+
 def colex_rank(state: int) -> int:
     return int(lib().orc_colex_rank(int(state)))
 

@@ -74,3 +74,21 @@ def test_nambu_green_functions_against_lehmann(ctx):
     # the pairing makes the anomalous function non-zero
     assert np.abs(Go[(0, 1)]).max() > 1e-3
     hc.close()
+
+
+@pytest.mark.parametrize("spin", [0, 1])
+def test_gnf_channel_against_oracle(ctx, spin):
+    """compute_greenAB in the Nambu basis with A = the projected c of
+    apply_Csz_N_updo and B = c (the GNF channel of correlations_dyn_stat.h:96):
+    the device chains from edk_apply_csz_ab's symmetric combinations against the
+    oracle's restatement on the same states (1e-9)."""
+    m = nambu_workload(5)
+    beta, nw, demax0 = 20.0, 32, 2.0
+    hc = solver.HCacheSz(ctx, m)
+    gs, e0, z, shift = solver.ground_states_sz(hc, range(0, 2 * m.ns + 1), beta, demax0, neigen=1, tolerance=1e-13)
+    G = solver.green_ab_nambu(hc, gs, beta, nw, 200, spin=spin, cutoff_dynamic=0.0)[(0, 0)]
+    gso = [dict(npart=s["npart"], E=s["E"], psi=s["psi"].double().cpu().numpy(), boltz=s["boltz"]) for s in gs]
+    Go = O.green_ab_nambu(m, gso, beta, nw, 200, spin=spin, cutoff_dynamic=0.0)[(0, 0)]
+    assert np.abs(G - Go).max() < 1e-9 * max(1.0, np.abs(Go).max())
+    assert np.abs(Go).max() > 1e-3
+    hc.close()

@@ -12,12 +12,13 @@
 * the two term orders (tabulated HAIMsz_multr, HAIMsz_mult_fly_r) agree to
   rounding, and the tabulated CSR is the sequential one."""
 import itertools
+import math
 
 import numpy as np
 import pytest
 
 import oracle as O
-from ed_solver_b200.model import NambuModel, nambu_star_model, nambu_workload, star_model
+from ed_solver_b200.model import NambuModel, matsubara, nambu_star_model, nambu_workload, star_model
 
 
 def _two_orbital(pvbc=False, on_fly=False):
@@ -179,3 +180,45 @@ def test_projected_operator_splits_the_plain_one():
     st = ot.table()[0]
     hole = np.array([(int(s) >> (m.ns + m.nb)) & 1 for s in st])
     assert np.array_equal(proj, np.where(hole == 0, full, 0.0))
+
+
+def _ab_lehmann(m, beta, nw, demax0, proj_a, proj_b, spin=0):
+    """G_AB = sum_s w_s [ sum_m <s|A|m><m|B+|s>/(iw - (E_m - E_s)) + <s|B+|m><m|A|s>/(iw + (E_m - E_s)) ]
+    over the dense Nambu sectors, for A = (projected) c of spin `spin` on site 0, B likewise."""
+    wn = matsubara(beta, nw)
+    eig = {n: np.linalg.eigh(O.OracleSz(m, n).dense()) for n in range(2 * m.ns + 1)}
+    e0 = min(w[0] for w, _ in eig.values())
+    states = [(n, k) for n, (w, _) in eig.items() for k in range(len(w)) if w[k] <= e0 + demax0 / beta]
+    z = sum(math.exp(-beta * (eig[n][0][k] - e0)) for n, k in states)
+    g = np.zeros(nw, complex)
+    for n, k in states:
+        ws = math.exp(-beta * (eig[n][0][k] - e0)) / z
+        psi, Es = eig[n][1][:, k], eig[n][0][k]
+        for dagger, sgn in ((True, -1.0), (False, 1.0)):
+            try:
+                pa, npt = O.OracleSz(m, n).apply_c(psi, 0, spin, dagger, projected=proj_a)
+                pb, _ = O.OracleSz(m, n).apply_c(psi, 0, spin, dagger, projected=proj_b)
+            except ValueError:
+                continue
+            W, V = eig[npt]
+            amp = (V.T @ pa) * (V.T @ pb)
+            g += np.array([np.sum(amp / (1j * w + sgn * (W - Es))) for w in wn]) * ws
+    return g, states, eig, e0, z
+
+
+def test_green_ab_nambu_against_lehmann():
+    """The oracle's compute_greenAB restatement (symmetric combinations, then
+    (G_{A+B} - G_AA - G_BB)/2) equals the Lehmann sum <A ; B+> on the dense
+    Nambu sectors of a 4-site superconducting model, for the GNF pair
+    (A projected, B plain) and for A = B = c (where it is G itself)."""
+    from ed_solver_b200.model import nambu_workload
+    m = nambu_workload(4)
+    beta, nw, demax0 = 20.0, 12, 2.0
+    for proj_a, proj_b in ((True, False), (False, False)):
+        g_ref, states, eig, e0, z = _ab_lehmann(m, beta, nw, demax0, proj_a, proj_b)
+        gs = [dict(npart=n, E=float(eig[n][0][k]), psi=eig[n][1][:, k],
+                   boltz=math.exp(-beta * (eig[n][0][k] - e0)) / z) for n, k in states]
+        G = O.green_ab_nambu(m, gs, beta, nw, 200, spin=0, sites=[0], proj_a=proj_a, proj_b=proj_b,
+                             cutoff_dynamic=0.0)[(0, 0)]
+        assert np.abs(G - g_ref).max() < 1e-9 * max(1.0, np.abs(g_ref).max())
+        assert np.abs(g_ref).max() > 1e-3
