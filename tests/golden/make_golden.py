@@ -2,8 +2,11 @@
 
 Reads the reference's test/2b/bm/g_bm (1000 Matsubara rows x 8 columns: Re/Im
 of G11, G12, G21, G22 of the two-orbital test at beta=50) and keeps the first
-200 rows of G11 and G22 as tests/golden/g_bm_2b.txt.  Run in a container that
-has the reference checked out:
+200 rows of G11 and G22 as tests/golden/g_bm_2b.txt; reads the deck's input
+hybridisation test/2b/delta1.inp (the frequency, then Re/Im of Delta11,
+Delta12, Delta21, Delta22) and keeps its first 200 rows of Delta11 and
+Delta22 (fit_nw = 200 in test/2b/ED/ED.in) as tests/golden/delta_2b.txt.
+Run in a container that has the reference checked out:
 
     python tests/golden/make_golden.py /path/to/reference
 
@@ -26,3 +29,8 @@ here = os.path.dirname(os.path.abspath(__file__))
 np.savetxt(os.path.join(here, "g_bm_2b.txt"), out, fmt="%.10f",
            header="wn ReG11 ImG11 ReG22 ImG22  (reference test/2b/bm/g_bm, first 200 rows)")
 print("wrote", os.path.join(here, "g_bm_2b.txt"))
+d = np.loadtxt(os.path.join(ref, "test", "2b", "delta1.inp"))
+out = np.column_stack([d[:n, 0], d[:n, 1], d[:n, 2], d[:n, 7], d[:n, 8]])
+np.savetxt(os.path.join(here, "delta_2b.txt"), out, fmt="%.12f",
+           header="wn ReD11 ImD11 ReD22 ImD22  (reference test/2b/delta1.inp, first 200 rows)")
+print("wrote", os.path.join(here, "delta_2b.txt"))

@@ -67,3 +67,35 @@ def test_fit_recovers_a_bath_from_its_hybridisation(pairing):
     o = np.argsort(fitted.eps)
     assert np.allclose(fitted.eps[o], np.sort(truth.eps), atol=1e-4)
     assert np.allclose(np.abs(fitted.V[o]), np.abs(truth.V[np.argsort(truth.eps)]), atol=1e-4)
+
+
+def _deck_2b():
+    """The hybridisation the reference's two-orbital test deck fits its bath to
+    (test/2b/delta1.inp, fixture written by tests/golden/make_golden.py), in
+    the Nambu form of bath2hybrid: diag(D11, D22, -conj D11, -conj D22)."""
+    import os
+    d = np.loadtxt(os.path.join(os.path.dirname(__file__), "golden", "delta_2b.txt"))
+    wn = d[:, 0]
+    d11, d22 = d[:, 1] + 1j * d[:, 2], d[:, 3] + 1j * d[:, 4]
+    D = np.zeros((len(wn), 4, 4), complex)
+    D[:, 0, 0], D[:, 1, 1] = d11, d22
+    D[:, 2, 2], D[:, 3, 3] = -np.conj(d11), -np.conj(d22)
+    return wn, D
+
+
+def fit_deck_2b():
+    """hybrid2bath on the test/2b deck with its fit options (test/2b/ED/ED.in:
+    fit_nw=200, fit_weight_power=1, fit_shift=0, weight_expo=2, dist_max=1e-12):
+    one bath level per orbital, started away from the answer."""
+    wn, D = _deck_2b()
+    b0 = StarBath(np.array([0.5, -0.4]), np.array([[0.5, 0.0], [0.0, 0.7]]))
+    return fit_hybrid(b0, D, wn, fit_nw=200, niter=400, dist_max=1e-12, fit_shift=0.0, power=1.0)
+
+
+def test_fit_recovers_the_2b_deck_bath():
+    """The deck's hybridisation is analytic, V^2 = 0.2 and 0.3 at level 0
+    (test/2b/test.py): the fit recovers that bath."""
+    b, d, it = fit_deck_2b()
+    assert d < 1e-12
+    assert np.abs(b.eps).max() < 1e-5
+    assert abs(b.V[0, 0] ** 2 - 0.2) < 1e-6 and abs(b.V[1, 1] ** 2 - 0.3) < 1e-6

@@ -112,3 +112,40 @@ def test_autograd_function_matches_the_direct_vjp(ctx):
     h, psi, e0v = _ground_state(ctx, m, (4, 4))
     ref, _, _ = h.grad_green(psi, e0v, prob.chains, 60, wn, gbar, prob.params, e0bar=0.3)
     assert np.abs(theta.grad.numpy() - ref).max() <= 1e-8 * np.abs(ref).max()
+
+
+def _oracle_loss(m, sec, chains, nit, wn, gbar, e0bar):
+    """E0 and the chains' G from the oracle alone: the exact ground state (dense
+    diagonalisation of the sector) and the oracle's FP64 compute_dynamic."""
+    ho = O.OracleH(m, *sec)
+    E, V = np.linalg.eigh(ho.dense())
+    e0, psi = float(E[0]), V[:, 0]
+    val = e0bar * e0
+    for c, (site, spin, dag) in enumerate(chains):
+        phi, ts = O.apply_c(m, *sec, site, spin, dag, psi)
+        G, _, _ = O.green_chain(O.OracleH(m, *ts), phi, nit, e0, 1 if dag else 2, wn, cutoff_dynamic=0.0)
+        val += float(np.sum((np.conj(gbar[c]) * G).real))
+    return val
+
+
+def test_grad_green_against_the_oracle_fp64_gradient(ctx):
+    """The device adjoint of E0 + G (one-orbital star, ns = 6, sector (3,3)) against
+    an FP64 reference gradient that involves no device code: central differences
+    (h = 1e-5) of the oracle's own solve (dense ground state, compute_dynamic
+    chains of 60 steps, 32 Matsubara points).  Bound 1e-6 of the largest
+    component."""
+    rng = np.random.default_rng(9)
+    m = star_model(-0.8, 2.0, rng.uniform(-1, 1, 5), rng.uniform(0.2, 0.6, 5))
+    sec = (3, 3)
+    params = edk.star_params(m)
+    chains = [(0, 0, True), (0, 0, False), (0, 1, True)]
+    nit = 60
+    wn = matsubara(30.0, 32)
+    gbar = rng.normal(size=(3, 32)) + 1j * rng.normal(size=(3, 32))
+    e0bar = 0.4
+    h, psi, e0 = _ground_state(ctx, m, sec)
+    grad, G, st = h.grad_green(psi, e0, chains, nit, wn, gbar, params, e0bar=e0bar, cg_tol=1e-13)
+    ref = np.array([(_oracle_loss(edk.perturb(m, p, H_FD), sec, chains, nit, wn, gbar, e0bar) -
+                     _oracle_loss(edk.perturb(m, p, -H_FD), sec, chains, nit, wn, gbar, e0bar)) / (2 * H_FD)
+                    for p in params])
+    assert np.abs(grad - ref).max() <= 1e-6 * np.abs(ref).max(), (grad, ref)
