@@ -37,7 +37,7 @@ WORKLOAD = dict(name="ns16_halffilled_E0_G512", nc=1, nb=15, sector=(8, 8), beta
 # measured on B200 with the library's start-vector table; used to convert a
 # per-step CPU time into solves/s for the reference arm.
 FP64_STEPS_PER_SOLVE = 1418
-PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "row_fast_kernel_step_ns16_f32.txt")
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "row_lean_kernel_step_ns16_9_8_f32.md")
 
 
 def _peaks():
@@ -297,7 +297,9 @@ def run_ours(args):
                        "l2": "vectors (662 MB FP32) exceed L2 (126 MB); no flush needed"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
-                         "traffic": traffic, "kernel": "row_fast_kernel<float> fused Lanczos step",
+                         "traffic": traffic,
+                         "kernel": "fused FP32 Lanczos step (row kernel timed per sector shape; "
+                                   "row_lean_kernel on the chain sectors)",
                          "launches": n6, "avg_launch_ms": (t6 / n6) if n6 else None,
                          "algorithmic_bytes_per_launch": (step_bytes / n6) if n6 else None},
             "cpu_baseline": cpu,
@@ -328,9 +330,9 @@ def run_kernel_case(args):
     sector = tuple(int(v) for v in args.kernel_sector.split(",")) if args.kernel_sector else WORKLOAD["sector"]
     h = edk.Hamiltonian(ctx, _model(), *sector)
     # one fixed launch shape (--kernel-shape, an index into the sector's list), no timing launches
+    ctx.set_fp32_sums(args.fp32_sums)
     shapes = h.launch_shapes("f32")
     ctx.set_kernel_path(16 + args.kernel_shape)
-    ctx.set_fp32_sums(args.fp32_sums)
     r = h.lanczos_e0(dtype="f32", nitermax=6, tolerance=0.0, check_every=6)
     torch.cuda.synchronize()
     print(json.dumps({"kernel_case": f"ns16 {sector} FP32 Lanczos", "dim": h.dim, "niter": r["niter"],

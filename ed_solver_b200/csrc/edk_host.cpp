@@ -310,7 +310,7 @@ struct edk_h {
     int hund = 0;
     // device copies
     struct SpinDev {
-        DevBuf ptr, tgt, val, diag, imp, move, ell, ell_val, pal;
+        DevBuf ptr, tgt, val, diag, imp, move, ell, ell_val, pal, lean, lean_kw;
     } sd[2];
     DevBuf int_off_d, int_coef_d, jj_d, umask_d, row_order_d;
     HamDev H;
@@ -360,6 +360,8 @@ int upload_spin(edk_h *h, int s)
     if ((rc = c->cuda(upload(d.ell, t.ell, st), "upload ell"))) return rc;
     if ((rc = c->cuda(upload(d.ell_val, t.ell_val, st), "upload ell_val"))) return rc;
     if ((rc = c->cuda(upload(d.pal, t.palette, st), "upload pal"))) return rc;
+    if ((rc = c->cuda(upload(d.lean, t.lean, st), "upload lean"))) return rc;
+    if ((rc = c->cuda(upload(d.lean_kw, t.lean_kw, st), "upload lean_kw"))) return rc;
     SpinTabDev &o = (s == 0) ? h->H.up : h->H.dn;
     o.ptr = d.ptr.as<int32_t>();
     o.tgt = d.tgt.as<int32_t>();
@@ -373,6 +375,9 @@ int upload_spin(edk_h *h, int s)
     o.ell = d.ell.as<uint32_t>();
     o.ell_val = d.ell_val.as<double>();
     o.pal = d.pal.as<double>();
+    o.lean_ks = t.lean.empty() ? 0 : t.lean_ks;
+    o.lean = t.lean.empty() ? nullptr : d.lean.as<uint32_t>();
+    o.lean_kw = t.lean.empty() ? nullptr : d.lean_kw.as<uint8_t>();
     return EDK_OK;
 }
 
@@ -437,6 +442,14 @@ RowArgs base_args(edk_h *h)
 // real launch then overwrites; the fastest is kept on the Hamiltonian.
 constexpr int kMaxShapes = 32;
 
+// FP32 hop sums for a launch of this sector and element type: FP32 vectors
+// of sectors at least as large as the context's threshold.
+int sum32_for(const edk_h *h, int dtype)
+{
+    const edk_ctx *c = h->ctx;
+    return dtype == EDK_F32 && c->fp32_sums && h->dim >= c->fp32_sums_min_dim && !h->sz ? 1 : 0;
+}
+
 // aligned: every vector of the call is aligned to twice the element size,
 // which the register-staged kernel (kind 0) needs; without it only the
 // bulk-copy kernel (kind 1) is a candidate, taken untimed and not remembered.
@@ -448,14 +461,14 @@ int fast_shape_for(edk_h *h, int dtype, const RowArgs &a, bool aligned, FastShap
     const int slot = dtype + 2 * a.sum32;
     if (c->kernel_path >= 16) {
         // a fixed candidate, for measurements
-        const int n = fast_shapes(h->H, eb, c->num_sms, cand, kMaxShapes);
+        const int n = fast_shapes(h->H, eb, c->num_sms, cand, kMaxShapes, a.sum32);
         if (n == 0) return c->fail(EDK_ERR_INVALID, "fast row kernel: no launch shape");
         out = cand[(c->kernel_path - 16) % n];
         return EDK_OK;
     }
     if (h->fast_tuned[slot]) { out = h->fast_shape[slot]; return EDK_OK; }
     if (!aligned) {
-        const int n = fast_shapes(h->H, eb, c->num_sms, cand, kMaxShapes);
+        const int n = fast_shapes(h->H, eb, c->num_sms, cand, kMaxShapes, a.sum32);
         for (int i = 0; i < n; ++i)
             if (!shape_needs_pairs(cand[i].kind)) { out = cand[i]; return EDK_OK; }
         if (n == 0) return c->fail(EDK_ERR_INVALID, "fast row kernel: no launch shape");
@@ -472,7 +485,7 @@ int fast_shape_for(edk_h *h, int dtype, const RowArgs &a, bool aligned, FastShap
                 h->fast_tuned[slot] = true;
                 return EDK_OK;
             }
-    const int n = fast_shapes(h->H, eb, c->num_sms, cand, kMaxShapes);
+    const int n = fast_shapes(h->H, eb, c->num_sms, cand, kMaxShapes, a.sum32);
     if (n == 0) return c->fail(EDK_ERR_INVALID, "fast row kernel: no launch shape");
     out = cand[0];
     if (c->kernel_path != 0 || n == 1 || !a.x || !a.y) {
@@ -550,7 +563,7 @@ int rows(edk_h *h, int dtype, const RowArgs &a_in)
     const int eb = dtype == EDK_F64 ? 8 : 4;
     RowArgs a = a_in;
     // FP32 hop sums where the context allows them (FP32 vectors of large sectors)
-    a.sum32 = dtype == EDK_F32 && c->fp32_sums && h->dim >= c->fp32_sums_min_dim && !h->sz ? 1 : 0;
+    a.sum32 = sum32_for(h, dtype);
     LaunchCfg cfg;
     if (!h->sz) {
         cfg = plan_rows(h->H, eb, c->num_sms);
@@ -561,7 +574,7 @@ int rows(edk_h *h, int dtype, const RowArgs &a_in)
         // kinds 0, 2 and 3 need those aligned column pairs; kinds 1 and 4 read
         // single elements at any alignment
         FastShape any[kMaxShapes];
-        cfg.fast = c->kernel_path != 1 && fast_rows_ok(h->H, eb) && fast_shapes(h->H, eb, c->num_sms, any, kMaxShapes) > 0;
+        cfg.fast = c->kernel_path != 1 && fast_rows_ok(h->H, eb) && fast_shapes(h->H, eb, c->num_sms, any, kMaxShapes, a.sum32) > 0;
         if (cfg.fast) {
             int rc = fast_shape_for(h, dtype, a, aligned, cfg.fast_shape);
             if (rc) return rc;
@@ -1195,7 +1208,7 @@ int edk_h_create(edk_ctx *ctx, const edk_model *m, int nup, int ndn, edk_h **out
             const SpinTableHost &t = h->tab[s];
             b += (int64_t)(t.ptr.size() * 4 + t.tgt.size() * 4 + t.val.size() * 12 + t.diag.size() * 12 +
                            t.imp.size() + t.move.size() * 4 + t.ell.size() * 4 + t.ell_val.size() * 12 +
-                           t.palette.size() * 12);
+                           t.palette.size() * 12 + t.lean.size() * 4 + t.lean_kw.size());
         }
         b += (int64_t)(order.size() * 4 + h->int_coef.size() * 12 + h->int_off.size() * 4);
         ctx->h2d_bytes += b;
@@ -1367,7 +1380,7 @@ int edk_h_launch_shapes(const edk_h *h, int dtype, int32_t *desc, int32_t cap)
     if (!h || (dtype != EDK_F64 && dtype != EDK_F32) || cap < 0 || (cap > 0 && !desc)) return -1;
     if (h->sz) return 0;
     FastShape cand[kMaxShapes];
-    const int n = fast_shapes(h->H, dtype == EDK_F64 ? 8 : 4, h->ctx->num_sms, cand, kMaxShapes);
+    const int n = fast_shapes(h->H, dtype == EDK_F64 ? 8 : 4, h->ctx->num_sms, cand, kMaxShapes, sum32_for(h, dtype));
     for (int i = 0; i < n && i < cap; ++i) {
         desc[5 * i] = cand[i].r;
         desc[5 * i + 1] = cand[i].kmu;

@@ -36,6 +36,15 @@ struct SpinTabDev {
     const uint32_t *ell = nullptr;
     const double *ell_val = nullptr;
     const double *pal = nullptr;      // npal <= 256
+    // Copy for the lean FP32 kernel (kind 3): the lean_ks entries of
+    // column c contiguous at c*lean_ks + k (lean_ks = ell_k rounded up to an
+    // even count), each (target << 14) | (palette index << 3) (padding: the
+    // column itself, palette slot 0); lean_kw[j] = the largest hop count of
+    // columns [64j, 64j + 64).  Null when the table is not packed, dim is odd
+    // or at least 2^18.
+    int lean_ks = 0;
+    const uint32_t *lean = nullptr;
+    const uint8_t *lean_kw = nullptr;
 };
 
 // Everything a row kernel needs to evaluate (H x) for an element.
@@ -99,7 +108,10 @@ struct RowArgs {
 // need vectors aligned to twice the element size and even rows.  Block
 // variants: 0 = 512 threads x 1 block per SM, 1 = 256 x 2, 2 = 128 x 4,
 // 3 = 768 x 1 and 4 = 640 x 1 (kind 2).
-inline bool shape_needs_pairs(int kind) { return kind == 0 || kind == 2; }
+// kind 3: the lean FP32 kernel (edk_rows_lean.cuh), FP32 vectors with FP32
+// hop sums only; kmu is its table width lean_ks; variants 0 = 256 x 2
+// and 1 = 512 x 1; needs aligned column pairs.
+inline bool shape_needs_pairs(int kind) { return kind == 0 || kind == 2 || kind == 3; }
 struct FastShape {
     int r = 0, kmu = 0, kmd = 0, variant = 0, kind = 0;
 };
@@ -214,7 +226,8 @@ cudaError_t launch_rows(const HamDev &H, int dtype, const RowArgs &a, const Laun
                         cudaStream_t st);
 bool fast_rows_ok(const HamDev &H, int elem_bytes);
 // The feasible launch shapes of the fast kernel for H (the first is the default).
-int fast_shapes(const HamDev &H, int elem_bytes, int num_sms, FastShape *out, int cap);
+// sum32: FP32 vectors with FP32 hop sums, which adds the lean kernel's shapes.
+int fast_shapes(const HamDev &H, int elem_bytes, int num_sms, FastShape *out, int cap, int sum32 = 0);
 cudaError_t launch_rows_fast(const HamDev &H, int dtype, const RowArgs &a, int num_sms, const FastShape &s,
                              cudaStream_t st);
 cudaError_t launch_set_int(int *p, int v, cudaStream_t st);

@@ -2,6 +2,7 @@
 // The kernel itself is in edk_rows_fast.cuh.
 #include "edk_rows_fast.cuh"
 #include "edk_rows_tma.cuh"
+#include "edk_rows_lean.cuh"
 
 namespace edk {
 
@@ -42,7 +43,7 @@ bool fast_rows_ok(const HamDev &H, int elem_bytes)
            H.dup * H.ddn < (int64_t)1 << 31 && H.up.ell_k >= 0;
 }
 
-int fast_shapes(const HamDev &H, int elem_bytes, int num_sms, FastShape *out, int cap)
+int fast_shapes(const HamDev &H, int elem_bytes, int num_sms, FastShape *out, int cap, int sum32)
 {
     if (!fast_rows_ok(H, elem_bytes)) return 0;
     const int kmu = H.up.ell_k <= 8 ? 8 : 16;
@@ -94,12 +95,24 @@ int fast_shapes(const HamDev &H, int elem_bytes, int num_sms, FastShape *out, in
                 if (n < cap && feasible(r, variant >= 3 ? 0 : variant)) out[n++] = FastShape{r, ku, kd, variant, 2};
         }
     }
+    // kind 3, the lean FP32 kernel (FP32 hop sums only): two interleaved rows
+    // per block; 256 threads x 2 blocks or 512 x 1 per SM; down-row
+    // bounds 7, 8 and 9, lean table widths 8 and 10
+    if (elem_bytes == 4 && sum32 && H.up.lean && (H.dup % 2) == 0 && H.dn_kmax <= 9 &&
+        (H.up.lean_ks == 8 || H.up.lean_ks == 10) && (H.ddn + 1) / 2 >= num_sms) {
+        const int ks = H.up.lean_ks;   // the table's stride: instances 8 and 10
+        const int kd = H.dn_kmax <= 7 ? 7 : H.dn_kmax;
+        const int64_t smem = lean_smem_bytes(H.dup);
+        if (n < cap && 2 * smem + 16 * 1024 <= 228 * 1024) out[n++] = FastShape{2, ks, kd, 0, 3};
+        if (n < cap && smem + 8 * 1024 <= 228 * 1024) out[n++] = FastShape{2, ks, kd, 1, 3};
+    }
     return n;
 }
 
 cudaError_t launch_rows_fast(const HamDev &H, int dtype, const RowArgs &a, int num_sms, const FastShape &s,
                              cudaStream_t st)
 {
+    if (s.kind == 3) return dtype == EDK_F32 ? launch_lean_f32(H, a, num_sms, s, st) : cudaErrorInvalidValue;
     if (s.kind >= 1)
         return dtype == EDK_F64 ? launch_tma_f64(H, a, num_sms, s, st) : launch_tma_f32(H, a, num_sms, s, st);
     return dtype == EDK_F64 ? launch_fast_f64(H, a, num_sms, s, st) : launch_fast_f32(H, a, num_sms, s, st);

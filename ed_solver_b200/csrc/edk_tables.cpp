@@ -185,6 +185,26 @@ SpinTableHost build_spin_table(const ModelHost &m, int spin, int np, const std::
         }
     }
     if (packed) t.palette = pal;
+    // lean copy for the FP32 kernel: per column, the entries contiguous and
+    // pre-shifted (target << 14 | palette index << 3), the width rounded up to
+    // an even count; per 64-column block the largest hop count
+    if (spin == 0 && packed && dim % 2 == 0 && dim < (1 << 18) && kmax <= 16) {
+        const int ks = kmax + (kmax & 1);
+        t.lean_ks = ks;
+        t.lean.assign((size_t)ks * dim, 0);
+        t.lean_kw.assign((size_t)(dim + 63) / 64, 0);
+        for (int64_t i = 0; i < dim; ++i) {
+            const int n = t.ptr[i + 1] - t.ptr[i];
+            for (int k = 0; k < ks; ++k) {
+                const uint32_t e = k < kmax ? t.ell[(size_t)k * dim + i] : 0u;
+                const uint32_t tg = k < n ? (e & 0xFFFFFFu) : (uint32_t)i;
+                const uint32_t pi = k < n ? (e >> 24) : 0u;
+                t.lean[(size_t)i * ks + k] = (tg << 14) | (pi << 3);
+            }
+            uint8_t &w = t.lean_kw[(size_t)i / 64];
+            w = std::max<uint8_t>(w, (uint8_t)n);
+        }
+    }
     return t;
 }
 

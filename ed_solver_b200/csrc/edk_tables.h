@@ -23,6 +23,10 @@ struct SpinTableHost {
     std::vector<uint32_t> ell;
     std::vector<double> ell_val;
     std::vector<double> palette;
+    // lean copy for the FP32 kernel of kind 3 (see SpinTabDev::lean)
+    int lean_ks = 0;
+    std::vector<uint32_t> lean;
+    std::vector<uint8_t> lean_kw;
 };
 
 int64_t binom(int n, int k);

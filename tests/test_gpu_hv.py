@@ -213,3 +213,42 @@ def test_launch_shape_timed_once_per_sector_shape():
         assert c.launches - n2 > 1
     finally:
         c.close()
+
+
+@pytest.mark.parametrize("name,sec", [("c3", (7, 7)), ("c5", (9, 8)), ("c5", (8, 8))])
+def test_lean_kernel_fp32_sums(ctx, name, sec):
+    """The lean FP32 row kernel (kind 3: two rows staged interleaved by
+    column, packed FP32x2 FMAs) at each of its launch shapes: H*v of an
+    FP32-rounded input within 2e-6 of the largest element of the oracle's
+    FP64 H*v, and a 40-step Green chain whose Lanczos coefficients agree with
+    the FP64 chain's to 2e-5 relative (FP32 vectors and hop sums against
+    FP64 throughout)."""
+    import torch
+    m = workload(name).model
+    ctx.set_fp32_sums(True, 1)
+    try:
+        h = edk.Hamiltonian(ctx, m, *sec)
+        shapes = h.launch_shapes("f32")
+        lean = [i for i, sh in enumerate(shapes) if sh["kind"] == 3]
+        assert lean, shapes
+        rng = np.random.default_rng(5)
+        x = rng.normal(size=h.dim).astype(np.float32)
+        y = O.OracleH(m, *sec).hmult(x.astype(np.float64))
+        xf = torch.tensor(x, device="cuda")
+        ctx.set_kernel_path(0)
+        start = torch.tensor(rng.normal(size=h.dim), device="cuda")
+        wn = np.pi / 50.0 * (2 * np.arange(16) + 1)
+        G64, a64, b64, n64 = h.green_chain(start, 40, 0.0, 1, wn)
+        for i in lean:
+            ctx.set_kernel_path(16 + i)
+            yf = h.hmult(xf).double().cpu().numpy()
+            assert np.abs(yf - y).max() <= 2e-6 * np.abs(y).max(), (sec, shapes[i])
+            G32, a32, b32, n32 = h.green_chain(start.to(torch.float32), 40, 0.0, 1, wn)
+            assert n32 == n64 == 40
+            scale = np.abs(a64).max() + np.abs(b64).max()
+            assert np.abs(a32 - a64).max() <= 2e-5 * scale, (sec, shapes[i], np.abs(a32 - a64).max())
+            assert np.abs(b32 - b64).max() <= 2e-5 * scale, (sec, shapes[i], np.abs(b32 - b64).max())
+            assert np.abs(G32 - G64).max() <= 2e-5 * np.abs(G64).max()
+    finally:
+        ctx.set_kernel_path(0)
+        ctx.set_fp32_sums(False)
