@@ -313,6 +313,9 @@ struct edk_h {
         DevBuf ptr, tgt, val, diag, imp, move, ell, ell_val, pal, lean, lean_kw;
     } sd[2];
     DevBuf int_off_d, int_coef_d, jj_d, umask_d, row_order_d;
+    // density terms of the split form (HAIMupdo_multr_split), built on first use
+    DevBuf split_off_d, split_coef_d;
+    bool split_ready = false;
     HamDev H;
     // apply_c maps keyed by (spin, dagger, site)
     struct CMap {
@@ -1426,6 +1429,39 @@ int edk_hmult(edk_h *h, int dtype, int64_t n, const void *x_dev, void *y_dev)
     a.x = x_dev;
     a.y = y_dev;
     return rows(h, dtype, a);
+}
+
+int edk_hmult_split(edk_h *h, int dtype, int64_t n, const void *x_dev, void *y_dev)
+{
+    if (!h || !x_dev || !y_dev || (dtype != EDK_F64 && dtype != EDK_F32)) return EDK_ERR_INVALID;
+    edk_ctx *c = h->ctx;
+    if (n != h->dim) return c->fail(EDK_ERR_INVALID, "n=%lld differs from the sector dimension %lld",
+                                    (long long)n, (long long)h->dim);
+    if (x_dev == y_dev) return c->fail(EDK_ERR_INVALID, "x and y must not alias");
+    if (h->sz) return c->fail(EDK_ERR_UNSUPPORTED, "the split H*v is for (N_up, N_dn) sectors");
+    // the reference STOPs here (HAIMupdo.f90:1243-1246)
+    if (std::fabs(h->model.jhund) > 1e-5)
+        return c->fail(EDK_ERR_UNSUPPORTED, "Jhund not implemented in the split H*v (|Jhund| > 1e-5)");
+    int rc;
+    if (!h->split_ready) {
+        std::vector<int32_t> off;
+        std::vector<double> coef;
+        density_terms(h->model, off, coef, false);
+        if ((rc = c->cuda(upload(h->split_off_d, off, c->stream), "upload split terms"))) return rc;
+        if ((rc = c->cuda(upload(h->split_coef_d, coef, c->stream), "upload split terms"))) return rc;
+        h->split_ready = true;
+    }
+    // two workspace vectors that are neither x nor y hold the transposes
+    void *w[5];
+    if ((rc = work_ptrs(h, dtype, w))) return rc;
+    void *sc[2];
+    int ns = 0;
+    for (int i = 0; i < 5 && ns < 2; ++i)
+        if (w[i] != x_dev && w[i] != y_dev) sc[ns++] = w[i];
+    cudaError_t e = launch_split_hv(h->H, dtype, h->split_off_d.as<int32_t>(), h->split_coef_d.as<double>(), x_dev,
+                                    y_dev, sc[0], sc[1], c->num_sms, c->stream);
+    c->launches += 5;   // up pass, two transposes, down pass, transpose back
+    return c->cuda(e, "split H*v");
 }
 
 int edk_hmult_host(edk_h *h, int dtype, int64_t n, const void *x_host, void *y_host)

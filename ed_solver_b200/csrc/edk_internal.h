@@ -220,6 +220,12 @@ struct SzOp {
 cudaError_t launch_sz_apply_c(int dtype, const SzDev &src, const SzSectorDev &tgt, int nop, const SzOp *ops,
                               const void *in, void *out, int num_sms, cudaStream_t st);
 
+// HAIMupdo_multr_split (edk_split.cu): y = H x through two transposes; xt, yt
+// are scratch vectors of the sector's dimension; soff/scoef the split form's
+// density terms per impurity-configuration pair (no -JJ terms).
+cudaError_t launch_split_hv(const HamDev &H, int dtype, const int32_t *soff, const double *scoef, const void *x,
+                            void *y, void *xt, void *yt, int num_sms, cudaStream_t st);
+
 // ---- kernel launchers (edk_kernels.cu) ------------------------------------
 LaunchCfg plan_rows(const HamDev &H, int elem_bytes, int num_sms);
 cudaError_t launch_rows(const HamDev &H, int dtype, const RowArgs &a, const LaunchCfg &cfg,

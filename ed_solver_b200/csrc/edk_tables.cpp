@@ -212,8 +212,9 @@ SpinTableHost build_spin_table(const ModelHost &m, int spin, int np, const std::
 // (HAIMupdo.f90:784-829): U(c,c) for doubly occupied sites, then for each
 // pair c1<c2 with U(c1,c2) != 0 and both sites occupied: U*n1*n2, -JJ for an
 // up-up pair, -JJ for a down-down pair.  The second group only exists when U
-// has an off-diagonal element.
-void density_terms(const ModelHost &m, std::vector<int32_t> &off, std::vector<double> &coef)
+// has an off-diagonal element.  with_jj = false gives the terms of
+// HAIMupdo_multr_split (HAIMupdo.f90:1250-1284), which has no -JJ terms.
+void density_terms(const ModelHost &m, std::vector<int32_t> &off, std::vector<double> &coef, bool with_jj)
 {
     const int nc = m.nc, ncfg = 1 << nc;
     bool offc = false;
@@ -236,8 +237,8 @@ void density_terms(const ModelHost &m, std::vector<int32_t> &off, std::vector<do
                         const int u2 = (cu >> s2) & 1, d2 = (cd >> s2) & 1;
                         if (u2 + d2 == 0) continue;
                         coef.push_back(m.u[s1 * nc + s2] * (double)(u1 + d1) * (double)(u2 + d2));
-                        if (u1 && u2) coef.push_back(-m.jj[s1 * nc + s2]);
-                        if (d1 && d2) coef.push_back(-m.jj[s1 * nc + s2]);
+                        if (with_jj && u1 && u2) coef.push_back(-m.jj[s1 * nc + s2]);
+                        if (with_jj && d1 && d2) coef.push_back(-m.jj[s1 * nc + s2]);
                     }
                 }
             off[(size_t)cu * ncfg + cd + 1] = (int32_t)coef.size();

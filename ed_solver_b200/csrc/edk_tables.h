@@ -33,7 +33,7 @@ int64_t binom(int n, int k);
 std::vector<uint64_t> enumerate_states(int ns, int np);
 std::vector<int32_t> rank_table(int ns);
 SpinTableHost build_spin_table(const ModelHost &m, int spin, int np, const std::vector<int32_t> &rank);
-void density_terms(const ModelHost &m, std::vector<int32_t> &off, std::vector<double> &coef);
+void density_terms(const ModelHost &m, std::vector<int32_t> &off, std::vector<double> &coef, bool with_jj = true);
 std::vector<int32_t> row_schedule(const std::vector<uint64_t> &states, int nc, int nb);
 
 }  // namespace edk

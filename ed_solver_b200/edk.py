@@ -203,6 +203,7 @@ def lib():
         "edk_h_table": (C.c_int, [P, C.c_int, P, P, P, P, P]),
         "edk_hmult": (C.c_int, [P, C.c_int, I64, P, P]),
         "edk_hmult_host": (C.c_int, [P, C.c_int, I64, P, P]),
+        "edk_hmult_split": (C.c_int, [P, C.c_int, I64, P, P]),
         "edk_lanczos_e0": (C.c_int, [P, P, P]),
         "edk_lanczos_gs": (C.c_int, [P, P, I32, P, P]),
         "edk_apply_c": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, P, P]),
@@ -473,6 +474,17 @@ class Hamiltonian:
         x = x.contiguous()
         y = torch.empty_like(x) if out is None else out
         self.ctx.check(lib().edk_hmult(self.h, code, self.dim, _ptr(x), _ptr(y)), "edk_hmult")
+        return y
+
+    def hmult_split(self, x, out=None):
+        """HAIMupdo_multr_split (HAIMupdo.f90:1221-1347): y = H x through two
+        transposes, without the -JJ density terms; raises where the reference
+        STOPs (|Jhund| > 1e-5)."""
+        import torch
+        code = _dtype_code(x.dtype)
+        x = x.contiguous()
+        y = torch.empty_like(x) if out is None else out
+        self.ctx.check(lib().edk_hmult_split(self.h, code, self.dim, _ptr(x), _ptr(y)), "edk_hmult_split")
         return y
 
     def hmult_host(self, x: np.ndarray) -> np.ndarray:

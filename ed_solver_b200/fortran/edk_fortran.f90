@@ -161,6 +161,13 @@ module edk_fortran
       integer(c_int64_t), value :: n
       type(c_ptr), value :: x, y
     end function
+    integer(c_int) function edk_hmult_split(h, dtype, n, x, y) bind(C, name="edk_hmult_split")
+      import :: c_int, c_ptr, c_int64_t
+      type(c_ptr), value :: h
+      integer(c_int), value :: dtype
+      integer(c_int64_t), value :: n
+      type(c_ptr), value :: x, y
+    end function
     integer(c_int) function edk_hmult_host(h, dtype, n, x, y) bind(C, name="edk_hmult_host")
       import :: c_int, c_ptr, c_int64_t, c_double
       type(c_ptr), value :: h

@@ -162,6 +162,16 @@ int edk_h_table(const edk_h *h, int spin, int64_t *nnz, int64_t *ptr_host,
 int edk_hmult(edk_h *h, int dtype, int64_t n, const void *x_dev, void *y_dev);
 /* Same on host buffers: copies in, multiplies, copies out (synchronous). */
 int edk_hmult_host(edk_h *h, int dtype, int64_t n, const void *x_host, void *y_host);
+/* HAIMupdo_multr_split (HAIMupdo.f90:1221-1347, the matvec Hmultr calls under
+ * USE_TRANSPOSE_TRICK_MPI, H_class.f90:115-119) on one GPU: the U(c,c) and
+ * U(c1,c2) n1 n2 density terms (no -JJ terms, unlike edk_hmult), the
+ * diagonal and the up hops; then x and the partial y are transposed, the down
+ * hops are applied as up hops of the transposed arrays, and y is transposed
+ * back.  Two of the context's Krylov workspace vectors hold the transposes
+ * (x and y may be workspace vectors).  EDK_ERR_UNSUPPORTED where the reference
+ * STOPs (|Jhund| > 1e-5) and for Nambu sectors.  FP64: bit-identical to a
+ * sequential FP64 evaluation in the reference's order. */
+int edk_hmult_split(edk_h *h, int dtype, int64_t n, const void *x_dev, void *y_dev);
 
 /* ---- Lanczos (Lanczos_plain.f90:33-229, Lanczos_plain.h:66-173) --------- */
 typedef struct edk_lanczos_opts {

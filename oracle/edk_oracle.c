@@ -479,6 +479,90 @@ void orc_hmult(const orc_h *h, const double *x, double *y)
         }
 }
 
+/* Out-of-place transpose of an nrow x ncol array stored with the column index
+ * fastest (a[c + r*ncol]) into b[r + c*nrow] (distributed_memory_transpose_mat
+ * of one process, HAIMupdo.f90:1305-1306). */
+static void transpose_mat(const double *a, double *b, int64_t ncol, int64_t nrow)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t r = 0; r < nrow; ++r)
+        for (int64_t c = 0; c < ncol; ++c) b[r + c * nrow] = a[c + r * ncol];
+}
+
+/* HAIMupdo_multr_split (HAIMupdo.f90:1221-1347) on one process: U(c,c) terms,
+ * U(c1,c2) n1 n2 terms (no -JJ terms, unlike HAIMupdo_multr), the diagonal,
+ * the up hops; then both vectors transposed, the down hops applied as up hops
+ * of the transposed array, and both transposed back.  Returns -1 where the
+ * reference STOPs (|Jhund| > 1e-5, :1243-1246), 0 otherwise. */
+int orc_hmult_split(const orc_h *h, const double *x, double *y)
+{
+    if (h->sz || fabs(h->jhund) > 1e-5) return -1;
+    const int nc = h->nc, nb = h->nb;
+    const int64_t sec = h->dup, ddn = h->ddn, n = h->dim;
+    const orc_spin_table *tu = &h->t[0], *td = &h->t[1];
+    memset(y, 0, sizeof(double) * (size_t)n);
+    /* :1250-1261 */
+#pragma omp parallel for schedule(static)
+    for (int64_t iup = 0; iup < sec; ++iup)
+        for (int c = 0; c < nc; ++c) {
+            if (!(h->umask[c * nc + c] && bt(tu->st[iup], nb + c))) continue;
+            for (int64_t ido = 0; ido < ddn; ++ido)
+                if (bt(td->st[ido], nb + c)) {
+                    int64_t i = iup + ido * sec;
+                    y[i] = y[i] + h->u[c * nc + c] * x[i];
+                }
+        }
+    /* :1263-1284 */
+    if (h->offdiag_coulomb) {
+#pragma omp parallel for schedule(static)
+        for (int64_t iup = 0; iup < sec; ++iup)
+            for (int64_t ido = 0; ido < ddn; ++ido)
+                for (int s1 = 0; s1 < nc - 1; ++s1) {
+                    int n1 = bt(tu->st[iup], nb + s1) + bt(td->st[ido], nb + s1);
+                    if (n1 == 0) continue;
+                    for (int s2 = s1 + 1; s2 < nc; ++s2) {
+                        if (!h->umask[s1 * nc + s2]) continue;
+                        int n2 = bt(tu->st[iup], nb + s2) + bt(td->st[ido], nb + s2);
+                        if (n2 == 0) continue;
+                        int64_t i = iup + ido * sec;
+                        y[i] = y[i] + h->u[s1 * nc + s2] * (double)n1 * (double)n2 * x[i];
+                    }
+                }
+    }
+    /* :1286-1292 */
+#pragma omp parallel for schedule(static)
+    for (int64_t iup = 0; iup < sec; ++iup)
+        for (int64_t ido = 0; ido < ddn; ++ido) {
+            int64_t i = iup + ido * sec;
+            y[i] = y[i] + (tu->diag[iup] + td->diag[ido]) * x[i];
+        }
+    /* :1294-1311 */
+#pragma omp parallel for schedule(static)
+    for (int64_t iup = 0; iup < sec; ++iup)
+        for (int64_t e = tu->ptr[iup]; e < tu->ptr[iup + 1]; ++e) {
+            double hv = tu->val[e];
+            int64_t jup = tu->tgt[e];
+            for (int64_t ido = 0; ido < ddn; ++ido) y[iup + ido * sec] = y[iup + ido * sec] + hv * x[jup + ido * sec];
+        }
+    /* :1313-1314, then the down hops of the transposed arrays (:1316-1334) */
+    double *xt = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+    double *yt = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+    transpose_mat(x, xt, sec, ddn);
+    transpose_mat(y, yt, sec, ddn);
+#pragma omp parallel for schedule(static)
+    for (int64_t ido = 0; ido < ddn; ++ido)
+        for (int64_t e = td->ptr[ido]; e < td->ptr[ido + 1]; ++e) {
+            double hv = td->val[e];
+            int64_t jdo = td->tgt[e];
+            for (int64_t iup = 0; iup < sec; ++iup) yt[ido + iup * ddn] = yt[ido + iup * ddn] + hv * xt[jdo + iup * ddn];
+        }
+    /* :1336-1337 */
+    transpose_mat(yt, y, ddn, sec);
+    free(xt);
+    free(yt);
+    return 0;
+}
+
 /* ------------------------------------------------------------------------- */
 /* symmetric tridiagonal eigensolver (stands in for LAPACK DSTEDC,            */
 /* matrices_tridiag.f90:210-259): implicit QL with Wilkinson shifts.          */

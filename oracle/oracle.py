@@ -70,6 +70,8 @@ def lib():
         L.orc_h_table.restype = i64
         L.orc_h_table.argtypes = [P, i32, P, P, P, P, P]
         L.orc_hmult.argtypes = [P, P, P]
+        L.orc_hmult_split.argtypes = [P, P, P]
+        L.orc_hmult_split.restype = C.c_int
         L.orc_tridiag_eig.restype = i32
         L.orc_tridiag_eig.argtypes = [i32, P, P, P, P]
         L.orc_fix_initial_vector.argtypes = [i64, P, P]
@@ -167,6 +169,16 @@ class OracleH:
         x = np.ascontiguousarray(x, dtype=np.float64)
         y = np.empty(self.dim, dtype=np.float64)
         lib().orc_hmult(self.h, _p(x), _p(y))
+        return y
+
+    def hmult_split(self, x: np.ndarray) -> np.ndarray:
+        """HAIMupdo_multr_split (HAIMupdo.f90:1221-1347): up hops, transpose,
+        down hops as up hops, transpose back; no -JJ density terms.  None where
+        the reference STOPs (|Jhund| > 1e-5)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(self.dim, dtype=np.float64)
+        if lib().orc_hmult_split(self.h, _p(x), _p(y)) != 0:
+            return None
         return y
 
     def table(self, spin: int):

@@ -252,3 +252,54 @@ def test_lean_kernel_fp32_sums(ctx, name, sec):
     finally:
         ctx.set_kernel_path(0)
         ctx.set_fp32_sums(False)
+
+
+def _jj_model():
+    """Two orbitals with U' and a density-density J (JJ) but no Hund spin-flip
+    or pair-hop coupling (Jhund = 0): the split form applies (the reference
+    STOPs in it only for |Jhund| > 1e-5) and differs from HAIMupdo_multr by
+    the missing -JJ terms."""
+    rng = np.random.default_rng(31)
+    m = star_model(-1.0, 3.0, rng.uniform(-1, 1, 4), rng.uniform(0.2, 0.6, 4), orbital_of_bath=[0, 1, 1, 0],
+                   nc=2, J=0.5)
+    m.ec[:, 0, 1] = m.ec[:, 1, 0] = 0.3
+    m.jhund = 0.0
+    return m
+
+
+@pytest.mark.parametrize("name,sec", [("c1", (4, 4)), ("c1", (3, 5)), ("jj", (3, 3)), ("jj", (2, 4)),
+                                      ("c5", (8, 8))])
+def test_hmult_split_fp64_bit_exact(ctx, name, sec):
+    """edk_hmult_split (HAIMupdo_multr_split) against the oracle's restatement
+    of the split form, bit for bit in FP64 (the ns=16 sector included); equal
+    to edk_hmult where the model has no -JJ terms, different where it has."""
+    import torch
+    m = _jj_model() if name == "jj" else workload(name).model
+    h = edk.Hamiltonian(ctx, m, *sec)
+    ho = O.OracleH(m, *sec)
+    x = np.random.default_rng(41).normal(size=h.dim)
+    xd = torch.tensor(x, device="cuda")
+    y = h.hmult_split(xd).cpu().numpy()
+    y_ref = ho.hmult_split(x)
+    assert np.array_equal(y, y_ref), np.abs(y - y_ref).max()
+    if name == "jj":
+        assert not np.array_equal(y, ho.hmult(x))
+    else:
+        assert np.array_equal(y, h.hmult(xd).cpu().numpy())
+    # FP32 vectors: FP64 accumulation, the pass-1 partial sums stored in FP32
+    xf = xd.to(torch.float32)
+    yf = h.hmult_split(xf).double().cpu().numpy()
+    y32 = ho.hmult_split(x.astype(np.float32).astype(np.float64))
+    assert np.abs(yf - y32).max() <= 2.5e-7 * np.abs(y32).max()
+
+
+def test_hmult_split_rejects_hund_models(ctx):
+    """The reference STOPs in the split form when |Jhund| > 1e-5; the library
+    returns EDK_ERR_UNSUPPORTED (and the oracle None)."""
+    import torch
+    m = workload("c2").model
+    h = edk.Hamiltonian(ctx, m, 5, 5)
+    assert O.OracleH(m, 5, 5).hmult_split(np.zeros(h.dim)) is None
+    with pytest.raises(edk.EdkError) as e:
+        h.hmult_split(torch.zeros(h.dim, dtype=torch.float64, device="cuda"))
+    assert e.value.code == edk.EDK_ERR_UNSUPPORTED

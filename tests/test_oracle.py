@@ -33,6 +33,31 @@ def test_hmult_matches_second_quantised_build(mi):
         assert np.abs(A - A.T).max() == 0.0
 
 
+def test_split_form_is_the_matvec_without_the_jj_terms():
+    """The restatement of HAIMupdo_multr_split (transposes, no -JJ terms)
+    equals the restatement of HAIMupdo_multr with JJ set to zero, bit for bit,
+    on a two-orbital model without Hund spin-flip terms; on a single-orbital
+    model it equals the plain matvec; with |Jhund| > 1e-5 the reference STOPs
+    (None)."""
+    import dataclasses
+    m = _models()[1]
+    m.jhund = 0.0
+    m0 = dataclasses.replace(m, jj=np.zeros_like(m.jj))
+    rng = np.random.default_rng(4)
+    for nu, nd in [(2, 2), (3, 2), (1, 3), (0, 2)]:
+        x = rng.normal(size=O.OracleH(m, nu, nd).dim)
+        ys = O.OracleH(m, nu, nd).hmult_split(x)
+        assert np.array_equal(ys, O.OracleH(m0, nu, nd).hmult(x))
+    h = O.OracleH(m, 2, 2)
+    x = rng.normal(size=h.dim)
+    assert not np.array_equal(h.hmult_split(x), h.hmult(x))
+    m1 = _models()[0]
+    h = O.OracleH(m1, 2, 3)
+    x = rng.normal(size=h.dim)
+    assert np.array_equal(h.hmult_split(x), h.hmult(x))
+    assert O.OracleH(_models()[1], 2, 2).hmult_split(np.zeros(O.OracleH(_models()[1], 2, 2).dim)) is None
+
+
 def test_tridiagonal_solver_against_numpy():
     rng = np.random.default_rng(3)
     for n in (1, 2, 5, 40):
