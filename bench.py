@@ -405,6 +405,89 @@ def run_grad(args):
     ctx.close()
 
 
+def run_configs(args):
+    """The smaller configurations as measured records, one JSON line each:
+    C1 (ns=8, FP64, ground state to |r| < 1e-12, 1024 Matsubara points,
+    200-step chains), C2 (ns=10 Kanamori, all 121 sectors, FP32 Krylov in
+    every sector of at least 1000 states beside the FP64 solve: errors in E0,
+    double occupancy and G at 512 points, beta = 40) and C3 (ns=14 (7,7):
+    H*v and fused-step GB/s in both precisions, mixed against FP64 solve time
+    and accuracy, four 300-step chains).  Solve times are wall-clock over one
+    solve after a warm-up solve; kernel times are CUDA events."""
+    import numpy as np
+    import torch
+    from ed_solver_b200 import edk
+    from ed_solver_b200.model import workload
+    peak, peak_kind = _peaks()
+    ctx = edk.Context(0)
+
+    def timed_solve(*a, **k):
+        edk.solve(ctx, *a, **k)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = edk.solve(ctx, *a, **k)
+        torch.cuda.synchronize()
+        return r, time.perf_counter() - t0
+
+    # ---- C1 ----
+    w = workload("c1")
+    r, t = timed_solve(w.model, w.sectors, w.beta, w.nw, dtype="f64", nitergreen=w.nitergreen, spins=(0, 1),
+                       pairs=[(0, 0)], tolerance=1e-14, residual_tol=1e-12)
+    print(json.dumps({"config": "C1 ns=8 (4,4) FP64", "solve_s": t, "e0": r["e0"], "residual": r["residual"],
+                      "nw": w.nw, "nitergreen": w.nitergreen, "lanczos_steps": r["lanczos_steps"],
+                      "green_steps": r["green_steps"]}), flush=True)
+    # ---- C2 ----
+    w = workload("c2")
+    kw = dict(neigen=1, nitergreen=w.nitergreen, spins=(0, 1), pairs=[(0, 0), (1, 1)], tolerance=1e-12)
+    r64, t64 = timed_solve(w.model, w.sectors, w.beta, w.nw, dtype="f64", **kw)
+    r32, t32 = timed_solve(w.model, w.sectors, w.beta, w.nw, dtype="f32", lowprec_min_dim=1000, **kw)
+    print(json.dumps({"config": "C2 ns=10 Kanamori, 121 sectors, FP32 Krylov in sectors >= 1000 states",
+                      "solve_s_fp64": t64, "solve_s_mixed": t32,
+                      "rel_dE0": abs(r32["e0"] - r64["e0"]) / abs(r64["e0"]),
+                      "max_abs_ddocc": float(np.abs(r32["docc"] - r64["docc"]).max()),
+                      "max_abs_dG": float(np.abs(r32["G"] - r64["G"]).max()), "nw": w.nw, "beta": w.beta,
+                      "nstates": r64["nstates"]}), flush=True)
+    # ---- C3 ----
+    w = workload("c3")
+    h = edk.Hamiltonian(ctx, w.model, *w.sectors[0])
+    rec = {"config": "C3 ns=14 (7,7)", "dim": h.dim, "peak_hbm_gbs": peak, "peak": peak_kind}
+    for dt, eb, s32 in (("f64", 8, False), ("f32", 4, False), ("f32", 4, True)):
+        tdt = torch.float64 if dt == "f64" else torch.float32
+        ctx.set_fp32_sums(s32, 1)
+        x = torch.randn(h.dim, dtype=tdt, device="cuda")
+        y = torch.empty_like(x)
+        for _ in range(3):
+            h.hmult(x, out=y)
+        torch.cuda.synchronize()
+        ctx.timing(True)
+        for _ in range(10):
+            h.hmult(x, out=y)
+        torch.cuda.synchronize()
+        n, ms, _ = ctx.timing_report(0 if dt == "f64" else 4)
+        ctx.timing(False)
+        ctx.timing(True)
+        h.lanczos_e0(dtype=dt, nitermax=40, tolerance=0.0, check_every=40)
+        torch.cuda.synchronize()
+        ns_, mss, _ = ctx.timing_report(2 if dt == "f64" else 6)
+        ctx.timing(False)
+        key = dt + ("_fp32sums" if s32 else "")
+        t_hv, t_st = ms / max(n, 1), mss / max(ns_, 1)
+        rec["hv_" + key] = {"ms": t_hv, "gbs": 2 * eb * h.dim / (t_hv * 1e6), "frac": 2 * eb * h.dim / (t_hv * 1e6) / peak}
+        rec["step_" + key] = {"ms": t_st, "gbs": 3 * eb * h.dim / (t_st * 1e6), "frac": 3 * eb * h.dim / (t_st * 1e6) / peak}
+        del x, y
+    ctx.set_fp32_sums(False)
+    h.close()
+    kw = dict(neigen=1, nitergreen=w.nitergreen, spins=(0, 1), pairs=[(0, 0)], tolerance=1e-12, residual_tol=1e-9)
+    r64, t64 = timed_solve(w.model, w.sectors, w.beta, w.nw, dtype="f64", **kw)
+    r32, t32 = timed_solve(w.model, w.sectors, w.beta, w.nw, dtype="f32", fp32_sums=True, **kw)
+    rec.update({"solve_s_fp64": t64, "solve_s_mixed": t32, "speedup_mixed_vs_fp64": t64 / t32,
+                "rel_dE0": abs(r32["e0"] - r64["e0"]) / abs(r64["e0"]),
+                "max_abs_dG": float(np.abs(r32["G"] - r64["G"]).max()),
+                "max_abs_ddocc": float(np.abs(r32["docc"] - r64["docc"]).max())})
+    print(json.dumps(rec), flush=True)
+    ctx.close()
+
+
 def run_c4(args):
     """The many-small-sectors workload: two-orbital Kanamori model, ns = 12
     (169 sectors, dims up to 924^2), 3 lowest states per sector inside the
@@ -617,6 +700,7 @@ def main():
                     help="time the 32 parameter gradients of E0 + G and check them by central differences")
     ap.add_argument("--grad-fd", type=int, default=4, help="parameters checked by central differences (--grad)")
     ap.add_argument("--c4", action="store_true", help="time the many-small-sectors solve, batched vs per chain")
+    ap.add_argument("--configs", action="store_true", help="measured records of the C1, C2 and C3 configurations")
     ap.add_argument("--sz", action="store_true", help="time H*v and fused steps of Nambu (Sz) sectors")
     ap.add_argument("--sz-case", action="store_true", help="three Nambu H*v launches (profiling case)")
     ap.add_argument("--chiloc", action="store_true", help="time the local vertex against the reference kernel")
@@ -638,6 +722,9 @@ def main():
         return
     if args.c4:
         run_c4(args)
+        return
+    if args.configs:
+        run_configs(args)
         return
     if args.grad:
         run_grad(args)

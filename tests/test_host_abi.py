@@ -39,6 +39,36 @@ def test_fortran_module_binds_every_declared_symbol():
     assert bound == declared_symbols(), (declared_symbols() - bound, bound - declared_symbols())
 
 
+def _header_arity():
+    """Number of parameters of every declared entry point."""
+    out = {}
+    for f in os.listdir(os.path.join(ROOT, "include")):
+        if not f.endswith(".h"):
+            continue
+        txt = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", f)).read(), flags=re.S)
+        for name, args in re.findall(r"(?:^|\n)\s*(?:int|int64_t|const char \*)\s*\**(edk_\w+)\s*\(([^;]*?)\)\s*;",
+                                     txt, re.S):
+            a = args.strip()
+            out[name] = 0 if a in ("", "void") else a.count(",") + 1
+    return out
+
+
+def test_fortran_interfaces_have_the_c_argument_counts():
+    """Each bind(C) interface of the Fortran module declares as many dummy
+    arguments as the C prototype has parameters."""
+    f90 = open(os.path.join(ROOT, "ed_solver_b200", "fortran", "edk_fortran.f90")).read()
+    f90 = re.sub(r"&\s*\n\s*&?", " ", f90)
+    fort = {}
+    for name, args, cname in re.findall(r"(?:function|subroutine)\s+(edk_\w+)\s*\(([^)]*)\)\s*bind\(C,\s*name=\"(edk_\w+)\"\)",
+                                        f90, re.I):
+        a = args.strip()
+        fort[cname] = 0 if not a else a.count(",") + 1
+    arity = _header_arity()
+    assert set(arity) == declared_symbols()
+    bad = {k: (arity[k], fort.get(k)) for k in arity if fort.get(k) != arity[k]}
+    assert not bad, bad
+
+
 def test_basis_and_rank_bit_exact():
     for ns in (1, 4, 8, 11, 16):
         for np_ in range(ns + 1):
