@@ -493,27 +493,59 @@ def run_c4(args):
     (169 sectors, dims up to 924^2), 3 lowest states per sector inside the
     exp(-beta (E - E0)) >= 1e-8 window, 8 Green start vectors per state
     (2 spins x particle/hole x 2 orbitals), 200-step chains, 512 Matsubara
-    points, FP64.  Times one solve with the chains batched into one persistent
-    launch per spin against one launch per chain step."""
+    points, FP64.  Times the solve sector by sector and chain by chain against
+    the chains batched into one persistent launch per spin and against the
+    ground states of the sectors below a size bound batched into two
+    persistent launches; the eigen part alone and the whole solve."""
     import torch
     from ed_solver_b200 import edk
     from ed_solver_b200.model import workload
     w = workload("c4")
     ctx = edk.Context(0)
     out = {"workload": "c4_ns12_kanamori_all_sectors", "sectors": len(w.sectors)}
-    for mode in (1, 0, 1, 0):
+    # (green_mode, batch_gs): per sector and per chain / chains batched / ground
+    # states of sectors up to 2^12, 2^14, 2^16 states batched; the eigen part
+    # alone (no Green chains) and the whole solve, median of 3 runs after one
+    # warm-up run of each
+    import numpy as np
+    modes = {"per_sector": (1, 0), "batched_chains": (0, 0), "batched_gs_4096": (1, 4096),
+             "batched_gs_16384": (1, 16384), "batched_gs_65536": (1, 65536)}
+
+    def run(gm, bg, spins):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         r = edk.solve(ctx, w.model, w.sectors, w.beta, 512, dtype="f64", neigen=3, nitergreen=200,
-                      demax0=w.demax0, spins=(0, 1), pairs=[(0, 0), (1, 1)], tolerance=1e-10, green_mode=mode)
+                      demax0=w.demax0, spins=spins, pairs=[(0, 0), (1, 1)], tolerance=1e-10, green_mode=gm,
+                      batch_gs=bg)
         torch.cuda.synchronize()
-        key = "batched" if mode == 0 else "per_chain"
-        out[key] = {"solve_s": time.perf_counter() - t0, "nstates": r["nstates"],
-                    "green_steps": r["green_steps"], "lanczos_steps": r["lanczos_steps"]}
-        out.setdefault("G_" + key, r["G"])
-    import numpy as np
-    out["max_abs_dG_batched_vs_per_chain"] = float(np.abs(out.pop("G_batched") - out.pop("G_per_chain")).max())
-    out["speedup_batched"] = out["per_chain"]["solve_s"] / out["batched"]["solve_s"]
+        return r, time.perf_counter() - t0
+
+    # warm-up: every mode twice (tables, launch shapes, workspaces, the basis pool)
+    for _ in range(2):
+        for gm, bg in modes.values():
+            run(gm, bg, (0, 1))
+    te = {k: [] for k in modes}
+    ts = {k: [] for k in modes}
+    last = {}
+    # timed runs interleaved over the modes, so slow phases of the box hit all of them
+    for _ in range(5):
+        for key, (gm, bg) in modes.items():
+            te[key].append(run(gm, bg, ())[1])
+    for _ in range(3):
+        for key, (gm, bg) in modes.items():
+            last[key], t = run(gm, bg, (0, 1))
+            ts[key].append(t)
+    for key in modes:
+        rs = last[key]
+        out[key] = {"solve_s": statistics.median(ts[key]), "eigen_s": statistics.median(te[key]),
+                    "solve_s_all": ts[key], "eigen_s_all": te[key], "nstates": rs["nstates"], "e0": rs["e0"],
+                    "green_steps": rs["green_steps"], "lanczos_steps": rs["lanczos_steps"]}
+        out["G_" + key] = rs["G"]
+    G0 = out["G_per_sector"]
+    for key in modes:
+        G = out.pop("G_" + key)
+        out[key]["max_abs_dG_vs_per_sector"] = float(np.abs(G - G0).max())
+        out[key]["speedup_vs_per_sector"] = out["per_sector"]["solve_s"] / out[key]["solve_s"]
     print(json.dumps(out), flush=True)
     ctx.close()
 

@@ -1881,6 +1881,143 @@ int edk_residual(edk_h *h, const void *psi_dev, double e, double *res_norm, doub
 // ---------------------------------------------------------------------------
 // batched Green chains (edk_batch.cu)
 // ---------------------------------------------------------------------------
+namespace edk {
+
+int gs_batch(edk_ctx *c, int nsec, edk_h *const *hs, int nitermax, int neigen, double tolerance, double demax,
+             const double *ran_tab, int every, GsBatchSector *out)
+{
+    if (nsec <= 0) return EDK_OK;
+    cudaStream_t st = c->stream;
+    int rc = EDK_OK;
+    const double *tab = ran_tab_for(c, ran_tab, &rc);
+    if (rc) return rc;
+    // items largest first (longest-processing-time order)
+    std::vector<int> order(nsec);
+    for (int i = 0; i < nsec; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return hs[a]->dim > hs[b]->dim; });
+    int64_t maxdim = 0, maxdup = 0;
+    int nmax = 1;
+    std::vector<HamDev> hd(nsec);
+    std::vector<GsItem> items(nsec);
+    for (int q = 0; q < nsec; ++q) {
+        const edk_h *h = hs[order[q]];
+        hd[q] = h->H;
+        GsItem &b = items[q];
+        b.ham = q;
+        b.dim = h->dim;
+        b.niter_max = (int32_t)std::min<int64_t>(nitermax, h->dim - 1);
+        b.ne = (int32_t)std::min<int64_t>(std::min<int64_t>(neigen, kGsMaxNe), b.niter_max);
+        b.tolerance = tolerance;
+        maxdim = std::max(maxdim, h->dim);
+        maxdup = std::max(maxdup, h->dup);
+        nmax = std::max(nmax, (int)b.niter_max);
+    }
+    const size_t ld = (size_t)nmax + 2;
+    DevBuf d_hams, d_items, d_alpha, d_beta, d_res, d_ptrs, d_coef;
+    if ((rc = c->cuda(d_alpha.ensure(sizeof(double) * ld * nsec), "alloc"))) return rc;
+    if ((rc = c->cuda(d_beta.ensure(sizeof(double) * ld * nsec), "alloc"))) return rc;
+    if ((rc = c->cuda(d_res.ensure(sizeof(int32_t) * 2 * nsec), "alloc"))) return rc;
+    for (int q = 0; q < nsec; ++q) {
+        items[q].alpha = d_alpha.as<double>() + (size_t)q * ld;
+        items[q].beta = d_beta.as<double>() + (size_t)q * ld;
+        items[q].result = d_res.as<int32_t>() + 2 * q;
+    }
+    const int R = 2 * maxdup * 8 + 16 * (int64_t)nmax <= 200 * 1024 ? 2 : 1;
+    if (maxdup * 8 + 16 * (int64_t)nmax > 200 * 1024)
+        return c->fail(EDK_ERR_UNSUPPORTED, "batched ground states: rows of at most 12288 states");
+    const int grid = (int)std::min<int64_t>(nsec, c->num_sms);
+    if ((rc = c->cuda(c->b_work.ensure(sizeof(double) * 4 * (size_t)maxdim * grid), "alloc batch workspace")))
+        return rc;
+    if ((rc = c->cuda(c->b_queue.ensure(sizeof(int)), "alloc"))) return rc;
+    if ((rc = c->cuda(upload(d_hams, hd, st), "upload hams"))) return rc;
+    if ((rc = c->cuda(upload(d_items, items, st), "upload items"))) return rc;
+    c->h2d_bytes += (int64_t)(hd.size() * sizeof(HamDev) + items.size() * sizeof(GsItem));
+    auto launch = [&](int pass) -> int {
+        int r2 = c->cuda(cudaMemsetAsync(c->b_queue.p, 0, sizeof(int), st), "memset");
+        if (r2) return r2;
+        r2 = c->cuda(launch_gs_batch(R, d_hams.as<HamDev>(), d_items.as<GsItem>(), nsec, c->b_queue.as<int>(),
+                                     c->b_work.p, maxdim, maxdup, nmax, tab, 1e-25, std::max(1, every), pass, grid,
+                                     st),
+                     "batched ground states");
+        c->launches++;
+        if (r2) return r2;
+        return c->cuda(cudaStreamSynchronize(st), "sync");
+    };
+    // ---- pass 1 ----
+    if ((rc = launch(1))) return rc;
+    std::vector<double> al(ld * nsec), be(ld * nsec);
+    std::vector<int32_t> res(2 * nsec);
+    cudaMemcpyAsync(al.data(), d_alpha.p, sizeof(double) * ld * nsec, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(be.data(), d_beta.p, sizeof(double) * ld * nsec, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(res.data(), d_res.p, sizeof(int32_t) * 2 * nsec, cudaMemcpyDeviceToHost, st);
+    if ((rc = c->cuda(cudaStreamSynchronize(st), "sync"))) return rc;
+    c->d2h_bytes += (int64_t)(sizeof(double) * 2 * ld * nsec + sizeof(int32_t) * 2 * nsec);
+    // ---- eigenpairs of every tridiagonal, the kept states (as edk_lanczos_e0) ----
+    std::vector<double> coef;
+    std::vector<void *> ptrs;
+    std::vector<int64_t> coef_off(nsec), ptr_off(nsec);
+    for (int q = 0; q < nsec; ++q) {
+        GsBatchSector &o = out[order[q]];
+        const int n = res[2 * q];
+        o.niter = n;
+        o.status = res[2 * q + 1];
+        if (o.status == 2 || n < 1) return c->fail(EDK_ERR_ZERO_START, "batched ground states: zero start vector");
+        const double *d = al.data() + q * ld, *e = be.data() + q * ld + 1;
+        for (int k = 0; k < n; ++k)
+            if (!std::isfinite(d[k]) || !std::isfinite(e[k])) return c->fail(EDK_ERR_NOT_FINITE, "non-finite Lanczos coefficient");
+        const int ne = items[q].ne;
+        const int m = std::min(ne, n);
+        std::vector<double> w(m), wp(m, 1e300);
+        tridiag_lowest(n, d, e, m, w.data());
+        if (n > 2) tridiag_lowest(n - 1, d, e, std::min(m, n - 1), wp.data());
+        coef_off[q] = (int64_t)coef.size();
+        ptr_off[q] = (int64_t)ptrs.size();
+        int kept = 0;
+        std::vector<double> kv;   // kept coefficient vectors
+        for (int j = 0; j < m; ++j) {
+            const bool conv = n > 2 && j < n - 1 && std::fabs(w[j] - wp[j]) < tolerance;
+            const bool inwin = w[j] >= w[0] && w[j] <= w[0] + demax;
+            if (!(j == 0 || (conv && inwin))) continue;
+            std::vector<double> prev, v(n);
+            int np = 0;
+            for (int p = 0; p < kept; ++p)
+                if (std::fabs(o.E[p] - w[j]) < 1e-8 * std::max(1.0, std::fabs(w[j]))) {
+                    prev.insert(prev.end(), kv.begin() + (size_t)p * n, kv.begin() + (size_t)(p + 1) * n);
+                    ++np;
+                }
+            tridiag_vector(n, d, e, w[j], prev.data(), np, v.data());
+            o.E[kept] = w[j];
+            o.converged[kept] = conv ? 1 : 0;
+            kv.insert(kv.end(), v.begin(), v.end());
+            void *p = nullptr;
+            if (cudaMalloc(&p, (size_t)hs[order[q]]->dim * 8) != cudaSuccess) {
+                (void)cudaGetLastError();
+                return c->fail(EDK_ERR_NOMEM, "batched ground states: state vector");
+            }
+            o.psi[kept] = p;
+            ptrs.push_back(p);
+            ++kept;
+        }
+        o.nkept = kept;
+        coef.insert(coef.end(), kv.begin(), kv.end());
+    }
+    // ---- pass 2: the kept states of every sector ----
+    if ((rc = c->cuda(upload(d_coef, coef, st), "upload coef"))) return rc;
+    if ((rc = c->cuda(upload(d_ptrs, ptrs, st), "upload state pointers"))) return rc;
+    for (int q = 0; q < nsec; ++q) {
+        const GsBatchSector &o = out[order[q]];
+        items[q].niter_max = o.niter;
+        items[q].ne = o.nkept;
+        items[q].coef = d_coef.as<double>() + coef_off[q];
+        items[q].psi = d_ptrs.as<void *const>() + ptr_off[q];
+    }
+    if ((rc = c->cuda(upload(d_items, items, st), "upload items"))) return rc;
+    c->h2d_bytes += (int64_t)(coef.size() * 8 + ptrs.size() * 8 + items.size() * sizeof(GsItem));
+    return launch(2);
+}
+
+}  // namespace edk
+
 extern "C" int edk_green_batch(edk_ctx *c, int dtype, int32_t nchain, const edk_chain *ch, int32_t nitergreen,
                                int32_t nw, const double *wn_host, double cutoff_dynamic, int32_t nout,
                                double *G_out, int32_t mode, edk_batch_stats *stats)

@@ -143,6 +143,43 @@ cudaError_t launch_batch(int dtype, int R, const HamDev *hams, const BatchItem *
                          cudaStream_t st);
 int batch_max_blocks_per_sm(int dtype, int R, int block, int64_t maxdup);
 
+// The ground state of one small FP64 sector in a batched launch (edk_batch.cu).
+// Pass 1: up to niter_max Lanczos steps from the table start vector with the
+// per-sector driver's convergence test on the lowest ne eigenvalues every
+// `every` steps; writes alpha[0..n), beta[0..n] and result = {n, status}
+// (status 1: Krylov space exhausted, 2: zero start).  Pass 2: niter_max = n
+// steps again, forming the ne normalised states psi + j*dim from the
+// tridiagonal eigenvector coefficients coef[j*niter_max + q].
+constexpr int kGsMaxNe = 3;
+struct GsItem {
+    int32_t ham;
+    int32_t niter_max;
+    int64_t dim;
+    int32_t ne;
+    int32_t pad = 0;
+    double tolerance;
+    double *alpha;
+    double *beta;
+    int32_t *result;
+    void *const *psi;      // pass 2: device array of ne state pointers
+    const double *coef;
+};
+// One sector's outcome of the batched ground states (gs_batch, edk_host.cpp).
+struct GsBatchSector {
+    int niter = 0, status = 0, nkept = 0;
+    double E[kGsMaxNe] = {0, 0, 0};
+    int converged[kGsMaxNe] = {0, 0, 0};
+    void *psi[kGsMaxNe] = {nullptr, nullptr, nullptr};   // cudaMalloc'd FP64 states, owned by the caller
+};
+// Ground states of nsec small FP64 sectors: pass 1 of all of them in one
+// persistent launch, the host's eigenpairs of each tridiagonal (the window
+// and kept states of edk_lanczos_e0), pass 2 in a second launch.
+int gs_batch(edk_ctx *c, int nsec, edk_h *const *hs, int nitermax, int neigen, double tolerance, double demax,
+             const double *ran_tab, int every, GsBatchSector *out);
+cudaError_t launch_gs_batch(int R, const HamDev *hams, const GsItem *items, int nitems, int *queue, void *work,
+                            int64_t maxdim, int64_t maxdup, int nmax, const double *tab, double cutoff, int every,
+                            int pass, int grid, cudaStream_t st);
+
 // ---- Nambu (Sz) sectors (edk_sz.cpp, edk_sz.cu) ----------------------------
 // A Nambu state is 2*ns bits: low half l = up orbitals, high half h = down
 // holes.  The states of popcount npart in increasing order group into rows

@@ -36,6 +36,8 @@ struct DBuf {
     void *p = nullptr;
     DBuf() = default;
     explicit DBuf(size_t bytes) { if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) p = nullptr; }
+    // takes ownership of a cudaMalloc'd pointer
+    static DBuf adopt(void *q) { DBuf b; b.p = q; return b; }
     DBuf(DBuf &&o) noexcept : p(o.p) { o.p = nullptr; }
     DBuf &operator=(DBuf &&o) noexcept { std::swap(p, o.p); return *this; }
     DBuf(const DBuf &) = delete;
@@ -54,6 +56,10 @@ constexpr int64_t kLowprecMinDim = (int64_t)1 << 20;
 constexpr int64_t kFp32SumsMinDim = (int64_t)1 << 20;
 // Longest row the batched kernel stages in shared memory (FP64 elements).
 constexpr int64_t kBatchMaxDup = 96 * 1024 / 8;
+// With edk_solve_opts.batch_gs = 1, FP64 sectors of more than kFullEdSwitch
+// and at most this many states run their ground states batched (gs_batch);
+// a larger value of batch_gs is the bound itself.
+constexpr int64_t kBatchGsMaxDim = (int64_t)1 << 14;
 // Sectors of at most this many states are diagonalised densely (ED_diago),
 // and with edk_solve_opts.reference_small_sectors their Green functions are
 // Lehmann sums (FULL_ED_SWITCH, Global_Variables.f90:23).
@@ -225,21 +231,74 @@ int edk_solve(edk_ctx *ctx, const edk_model *m, const edk_solve_opts *o, edk_sol
             states.push_back(std::move(stt));
         }
     }
+    auto in_bounds = [&](int nu, int nd) {
+        // goforit of get_eigen_energies (solver.h:134-137)
+        const int w = o->iwindow;
+        return !bounds_present ||
+               (nu <= bounds[1] + w && nd <= bounds[3] + w && nu >= bounds[0] - w && nd >= bounds[2] - w);
+    };
+    // batched ground states of the small FP64 sectors (edk_solve_opts.batch_gs)
+    std::map<int, edk::GsBatchSector> batched;
+    struct BatchedGuard {   // states formed but not taken over (an error on the way) are freed
+        std::map<int, edk::GsBatchSector> &m;
+        ~BatchedGuard()
+        {
+            for (auto &kv : m)
+                for (int k = 0; k < kv.second.nkept; ++k) cudaFree(kv.second.psi[k]);
+        }
+    } batched_guard{batched};
+    if (o->batch_gs && !o->gs_in && o->neigen <= edk::kGsMaxNe && !(o->residual_tol > 0.0)) {
+        std::vector<int> idx;
+        std::vector<edk_h *> hs;
+        for (int s = 0; s < o->nsectors; ++s) {
+            const int nu = o->sectors[2 * s], nd = o->sectors[2 * s + 1];
+            if (nu < 0 || nu > ns || nd < 0 || nd > ns || !in_bounds(nu, nd)) continue;
+            edk_h *h = nullptr;
+            if ((rc = getH(nu, nd, &h))) return rc;
+            int64_t dim = 0, dup = 0;
+            edk_h_dims(h, &dim, &dup, nullptr);
+            const int64_t maxdim = o->batch_gs > 1 ? (int64_t)o->batch_gs : kBatchGsMaxDim;
+            if (dim <= kFullEdSwitch || dim > maxdim || dup > kBatchMaxDup || sector_dtype(dim) != EDK_F64) continue;
+            idx.push_back(s);
+            hs.push_back(h);
+        }
+        std::vector<edk::GsBatchSector> res(hs.size());
+        const int every = o->check_every > 0 ? o->check_every : 8;
+        rc = edk::gs_batch(ctx, (int)hs.size(), hs.data(), o->nitermax, std::max(1, o->neigen), o->tolerance, demax,
+                           o->ran_tab, every, res.data());
+        for (size_t q = 0; q < res.size(); ++q) {
+            if (rc) {
+                for (void *p : res[q].psi) if (p) cudaFree(p);
+            } else {
+                batched[idx[q]] = res[q];
+            }
+        }
+        if (rc) return rc;
+    }
     for (int s = 0; s < (o->gs_in ? 0 : o->nsectors); ++s) {
         const int nu = o->sectors[2 * s], nd = o->sectors[2 * s + 1];
         if (nu < 0 || nu > ns || nd < 0 || nd > ns) return edk_internal_fail(ctx, EDK_ERR_INVALID, "sector");
-        if (bounds_present) {
-            // goforit of get_eigen_energies (solver.h:134-137)
-            const int w = o->iwindow;
-            if (!(nu <= bounds[1] + w && nd <= bounds[3] + w && nu >= bounds[0] - w && nd >= bounds[2] - w)) continue;
-        }
+        if (!in_bounds(nu, nd)) continue;
         edk_h *h = nullptr;
         if ((rc = getH(nu, nd, &h))) return rc;
         int64_t dim = 0;
         edk_h_dims(h, &dim, nullptr, nullptr);
         if (dim == 0) continue;
         std::vector<std::unique_ptr<State>> found;
-        if (dim <= kFullEdSwitch) {
+        auto bt = batched.find(s);
+        if (bt != batched.end()) {
+            // the states the batched passes formed (FP64)
+            const edk::GsBatchSector &g = bt->second;
+            lanczos_steps += (int64_t)g.niter * (1 + g.nkept);
+            for (int k = 0; k < g.nkept; ++k) {
+                auto stt = std::make_unique<State>();
+                stt->nup = nu; stt->ndn = nd; stt->E = g.E[k]; stt->E_pass1 = g.E[k]; stt->dtype = EDK_F64;
+                stt->converged = g.converged[k];
+                stt->psi = DBuf::adopt(g.psi[k]);
+                found.push_back(std::move(stt));
+            }
+            batched.erase(bt);
+        } else if (dim <= kFullEdSwitch) {
             // dense H from Hmult__ on unit vectors, FP64
             DBuf ecol((size_t)dim * 8), hcol((size_t)dim * dim * 8);
             std::vector<double> unit(dim, 0.0), Hd((size_t)dim * dim);

@@ -72,7 +72,7 @@ class _SolveOpts(C.Structure):
                 ("residual_tol", C.c_double), ("green_mode", C.c_int32), ("gs_in", C.c_char_p),
                 ("gs_out", C.c_char_p), ("sector_bound_file", C.c_char_p), ("iwindow", C.c_int32),
                 ("recompute_pass2", C.c_int32), ("reference_small_sectors", C.c_int32),
-                ("lowprec_min_dim", C.c_int64), ("fp32_sums", C.c_int32)]
+                ("lowprec_min_dim", C.c_int64), ("fp32_sums", C.c_int32), ("batch_gs", C.c_int32)]
 
 
 class _ChilocSectors(C.Structure):
@@ -855,7 +855,7 @@ def solve(ctx: Context, model: AIMModel, sectors, beta: float, nw: int, dtype="f
           nitermax=1000, tolerance=1e-12, tolerance_lowprec=1e-6, demax0=5.0, nitergreen=200,
           spins=(0, 1), pairs=None, cutoff_dynamic=1e-8, check_every=8, ran_tab=None, residual_tol=0.0,
           green_mode=0, gs_in=None, gs_out=None, sector_bound_file=None, iwindow=1, recompute_pass2=False,
-          reference_small_sectors=False, lowprec_min_dim=0, fp32_sums=False):
+          reference_small_sectors=False, lowprec_min_dim=0, fp32_sums=False, batch_gs=False):
     """One impurity solve through the C-ABI (edk_solve): host inputs, host outputs.
     recompute_pass2: rerun the Lanczos recurrence in pass 2 (the reference's way)
     instead of forming the eigenvectors from the Krylov vectors pass 1 kept.
@@ -866,6 +866,10 @@ def solve(ctx: Context, model: AIMModel, sectors, beta: float, nw: int, dtype="f
     vectors (0: 2^20).
     fp32_sums: in mixed precision, sum the hop terms of H*v in FP32 in sectors
     of at least 2^20 states (the recurrence, norms and alpha/beta stay FP64).
+    batch_gs: the ground states of the small FP64 sectors in persistent
+    launches over a work queue (pass 1 of all of them in one launch, pass 2 in
+    a second) instead of sector by sector; True batches sectors of at most
+    2^14 states, an integer above 1 is that bound.
 
     Returns dict(e0, z, residual, nstates, lanczos_steps, green_steps, G (2, npairs, nw) complex,
     docc (nc,), energies, sectors, e0_lowprec).
@@ -883,7 +887,7 @@ def solve(ctx: Context, model: AIMModel, sectors, beta: float, nw: int, dtype="f
                    None if gs_in is None else gs_in.encode(), None if gs_out is None else gs_out.encode(),
                    None if sector_bound_file is None else sector_bound_file.encode(), int(iwindow),
                    1 if recompute_pass2 else 0, 1 if reference_small_sectors else 0, int(lowprec_min_dim),
-                   1 if fp32_sums else 0)
+                   1 if fp32_sums else 0, int(batch_gs))
     G = np.zeros((2, len(pr) // 2, nw, 2))
     docc = np.zeros(model.nc)
     en = np.zeros(64)

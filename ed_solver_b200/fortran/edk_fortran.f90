@@ -111,7 +111,7 @@ module edk_fortran
     type(c_ptr) :: gs_in, gs_out, sector_bound_file
     integer(c_int32_t) :: iwindow, recompute_pass2, reference_small_sectors
     integer(c_int64_t) :: lowprec_min_dim
-    integer(c_int32_t) :: fp32_sums
+    integer(c_int32_t) :: fp32_sums, batch_gs
   end type
 
   type, bind(C) :: edk_solve_result

@@ -451,6 +451,15 @@ typedef struct edk_solve_opts {
     int32_t fp32_sums;           /* mixed precision: 1 sums the hop terms of H*v in FP32 in the
                                     FP32 passes of sectors of at least 2^20 states
                                     (edk_ctx_set_fp32_sums); 0 keeps every sum in FP64 */
+    int32_t batch_gs;            /* != 0: the ground states of the FP64 sectors of 41 to
+                                    (batch_gs == 1 ? 2^14 : batch_gs) states (rows of at most
+                                    12288 states; neigen <= 3; residual_tol 0) run batched: pass 1 of every such sector in one persistent
+                                    launch over a work queue (one block per sector, the
+                                    convergence test run on the device every check_every steps:
+                                    the lowest neigen eigenvalues of T_n against those of T_{n-1},
+                                    so a sector may take up to check_every-1 more steps than on
+                                    its own), pass 2 of their kept states in a second one.
+                                    0: every sector on its own (edk_lanczos_e0/gs) */
 } edk_solve_opts;
 
 typedef struct edk_solve_result {

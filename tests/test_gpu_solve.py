@@ -257,3 +257,26 @@ def test_c1_as_specified(ctx):
             G, _, _ = O.green_chain(O.OracleH(m, *tsec), phi, 200, e0, iph, wn)
             Go += G
         assert np.abs(r["G"][spin, 0] - Go).max() < 1e-8
+
+
+@pytest.mark.parametrize("name,neigen", [("c2", 1), ("c4", 3)])
+def test_batched_ground_states_equal_per_sector(ctx, name, neigen):
+    """edk_solve_opts.batch_gs: the ground states of the small FP64 sectors in
+    two persistent launches (pass 1 of every sector with its convergence test
+    on the device, then pass 2) against the sector-by-sector solve.  With the
+    step count fixed (tolerance 0, nitermax 60) both runs take the same steps:
+    E0 and G agree to 1e-9.  With the eigenvalue tolerance both stop on it
+    (the batched run checks every 8 steps, so it may take a few more): E0
+    agrees to 1e-9 and G to 2e-6."""
+    w = workload(name)
+    pairs = [(0, 0)] if w.model.nc == 1 else [(0, 0), (1, 1)]
+    kw = dict(neigen=neigen, nitergreen=100, spins=(0, 1), pairs=pairs, green_mode=1)
+    for extra, tol_g in ((dict(tolerance=0.0, nitermax=60), 1e-9), (dict(tolerance=1e-11), 2e-6)):
+        r0 = edk.solve(ctx, w.model, w.sectors, w.beta, 128, dtype="f64", **kw, **extra)
+        r1 = edk.solve(ctx, w.model, w.sectors, w.beta, 128, dtype="f64", batch_gs=True, **kw, **extra)
+        assert r1["nstates"] == r0["nstates"]
+        assert list(r1["sectors"]) == list(r0["sectors"])
+        assert abs(r1["e0"] - r0["e0"]) <= 1e-9 * abs(r0["e0"])
+        assert np.abs(np.array(r1["energies"]) - np.array(r0["energies"])).max() <= 1e-9 * abs(r0["e0"])
+        assert np.abs(r1["G"] - r0["G"]).max() <= tol_g * max(1.0, np.abs(r0["G"]).max()), \
+            np.abs(r1["G"] - r0["G"]).max()
