@@ -45,6 +45,10 @@ struct SpinTabDev {
     int lean_ks = 0;
     const uint32_t *lean = nullptr;
     const uint8_t *lean_kw = nullptr;
+    // The same entries blocked by 64 columns, entry-major inside a block:
+    // entry k of column c at (c/64)*64*lean_ks + k*64 + c%64, so entry k of a
+    // warp's 64 columns is one contiguous 256-byte load (the two-pass step).
+    const uint32_t *lean_b = nullptr;
 };
 
 // Everything a row kernel needs to evaluate (H x) for an element.
@@ -92,6 +96,7 @@ struct RowArgs {
     double *sums_out = nullptr;    // 4 doubles: final sums (deterministic order)
     int *flags = nullptr;          // [0] breakdown step (0 = none), [1] non-finite (1) or timeout (2)
     int sum32 = 0;                 // FP32 vectors: hop terms summed in FP32 (bulk-copy kernels)
+    void *scratch = nullptr;       // kind 5: an FP32 vector of the sector's dimension (partial sums)
 };
 
 // Launch shape of the fast row kernel: rows per group, up/down table-width
@@ -110,8 +115,11 @@ struct RowArgs {
 // 3 = 768 x 1 and 4 = 640 x 1 (kind 2).
 // kind 3: the lean FP32 kernel (edk_rows_lean.cuh), FP32 vectors with FP32
 // hop sums only; kmu is its table width lean_ks; variants 0 = 256 x 2
-// and 1 = 512 x 1; needs aligned column pairs.
-inline bool shape_needs_pairs(int kind) { return kind == 0 || kind == 2 || kind == 3; }
+// and 1 = 512 x 1; kind 5: the same arithmetic in two passes, the down-spin
+// hops from L2-resident column tiles (edk_rows_tiled.cuh), with an FP32
+// scratch vector (RowArgs::scratch); variant 0 stages two row pairs per
+// up-pass block, 1 one pair.  Both need aligned column pairs.
+inline bool shape_needs_pairs(int kind) { return kind == 0 || kind == 2 || kind == 3 || kind == 5; }
 struct FastShape {
     int r = 0, kmu = 0, kmd = 0, variant = 0, kind = 0;
 };

@@ -3,6 +3,7 @@
 #include "edk_rows_fast.cuh"
 #include "edk_rows_tma.cuh"
 #include "edk_rows_lean.cuh"
+#include "edk_rows_tiled.cuh"
 
 namespace edk {
 
@@ -105,6 +106,10 @@ int fast_shapes(const HamDev &H, int elem_bytes, int num_sms, FastShape *out, in
         const int64_t smem = lean_smem_bytes(H.dup);
         if (n < cap && 2 * smem + 16 * 1024 <= 228 * 1024) out[n++] = FastShape{2, ks, kd, 0, 3};
         if (n < cap && smem + 8 * 1024 <= 228 * 1024) out[n++] = FastShape{2, ks, kd, 1, 3};
+        // kind 5: up-spin pass with the rows staged (two row pairs or one per
+        // block), down-spin pass over L2-resident column tiles
+        if (n < cap && 2 * smem + 8 * 1024 <= 227 * 1024) out[n++] = FastShape{2, ks, kd, 0, 5};
+        if (n < cap && smem + 8 * 1024 <= 228 * 1024) out[n++] = FastShape{2, ks, kd, 1, 5};
     }
     return n;
 }
@@ -113,6 +118,7 @@ cudaError_t launch_rows_fast(const HamDev &H, int dtype, const RowArgs &a, int n
                              cudaStream_t st)
 {
     if (s.kind == 3) return dtype == EDK_F32 ? launch_lean_f32(H, a, num_sms, s, st) : cudaErrorInvalidValue;
+    if (s.kind == 5) return dtype == EDK_F32 ? launch_tiled_f32(H, a, num_sms, s, st) : cudaErrorInvalidValue;
     if (s.kind >= 1)
         return dtype == EDK_F64 ? launch_tma_f64(H, a, num_sms, s, st) : launch_tma_f32(H, a, num_sms, s, st);
     return dtype == EDK_F64 ? launch_fast_f64(H, a, num_sms, s, st) : launch_fast_f32(H, a, num_sms, s, st);

@@ -1,0 +1,282 @@
+// Two-pass FP32 row step with FP32 hop sums (launch shapes of kind 5): the
+// down-spin hops gathered from column tiles of x while the tile is resident
+// in L2.
+//
+// The fused row kernels gather the down-spin neighbours of a row at the full
+// width of x: about two thirds of those rows come from DRAM (a row-order
+// simulation of the neighbour graph gives about three reads of each row per
+// step), at DRAM latency.  Here the step is split the way the reference's
+// HAIMupdo_multr_split separates the two hop directions
+// (ed_solver/HAIMupdo.f90:1221-1347), without its transposes:
+//   1. up_pass_kernel: the up-spin hops and the diagonal of every element,
+//      rows staged in shared memory two at a time interleaved by column (the
+//      lean kernel's gathers), written to a scratch vector y1 (FP32);
+//   2. down_pass_kernel: column tiles of kTileW up-spin columns swept over all
+//      down rows, tile by tile across the whole grid (work unit = a tile and
+//      kTileRows rows, taken in tile-major order), so that every block
+//      gathers the neighbour rows' pieces of the tile -- kTileW x dim_dn x 4 B
+//      = 26 MB at ns=16, resident in L2 after its first touch -- and adds them
+//      to y1, then runs the Lanczos epilogue of the mode and the reductions.
+// x is read from DRAM about once per pass, at the price of writing and reading
+// y1.  All arithmetic as in the lean kernel: hop sums in FP32 (packed FP32x2
+// FMAs), the diagonal, the epilogue and the reductions in FP64.  No cluster,
+// no multicast, no inter-block waits.
+#pragma once
+#include "edk_rows_lean.cuh"
+
+namespace edk {
+
+constexpr int kTileW = 512;      // up-spin columns per tile (2 per thread of a 256-thread block)
+constexpr int kTileRows = 16;    // down rows per work unit
+
+// Pass 1: y1 = (diagonal + density) x + up-spin hops, FP32 out.  NP row
+// pairs per group, each staged interleaved by column in its own buffer, so one
+// table entry and palette value serve 2*NP rows.
+template <int KS, int NP, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) up_pass_kernel(const HamDev H, const float *__restrict__ x,
+                                                           float *__restrict__ y1)
+{
+    extern __shared__ __align__(16) float2 xs2[];    // [NP][dup]: {x[u,d0], x[u,d1]} per pair
+    __shared__ __align__(16) float2 pal2[256];
+    __shared__ double s_dsum[16];
+    constexpr int R = 2 * NP;
+    const int dup = (int)H.dup;
+    const int64_t ddn = H.ddn;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < H.up.npal; i += NT) {
+        const float h = (float)H.up.pal[i];
+        pal2[i] = make_float2(h, h);
+    }
+    if (tid < H.ncfg * H.ncfg) {
+        double t = 0.0;
+        for (int o2 = H.int_off[tid]; o2 < H.int_off[tid + 1]; ++o2) t += H.int_coef[o2];
+        s_dsum[tid] = t;
+    }
+    const uint64_t keep = l2_keep(), stream = l2_stream();
+    const uint32_t *__restrict__ lt = H.up.lean_b;
+    const uint8_t *__restrict__ kwb = H.up.lean_kw;
+    const double *__restrict__ upd = H.up.diag;
+    const uint8_t *__restrict__ upi = H.up.imp;
+    const int ncfg = H.ncfg;
+    const unsigned char *palb = reinterpret_cast<const unsigned char *>(pal2);
+    const int64_t ngroups = (ddn + R - 1) / R;
+    for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
+        int d[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) d[r] = (int)(R * g + r < ddn ? R * g + r : R * g);
+        __syncthreads();
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            const float *x0 = x + (int64_t)d[2 * p] * dup, *x1 = x + (int64_t)d[2 * p + 1] * dup;
+            float2 *dst = xs2 + (size_t)p * dup;
+#pragma unroll 4
+            for (int u = 2 * tid; u < dup; u += 2 * NT) {
+                const float2 a0 = ld2(x0 + u, keep), a1 = ld2(x1 + u, keep);
+                *reinterpret_cast<float4 *>(dst + u) = make_float4(a0.x, a1.x, a0.y, a1.y);
+            }
+        }
+        __syncthreads();
+        int cd[R];
+        double dd[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            cd[r] = (int)H.dn.imp[d[r]];
+            dd[r] = H.dn.diag[d[r]];
+        }
+        for (int c = 2 * tid; c < dup; c += 2 * NT) {
+            // entry k of the column pair: one 8-byte load, contiguous over the warp
+            uint2 ent[KS];
+            const uint2 *tp = reinterpret_cast<const uint2 *>(lt + (size_t)(c >> 6) * 64 * KS + (c & 63));
+#pragma unroll
+            for (int k = 0; k < KS; ++k) ent[k] = __ldg(tp + k * 32);
+            const double2 du = __ldg(reinterpret_cast<const double2 *>(upd + c));
+            const uchar2 cu = *reinterpret_cast<const uchar2 *>(upi + c);
+            const int kw = kwb[c >> 6];
+            float2 U[NP][2];
+#pragma unroll
+            for (int p = 0; p < NP; ++p) U[p][0] = U[p][1] = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int k = 0; k < KS; ++k) {
+                if (k < kw) {
+                    const uint32_t e0 = ent[k].x, e1 = ent[k].y;
+                    const float2 h0 = *reinterpret_cast<const float2 *>(palb + (e0 & 0x7F8u));
+                    const float2 h1 = *reinterpret_cast<const float2 *>(palb + (e1 & 0x7F8u));
+#pragma unroll
+                    for (int p = 0; p < NP; ++p) {
+                        const unsigned char *xb = reinterpret_cast<const unsigned char *>(xs2 + (size_t)p * dup);
+                        U[p][0] = ffma2(h0, *reinterpret_cast<const float2 *>(xb + (e0 >> 11)), U[p][0]);
+                        U[p][1] = ffma2(h1, *reinterpret_cast<const float2 *>(xb + (e1 >> 11)), U[p][1]);
+                    }
+                }
+            }
+            const double due[2] = {du.x, du.y};
+            const int cue[2] = {(int)cu.x, (int)cu.y};
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                const float4 o = *reinterpret_cast<const float4 *>(xs2 + (size_t)p * dup + c);
+                const float up[2][2] = {{U[p][0].x, U[p][1].x}, {U[p][0].y, U[p][1].y}};
+                const float ov[2][2] = {{o.x, o.z}, {o.y, o.w}};
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const int r = 2 * p + q;
+                    if (R * g + r >= ddn) break;
+                    float out[2];
+#pragma unroll
+                    for (int e = 0; e < 2; ++e)
+                        out[e] = (float)fma(s_dsum[cue[e] * ncfg + cd[r]] + (due[e] + dd[r]), (double)ov[q][e],
+                                            (double)up[q][e]);
+                    st2(y1 + (size_t)d[r] * dup + c, out[0], out[1], stream);
+                }
+            }
+        }
+    }
+}
+
+// Pass 2: the down-spin hops from L2-resident column tiles, added to y1, and
+// the epilogue of the mode.  KMD: bound on the down rows' lengths.
+template <int KMD, bool STEP>
+__global__ void __launch_bounds__(256, 4) down_pass_kernel(const HamDev H, const RowArgs a, const float *__restrict__ y1)
+{
+    constexpr int NT = 256;
+    __shared__ int s_nofs[kTileRows][KMD];
+    __shared__ __align__(16) float2 s_hd2[kTileRows][KMD];
+    __shared__ int s_nd[kTileRows];
+    const int dup = (int)H.dup;
+    const int64_t ddn = H.ddn;
+    const float *__restrict__ x = static_cast<const float *>(a.x);
+    const float *__restrict__ vkp = static_cast<const float *>(a.vk);
+    const float *__restrict__ vmp = static_cast<const float *>(a.vkm1);
+    const int tid = threadIdx.x;
+    const int mode = STEP ? (int)kModeStep : a.mode;
+    StepScalars sc;
+    const int ks = step_index(a);
+    if (!step_scalars(a, ks, sc)) return;
+    const uint64_t keep = l2_keep(), stream = l2_stream();
+    const int ntiles = (dup + kTileW - 1) / kTileW;
+    const int nchunks = (int)((ddn + kTileRows - 1) / kTileRows);
+    const int64_t nunits = (int64_t)ntiles * nchunks;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int64_t q = blockIdx.x; q < nunits; q += gridDim.x) {
+        const int tile = (int)(q / nchunks), chunk = (int)(q - (int64_t)tile * nchunks);
+        const int r0 = chunk * kTileRows;
+        const int nr = (int)(ddn - r0 < kTileRows ? ddn - r0 : kTileRows);
+        __syncthreads();   // the previous unit is done with the row tables
+        for (int t = tid; t < kTileRows * KMD; t += NT) {
+            const int r = t / KMD, f = t - r * KMD;
+            const int d = r0 + (r < nr ? r : 0);
+            const int f0 = H.dn.ptr[d], nd = H.dn.ptr[d + 1] - f0;
+            const bool ok = r < nr && f < nd;
+            const float h = ok ? (float)H.dn.val[f0 + f] : 0.f;
+            s_nofs[r][f] = (ok ? H.dn.tgt[f0 + f] : d) * dup;
+            s_hd2[r][f] = make_float2(h, h);
+            if (f == 0) s_nd[r] = r < nr ? nd : 0;
+        }
+        __syncthreads();
+        const int c = tile * kTileW + 2 * tid;
+        if (c >= dup) continue;
+        for (int r = 0; r < nr; ++r) {
+            const int d = r0 + r;
+            const size_t i = (size_t)d * dup + c;
+            // every global load of the element pair first
+            float2 xd[KMD];
+#pragma unroll
+            for (int f = 0; f < KMD; ++f) xd[f] = ld2(x + s_nofs[r][f] + c, keep);
+            const float2 own = ld2(x + i, keep);
+            const float2 yv = ld2(y1 + i, stream);
+            float2 vk2 = make_float2(0.f, 0.f), vm2 = make_float2(0.f, 0.f);
+            if (mode == kModeStep) {
+                vk2 = ld2(vkp + i, stream);
+                if (vmp) vm2 = ld2(vmp + i, stream);
+            }
+            const int nd = s_nd[r];
+            float2 D = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int f = 0; f < KMD; ++f)
+                if (f < nd) D = ffma2(s_hd2[r][f], xd[f], D);
+            const double acc[2] = {(double)yv.x + (double)D.x, (double)yv.y + (double)D.y};
+            const double sv[2] = {(double)own.x, (double)own.y};
+            if (mode == kModeHv) {
+                st2(static_cast<float *>(a.y) + i, (float)acc[0], (float)acc[1], stream);
+            } else if (mode == kModeFirst) {
+                float st[2];
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    st[e] = (float)(acc[e] - sc.gam1 * sv[e]);
+                    const double sd = (double)st[e];
+                    s0 += sd * sd; s1 += sd * sv[e]; s2 += sv[e] * sv[e];
+                }
+                st2(static_cast<float *>(a.y) + i, st[0], st[1], stream);
+            } else if (mode == kModeStep) {
+                const double vk[2] = {(double)vk2.x, (double)vk2.y}, vm[2] = {(double)vm2.x, (double)vm2.y};
+                float wt[2], vt[2];
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    vt[e] = (float)((sv[e] - sc.delta * vk[e]) * sc.inv_b);
+                    const double hv1 = (acc[e] - sc.delta * (sv[e] + sc.gam * vk[e] + sc.beta_k * vm[e])) * sc.inv_b;
+                    const double w = hv1 - sc.beta_k1 * vk[e];
+                    const double vd = (double)vt[e];
+                    wt[e] = (float)(w - sc.gam1 * vd);
+                    const double wd = (double)wt[e];
+                    s0 += wd * wd; s1 += wd * vd; s2 += vd * vd;
+                }
+                st2(static_cast<float *>(a.y) + i, wt[0], wt[1], stream);
+                st2(static_cast<float *>(a.vout) + i, vt[0], vt[1], stream);
+                if (a.psi) {
+                    float *p = static_cast<float *>(a.psi) + i;
+                    const float2 pv = ld2(p, stream);
+                    st2(p, (float)((double)pv.x + sc.cpsi * (double)vt[0]), (float)((double)pv.y + sc.cpsi * (double)vt[1]),
+                        stream);
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const double rr = acc[e] - a.eshift * sv[e];
+                    s0 += rr * rr; s2 += sv[e] * sv[e];
+                }
+            }
+        }
+    }
+    if (mode == kModeHv) return;
+    double v[4] = {s0, s1, s2, 0.0};
+    if (grid_sum<4>(v, a.partials, a.counter, a.sums_out))
+        if (mode == kModeFirst || mode == kModeStep) lanczos_finalize(a, ks);
+}
+
+// variant 0: two row pairs per up-pass block when they fit, 1: one pair
+template <int KS, int KMD>
+cudaError_t launch_tiled_t(const HamDev &H, const RowArgs &a, int num_sms, int variant, cudaStream_t st)
+{
+    if (!a.scratch) return cudaErrorInvalidValue;
+    float *y1 = static_cast<float *>(a.scratch);
+    // pass 1: rows staged in pairs interleaved by column -- two pairs per block
+    // (one block of 512 threads per SM) or one pair (two blocks per SM)
+    {
+        const size_t pair = lean_smem_bytes(H.dup);
+        const bool two = variant == 0 && 2 * pair + 8 * 1024 <= 227 * 1024;
+        auto k = two ? up_pass_kernel<KS, 2, 512, 1> : up_pass_kernel<KS, 1, 512, 2>;
+        const size_t smem = two ? 2 * pair : pair;
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 512, smem);
+        if (e != cudaSuccess) return e;
+        if (per_sm < 1) return cudaErrorInvalidConfiguration;
+        const int64_t groups = (H.ddn + (two ? 3 : 1)) / (two ? 4 : 2);
+        int64_t grid = (int64_t)num_sms * per_sm;
+        if (grid > groups) grid = groups;
+        k<<<(int)grid, 512, smem, st>>>(H, static_cast<const float *>(a.x), y1);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    auto k2 = a.mode == kModeStep ? down_pass_kernel<KMD, true> : down_pass_kernel<KMD, false>;
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2, 256, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    k2<<<num_sms * per_sm, 256, 0, st>>>(H, a, y1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tiled_f32(const HamDev &H, const RowArgs &a, int num_sms, const FastShape &s, cudaStream_t st);
+
+}  // namespace edk

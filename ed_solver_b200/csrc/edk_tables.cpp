@@ -204,6 +204,11 @@ SpinTableHost build_spin_table(const ModelHost &m, int spin, int np, const std::
             uint8_t &w = t.lean_kw[(size_t)i / 64];
             w = std::max<uint8_t>(w, (uint8_t)n);
         }
+        // blocked copy: entry k of column i at (i/64)*64*ks + k*64 + i%64
+        t.lean_b.assign((size_t)(dim + 63) / 64 * 64 * ks, 0);
+        for (int64_t i = 0; i < dim; ++i)
+            for (int k = 0; k < ks; ++k)
+                t.lean_b[(size_t)(i / 64) * 64 * ks + (size_t)k * 64 + (size_t)(i % 64)] = t.lean[(size_t)i * ks + k];
     }
     return t;
 }

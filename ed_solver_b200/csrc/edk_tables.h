@@ -27,6 +27,7 @@ struct SpinTableHost {
     int lean_ks = 0;
     std::vector<uint32_t> lean;
     std::vector<uint8_t> lean_kw;
+    std::vector<uint32_t> lean_b;   // the same entries blocked by 64 columns (see SpinTabDev::lean_b)
 };
 
 int64_t binom(int n, int k);
