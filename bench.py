@@ -298,8 +298,8 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
                          "traffic": traffic,
-                         "kernel": "fused FP32 Lanczos step (row kernel timed per sector shape; "
-                                   "row_lean_kernel on the chain sectors)",
+                         "kernel": "fused FP32 Lanczos step (row kernel timed per sector shape: "
+                                   "row_lean_kernel or the two-pass tiled step on the chain sectors)",
                          "launches": n6, "avg_launch_ms": (t6 / n6) if n6 else None,
                          "algorithmic_bytes_per_launch": (step_bytes / n6) if n6 else None},
             "cpu_baseline": cpu,
