@@ -32,7 +32,10 @@ constexpr int kTileRows = 16;    // down rows per work unit
 // Pass 1: y1 = (diagonal + density) x + up-spin hops, FP32 out.  NP row
 // pairs per group, each staged interleaved by column in its own buffer, so one
 // table entry and palette value serve 2*NP rows.
-template <int KS, int NP, int NT, int MINB>
+// SP: the palette has at most 32 values; lane l of every warp holds value l
+// in a register and a hop's value comes by a shuffle instead of a shared
+// load (the pass is bound by L1 / shared-memory throughput).
+template <int KS, int NP, int NT, int MINB, bool SP>
 __global__ void __launch_bounds__(NT, MINB) up_pass_kernel(const HamDev H, const float *__restrict__ x,
                                                            float *__restrict__ y1)
 {
@@ -59,6 +62,7 @@ __global__ void __launch_bounds__(NT, MINB) up_pass_kernel(const HamDev H, const
     const uint8_t *__restrict__ upi = H.up.imp;
     const int ncfg = H.ncfg;
     const unsigned char *palb = reinterpret_cast<const unsigned char *>(pal2);
+    const float palr = SP && (tid & 31) < H.up.npal ? (float)H.up.pal[tid & 31] : 0.f;
     const int64_t ngroups = (ddn + R - 1) / R;
     for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
         int d[R];
@@ -83,7 +87,14 @@ __global__ void __launch_bounds__(NT, MINB) up_pass_kernel(const HamDev H, const
             cd[r] = (int)H.dn.imp[d[r]];
             dd[r] = H.dn.diag[d[r]];
         }
-        for (int c = 2 * tid; c < dup; c += 2 * NT) {
+        // a warp's lanes iterate together (the shuffles need the whole warp):
+        // the loop runs on the warp's first column, lanes past the row end
+        // compute on the warp's first column and store nothing
+        const int lane = tid & 31;
+        for (int cw = 2 * (tid - lane); cw < dup; cw += 2 * NT) {
+            const int cl = cw + 2 * lane;
+            const bool valid = cl < dup;
+            const int c = valid ? cl : cw;
             // entry k of the column pair: one 8-byte load, contiguous over the warp
             uint2 ent[KS];
             const uint2 *tp = reinterpret_cast<const uint2 *>(lt + (size_t)(c >> 6) * 64 * KS + (c & 63));
@@ -91,7 +102,7 @@ __global__ void __launch_bounds__(NT, MINB) up_pass_kernel(const HamDev H, const
             for (int k = 0; k < KS; ++k) ent[k] = __ldg(tp + k * 32);
             const double2 du = __ldg(reinterpret_cast<const double2 *>(upd + c));
             const uchar2 cu = *reinterpret_cast<const uchar2 *>(upi + c);
-            const int kw = kwb[c >> 6];
+            const int kw = kwb[cw >> 6];
             float2 U[NP][2];
 #pragma unroll
             for (int p = 0; p < NP; ++p) U[p][0] = U[p][1] = make_float2(0.f, 0.f);
@@ -99,8 +110,16 @@ __global__ void __launch_bounds__(NT, MINB) up_pass_kernel(const HamDev H, const
             for (int k = 0; k < KS; ++k) {
                 if (k < kw) {
                     const uint32_t e0 = ent[k].x, e1 = ent[k].y;
-                    const float2 h0 = *reinterpret_cast<const float2 *>(palb + (e0 & 0x7F8u));
-                    const float2 h1 = *reinterpret_cast<const float2 *>(palb + (e1 & 0x7F8u));
+                    float2 h0, h1;
+                    if (SP) {
+                        const float a0 = __shfl_sync(0xffffffffu, palr, (int)((e0 >> 3) & 31u));
+                        const float a1 = __shfl_sync(0xffffffffu, palr, (int)((e1 >> 3) & 31u));
+                        h0 = make_float2(a0, a0);
+                        h1 = make_float2(a1, a1);
+                    } else {
+                        h0 = *reinterpret_cast<const float2 *>(palb + (e0 & 0x7F8u));
+                        h1 = *reinterpret_cast<const float2 *>(palb + (e1 & 0x7F8u));
+                    }
 #pragma unroll
                     for (int p = 0; p < NP; ++p) {
                         const unsigned char *xb = reinterpret_cast<const unsigned char *>(xs2 + (size_t)p * dup);
@@ -119,7 +138,7 @@ __global__ void __launch_bounds__(NT, MINB) up_pass_kernel(const HamDev H, const
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
                     const int r = 2 * p + q;
-                    if (R * g + r >= ddn) break;
+                    if (R * g + r >= ddn || !valid) break;
                     float out[2];
 #pragma unroll
                     for (int e = 0; e < 2; ++e)
@@ -253,7 +272,9 @@ cudaError_t launch_tiled_t(const HamDev &H, const RowArgs &a, int num_sms, int v
     {
         const size_t pair = lean_smem_bytes(H.dup);
         const bool two = variant == 0 && 2 * pair + 8 * 1024 <= 227 * 1024;
-        auto k = two ? up_pass_kernel<KS, 2, 512, 1> : up_pass_kernel<KS, 1, 512, 2>;
+        const bool sp = H.up.npal <= 32;
+        auto k = two ? (sp ? up_pass_kernel<KS, 2, 512, 1, true> : up_pass_kernel<KS, 2, 512, 1, false>)
+                     : (sp ? up_pass_kernel<KS, 1, 512, 2, true> : up_pass_kernel<KS, 1, 512, 2, false>);
         const size_t smem = two ? 2 * pair : pair;
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
