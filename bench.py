@@ -266,6 +266,12 @@ def run_ours(args):
         t64 = e_a.elapsed_time(e_b) * 1e-3 / n64
         # ---- plain H*v of the (8,8) sector, FP32 (the metric's first half) ----
         hv = _hv_time(ctx, model, peak)
+        # ---- the FP32 row-kernel launch shape the timing chose per sector of the solve ----
+        chosen = {}
+        for sec in [(8, 8), (9, 8), (7, 8), (8, 9), (8, 7)]:
+            hs = edk.Hamiltonian(ctx, model, *sec)
+            chosen["%d,%d" % sec] = hs.launch_shape_chosen("f32", WORKLOAD["fp32_sums"])
+            hs.close()
         steps64 = r64["lanczos_steps"] + r64["green_steps"]
         dG = float(np.abs(res["G"] - r64["G"]).max())
         dE = abs(res["e0"] - r64["e0"]) / abs(r64["e0"])
@@ -309,6 +315,7 @@ def run_ours(args):
             "clocks": clocks,
             "fp64": {"solve_s": t64, "solves_per_s": 1.0 / t64, "hv_steps": steps64, "solves_timed": n64},
             "hv": hv,
+            "row_kernel_shapes": chosen,
             "speedup_mixed_vs_fp64": t64 / (t_max * 1e-3 / args.steps),
             "accuracy_vs_fp64": {"rel_dE0": dE, "max_abs_dG": dG, "residual": res["residual"],
                                  "docc": float(res["docc"][0]), "docc_fp64": float(r64["docc"][0])},

@@ -1410,6 +1410,33 @@ int edk_h_launch_shapes(const edk_h *h, int dtype, int32_t *desc, int32_t cap)
     return n;
 }
 
+int edk_h_launch_shape_chosen(const edk_h *h, int dtype, int fp32_sums, int32_t *desc)
+{
+    if (!h || !desc || (dtype != EDK_F64 && dtype != EDK_F32)) return EDK_ERR_INVALID;
+    if (h->sz) return 0;
+    const int s32 = dtype == EDK_F32 && fp32_sums ? 1 : 0;
+    const int slot = dtype + 2 * s32;
+    FastShape out;
+    bool found = false;
+    if (h->fast_tuned[slot]) {
+        out = h->fast_shape[slot];
+        found = true;
+    } else {
+        char key[160];
+        std::snprintf(key, sizeof key, "%d:%lld:%lld:%d:%d:%d:%d", dtype, (long long)h->H.dup, (long long)h->H.ddn,
+                      h->H.up.ell_k, h->H.dn_kmax, h->H.nc, s32);
+        for (const auto &kv : h->ctx->fast_by_shape)
+            if (kv.first == key) { out = kv.second; found = true; }
+    }
+    if (!found) return 0;
+    desc[0] = out.r;
+    desc[1] = out.kmu;
+    desc[2] = out.kmd;
+    desc[3] = out.variant;
+    desc[4] = out.kind;
+    return 1;
+}
+
 int edk_h_dims(const edk_h *h, int64_t *dim, int64_t *dim_up, int64_t *dim_dn)
 {
     if (!h) return EDK_ERR_INVALID;

@@ -195,6 +195,7 @@ def lib():
         "edk_ctx_trim": (C.c_int, [P]),
         "edk_ctx_set_fp32_sums": (C.c_int, [P, C.c_int, C.c_int64]),
         "edk_h_launch_shapes": (C.c_int, [P, C.c_int, P, C.c_int32]),
+        "edk_h_launch_shape_chosen": (C.c_int, [P, C.c_int, C.c_int, P]),
         "edk_ctx_set_workspace_limit": (C.c_int, [P, C.c_int64]),
         "edk_ctx_timing_report": (C.c_int, [P, C.c_int, P, P]),
         "edk_h_create": (C.c_int, [P, P, C.c_int, C.c_int, P]),
@@ -466,6 +467,17 @@ class Hamiltonian:
             raise EdkError(EDK_ERR_INVALID, "launch_shapes")
         return [dict(zip(("rows", "kmu", "kmd", "variant", "kind"), map(int, desc[5 * i:5 * i + 5])))
                 for i in range(min(n, 32))]
+
+    def launch_shape_chosen(self, dtype="f32", fp32_sums=True):
+        """The launch shape the timing chose for this sector shape (a dict as
+        in launch_shapes), or None when none has been chosen yet."""
+        desc = np.zeros(5, np.int32)
+        rc = lib().edk_h_launch_shape_chosen(self.h, _dtype_code(dtype), int(bool(fp32_sums)), desc.ctypes.data)
+        if rc < 0:
+            raise EdkError(rc, "launch_shape_chosen")
+        if rc == 0:
+            return None
+        return dict(zip(("rows", "kmu", "kmd", "variant", "kind"), map(int, desc)))
 
     def hmult(self, x, out=None):
         """Hmult__: y = H x for a device tensor x (float64 or float32)."""

@@ -387,6 +387,13 @@ module edk_fortran
       import :: c_int, c_ptr
       type(c_ptr), value :: ctx
     end function
+    integer(c_int) function edk_h_launch_shape_chosen(h, dtype, fp32_sums, desc) &
+        bind(C, name="edk_h_launch_shape_chosen")
+      import :: c_int, c_ptr, c_int32_t
+      type(c_ptr), value :: h
+      integer(c_int), value :: dtype, fp32_sums
+      integer(c_int32_t) :: desc(5)
+    end function
     integer(c_int) function edk_h_launch_shapes(h, dtype, desc, cap) bind(C, name="edk_h_launch_shapes")
       import :: c_int, c_ptr, c_int32_t
       type(c_ptr), value :: h

@@ -144,10 +144,22 @@ int edk_h_dims(const edk_h *h, int64_t *dim, int64_t *dim_up, int64_t *dim_dn);
  * element type, in the order edk_ctx_set_kernel_path(ctx, 16 + i) selects
  * them; returns their number (or -1 on bad arguments) and writes the first
  * min(number, cap) as 5 ints each: rows per group, up-table bound, down-table
- * bound, block variant (0: 512 threads, 1: 256 x 2, 2: 128 x 4, 3: 768, 4: 640 per SM) and
- * kernel kind (0: register-staged rows, 1: rows staged by bulk copies with
- * the neighbour loads pipelined). */
+ * bound, block variant (0: 512 threads, 1: 256 x 2, 2: 128 x 4, 3: 768, 4: 640 per SM;
+ * kinds 3 and 5: see below) and kernel kind (0: register-staged rows, 1 and 2:
+ * rows staged by bulk copies, 3: two rows interleaved by column with packed
+ * FP32x2 hop sums, FP32 hop sums only, variant 0: 256 x 2, 1: 512 x 1; 5: the
+ * same arithmetic in two passes, the down-spin hops from L2-resident column
+ * tiles, variant 0: two row pairs per up-pass block, 1: one).  FP32 shapes of
+ * kinds 3 and 5 are listed while the context sums FP32 hops for this sector
+ * (edk_ctx_set_fp32_sums). */
 int edk_h_launch_shapes(const edk_h *h, int dtype, int32_t *desc, int32_t cap);
+/* The launch shape the timing chose for this sector shape and element type
+ * (with fp32_sums != 0: for FP32 hop sums): 1 and the 5 ints of
+ * edk_h_launch_shapes in desc when one was chosen on this handle or on
+ * another handle of the same sector shape in the context, 0 when none has
+ * been, EDK_ERR_INVALID on bad arguments.  No counterpart in the reference
+ * (a report of this library's own launch-shape tuning). */
+int edk_h_launch_shape_chosen(const edk_h *h, int dtype, int fp32_sums, int32_t *desc);
 /* Export one spin species' table (tab_HAIM2, HAIM_offdiag_arrays.f90:210-606)
  * as built for the device: CSR row pointer ptr[dim_s+1], 0-based target rank
  * tgt[nnz], value val[nnz], diagonal diag[dim_s].  Any pointer may be NULL;

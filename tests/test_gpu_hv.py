@@ -305,3 +305,22 @@ def test_hmult_split_rejects_hund_models(ctx):
     with pytest.raises(edk.EdkError) as e:
         h.hmult_split(torch.zeros(h.dim, dtype=torch.float64, device="cuda"))
     assert e.value.code == edk.EDK_ERR_UNSUPPORTED
+
+
+def test_launch_shape_chosen_is_reported():
+    """edk_h_launch_shape_chosen reports nothing before the first launch of a
+    sector shape in a context and the timed choice after it, also on a second
+    handle of the same sector shape."""
+    import torch
+    c = edk.Context(0)
+    try:
+        m = workload("c3").model
+        h1 = edk.Hamiltonian(c, m, 7, 6)
+        assert h1.launch_shape_chosen("f64", False) is None
+        h1.hmult(torch.zeros(h1.dim, dtype=torch.float64, device="cuda"))
+        s1 = h1.launch_shape_chosen("f64", False)
+        assert s1 is not None and s1 in h1.launch_shapes("f64")
+        h2 = edk.Hamiltonian(c, m, 7, 6)
+        assert h2.launch_shape_chosen("f64", False) == s1
+    finally:
+        c.close()
