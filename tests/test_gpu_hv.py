@@ -215,7 +215,7 @@ def test_launch_shape_timed_once_per_sector_shape():
         c.close()
 
 
-@pytest.mark.parametrize("name,sec", [("c3", (7, 7)), ("c5", (9, 8)), ("c5", (8, 8))])
+@pytest.mark.parametrize("name,sec", [("c3", (7, 7)), ("c3", (7, 6)), ("c5", (9, 8)), ("c5", (8, 8))])
 def test_lean_kernel_fp32_sums(ctx, name, sec):
     """The lean FP32 row kernels (kind 3: two rows staged interleaved by
     column, packed FP32x2 FMAs; kind 5: the same arithmetic in two passes,
