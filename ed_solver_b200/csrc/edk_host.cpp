@@ -577,10 +577,15 @@ int rows(edk_h *h, int dtype, const RowArgs &a_in)
     // FP32 hop sums where the context allows them (FP32 vectors of large sectors)
     a.sum32 = sum32_for(h, dtype);
     // the two-pass step (kind 5) keeps its partial sums in a scratch vector of
-    // the context; it is sized before any capture, by the sector's first launch
-    if (a.sum32 && h->H.up.lean && !c->capturing) {
-        int rc0 = c->cuda(c->tile_scratch.ensure(sizeof(float) * (size_t)h->dim), "alloc step scratch");
-        if (rc0) return rc0;
+    // the context; it is sized before any capture, by the sector's first
+    // launch.  Without room for it the other kinds serve (kind 5 launches
+    // fail without scratch, so the timing skips them).
+    if (a.sum32 && h->H.up.lean && !c->capturing && c->tile_scratch.bytes < sizeof(float) * (size_t)h->dim) {
+        if (c->tile_scratch.ensure(sizeof(float) * (size_t)h->dim) != cudaSuccess) {
+            (void)cudaGetLastError();
+            c->tile_scratch.p = nullptr;   // nothing was allocated
+            c->tile_scratch.bytes = 0;
+        }
     }
     if (a.sum32 && c->tile_scratch.bytes >= sizeof(float) * (size_t)h->dim) a.scratch = c->tile_scratch.p;
     LaunchCfg cfg;
@@ -598,6 +603,7 @@ int rows(edk_h *h, int dtype, const RowArgs &a_in)
             int rc = fast_shape_for(h, dtype, a, aligned, cfg.fast_shape);
             if (rc) return rc;
             if (shape_needs_pairs(cfg.fast_shape.kind) && !aligned) cfg.fast = false;
+            if (cfg.fast_shape.kind == 5 && !a.scratch) cfg.fast = false;   // chosen earlier, no scratch now
         }
     }
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;
