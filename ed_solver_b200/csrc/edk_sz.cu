@@ -24,6 +24,7 @@ namespace edk {
 namespace {
 
 constexpr int kSzBlock = 256;
+constexpr int kSeg = 4;        // hole-hole / pairing terms whose gathers are issued together
 
 // One entry of a row's list, in the order of the terms:
 //   kind 0: a whole up-up run (the per-state table of the run applies);
@@ -169,9 +170,49 @@ __global__ void __launch_bounds__(kSzBlock, 4) sz_row_kernel(const SzDev S, cons
                 for (int o = 0; o < nd; ++o)
                     if (!db[o] || (l & db[o])) acc = hmadd<T>(acc, de[o], xo);
             }
-            for (int e = 0; e < nt; ++e) {
+            for (int e = 0; e < nt;) {
                 const uint32_t kr = rt[e].kr;
-                if ((kr & 3u) == 0u) {
+                if ((kr & 3u) != 0u) {
+                    // up to kSeg consecutive hole-hole / pairing terms: every
+                    // target rank looked up, then every x gathered, then the
+                    // terms added in list order (the order of the reference)
+                    double hq[kSeg];
+                    int64_t jq[kSeg];
+                    bool on[kSeg];
+                    bool run = true;
+                    int taken = 0;
+#pragma unroll
+                    for (int q = 0; q < kSeg; ++q) {
+                        const int eq = e + q;
+                        run = run && eq < nt && (rt[eq].kr & 3u) != 0u;
+                        on[q] = false;
+                        hq[q] = 0.0;
+                        jq[q] = i;
+                        if (run) {
+                            ++taken;
+                            const RowTerm &t = rt[eq];
+                            if ((t.kr & 3u) == 1u) {
+                                on[q] = true;
+                                hq[q] = t.hv;
+                                jq[q] = (int64_t)t.joff + c;
+                            } else if ((l & t.lsrc) == t.lsrc && !(l & t.ltgt)) {
+                                on[q] = true;
+                                hq[q] = (__popc(l & t.lbtw) & 1) ? -t.hv : t.hv;
+                                jq[q] = (int64_t)t.joff + rank_low[l ^ t.lflip];
+                            }
+                        }
+                    }
+                    T xq[kSeg];
+#pragma unroll
+                    for (int q = 0; q < kSeg; ++q) xq[q] = on[q] ? __ldg(x + jq[q]) : T(0);
+#pragma unroll
+                    for (int q = 0; q < kSeg; ++q)
+                        if (on[q]) acc = hmadd<T>(acc, hq[q], xq[q]);
+                    e += taken;
+                    continue;
+                }
+                ++e;
+                {
                     // up-up run: this state's active terms from the run's table,
                     // four entries loaded ahead of their use
                     const SzRun &R = runs[kr >> 2];
@@ -195,14 +236,6 @@ __global__ void __launch_bounds__(kSzBlock, 4) sz_row_kernel(const SzDev S, cons
                         }
                         if (u[3] == kEllEnd) break;
                     }
-                } else if ((kr & 3u) == 1u) {
-                    acc = hmadd<T>(acc, rt[e].hv, __ldg(x + (int64_t)rt[e].joff + c));
-                } else {
-                    const uint32_t lsrc = rt[e].lsrc, ltgt = rt[e].ltgt;
-                    if ((l & lsrc) != lsrc || (l & ltgt)) continue;
-                    const int col = (int)rank_low[l ^ rt[e].lflip];
-                    const double hv = (__popc(l & rt[e].lbtw) & 1) ? -rt[e].hv : rt[e].hv;
-                    acc = hmadd<T>(acc, hv, __ldg(x + (int64_t)rt[e].joff + col));
                 }
             }
             row_epilogue<T>(a, sc, i, acc, xo, s0, s1, s2);
