@@ -107,9 +107,12 @@ int fast_shapes(const HamDev &H, int elem_bytes, int num_sms, FastShape *out, in
         if (n < cap && 2 * smem + 16 * 1024 <= 228 * 1024) out[n++] = FastShape{2, ks, kd, 0, 3};
         if (n < cap && smem + 8 * 1024 <= 228 * 1024) out[n++] = FastShape{2, ks, kd, 1, 3};
         // kind 5: up-spin pass with the rows staged (two row pairs or one per
-        // block), down-spin pass over L2-resident column tiles
+        // block, or four rows interleaved in one buffer), down-spin pass over
+        // L2-resident column tiles
         if (n < cap && 2 * smem + 8 * 1024 <= 227 * 1024) out[n++] = FastShape{2, ks, kd, 0, 5};
         if (n < cap && smem + 8 * 1024 <= 228 * 1024) out[n++] = FastShape{2, ks, kd, 1, 5};
+        if (n < cap && 2 * smem + 8 * 1024 <= 227 * 1024) out[n++] = FastShape{2, ks, kd, 2, 5};
+        if (n < cap && 2 * smem + 8 * 1024 <= 227 * 1024) out[n++] = FastShape{2, ks, kd, 3, 5};
     }
     return n;
 }

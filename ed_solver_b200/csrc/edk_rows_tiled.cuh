@@ -151,6 +151,124 @@ __global__ void __launch_bounds__(NT, MINB) up_pass_kernel(const HamDev H, const
     }
 }
 
+// Pass 1 with four rows interleaved by column in one buffer
+// ({x[u,d0], x[u,d1], x[u,d2], x[u,d3]} per column): one 16-byte shared load
+// per hop serves the four rows, where the two-buffer form issues two 8-byte
+// loads, so the random gathers take fewer shared-memory wavefronts.  The FMAs
+// and their order per element are those of up_pass_kernel.
+template <int KS, int NT, bool SP>
+__global__ void __launch_bounds__(NT, 1) up_pass_quad_kernel(const HamDev H, const float *__restrict__ x,
+                                                             float *__restrict__ y1)
+{
+    extern __shared__ __align__(16) float4 xs4[];    // [dup]
+    __shared__ __align__(16) float2 pal2[256];
+    __shared__ double s_dsum[16];
+    constexpr int R = 4;
+    const int dup = (int)H.dup;
+    const int64_t ddn = H.ddn;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < H.up.npal; i += NT) {
+        const float h = (float)H.up.pal[i];
+        pal2[i] = make_float2(h, h);
+    }
+    if (tid < H.ncfg * H.ncfg) {
+        double t = 0.0;
+        for (int o2 = H.int_off[tid]; o2 < H.int_off[tid + 1]; ++o2) t += H.int_coef[o2];
+        s_dsum[tid] = t;
+    }
+    const uint64_t keep = l2_keep(), stream = l2_stream();
+    const uint32_t *__restrict__ lt = H.up.lean_b;
+    const uint8_t *__restrict__ kwb = H.up.lean_kw;
+    const double *__restrict__ upd = H.up.diag;
+    const uint8_t *__restrict__ upi = H.up.imp;
+    const int ncfg = H.ncfg;
+    const unsigned char *palb = reinterpret_cast<const unsigned char *>(pal2);
+    const unsigned char *xb = reinterpret_cast<const unsigned char *>(xs4);
+    const float palr = SP && (tid & 31) < H.up.npal ? (float)H.up.pal[tid & 31] : 0.f;
+    const int64_t ngroups = (ddn + R - 1) / R;
+    for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
+        int d[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) d[r] = (int)(R * g + r < ddn ? R * g + r : R * g);
+        __syncthreads();
+        {
+            const float *x0 = x + (int64_t)d[0] * dup, *x1 = x + (int64_t)d[1] * dup;
+            const float *x2 = x + (int64_t)d[2] * dup, *x3 = x + (int64_t)d[3] * dup;
+#pragma unroll 2
+            for (int u = 2 * tid; u < dup; u += 2 * NT) {
+                const float2 a0 = ld2(x0 + u, keep), a1 = ld2(x1 + u, keep);
+                const float2 a2 = ld2(x2 + u, keep), a3 = ld2(x3 + u, keep);
+                xs4[u] = make_float4(a0.x, a1.x, a2.x, a3.x);
+                xs4[u + 1] = make_float4(a0.y, a1.y, a2.y, a3.y);
+            }
+        }
+        __syncthreads();
+        int cd[R];
+        double dd[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            cd[r] = (int)H.dn.imp[d[r]];
+            dd[r] = H.dn.diag[d[r]];
+        }
+        const int lane = tid & 31;
+        for (int cw = 2 * (tid - lane); cw < dup; cw += 2 * NT) {
+            const int cl = cw + 2 * lane;
+            const bool valid = cl < dup;
+            const int c = valid ? cl : cw;
+            uint2 ent[KS];
+            const uint2 *tp = reinterpret_cast<const uint2 *>(lt + (size_t)(c >> 6) * 64 * KS + (c & 63));
+#pragma unroll
+            for (int k = 0; k < KS; ++k) ent[k] = __ldg(tp + k * 32);
+            const double2 du = __ldg(reinterpret_cast<const double2 *>(upd + c));
+            const uchar2 cu = *reinterpret_cast<const uchar2 *>(upi + c);
+            const int kw = kwb[cw >> 6];
+            // U[p][e]: rows 2p, 2p+1 of column c+e
+            float2 U[2][2];
+            U[0][0] = U[0][1] = U[1][0] = U[1][1] = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int k = 0; k < KS; ++k) {
+                if (k < kw) {
+                    const uint32_t e0 = ent[k].x, e1 = ent[k].y;
+                    float2 h0, h1;
+                    if (SP) {
+                        const float a0 = __shfl_sync(0xffffffffu, palr, (int)((e0 >> 3) & 31u));
+                        const float a1 = __shfl_sync(0xffffffffu, palr, (int)((e1 >> 3) & 31u));
+                        h0 = make_float2(a0, a0);
+                        h1 = make_float2(a1, a1);
+                    } else {
+                        h0 = *reinterpret_cast<const float2 *>(palb + (e0 & 0x7F8u));
+                        h1 = *reinterpret_cast<const float2 *>(palb + (e1 & 0x7F8u));
+                    }
+                    // byte offset target * 16; bit 14 of an entry is the target's
+                    // lowest bit, and the palette index above bit 6 is masked off
+                    const float4 g0 = *reinterpret_cast<const float4 *>(xb + ((e0 >> 10) & ~15u));
+                    const float4 g1 = *reinterpret_cast<const float4 *>(xb + ((e1 >> 10) & ~15u));
+                    U[0][0] = ffma2(h0, make_float2(g0.x, g0.y), U[0][0]);
+                    U[1][0] = ffma2(h0, make_float2(g0.z, g0.w), U[1][0]);
+                    U[0][1] = ffma2(h1, make_float2(g1.x, g1.y), U[0][1]);
+                    U[1][1] = ffma2(h1, make_float2(g1.z, g1.w), U[1][1]);
+                }
+            }
+            const double due[2] = {du.x, du.y};
+            const int cue[2] = {(int)cu.x, (int)cu.y};
+            const float4 o0 = xs4[c], o1 = xs4[c + 1];
+            const float ov[R][2] = {{o0.x, o1.x}, {o0.y, o1.y}, {o0.z, o1.z}, {o0.w, o1.w}};
+            const float up[R][2] = {{U[0][0].x, U[0][1].x}, {U[0][0].y, U[0][1].y},
+                                    {U[1][0].x, U[1][1].x}, {U[1][0].y, U[1][1].y}};
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (R * g + r >= ddn || !valid) break;
+                float out[2];
+#pragma unroll
+                for (int e = 0; e < 2; ++e)
+                    out[e] = (float)fma(s_dsum[cue[e] * ncfg + cd[r]] + (due[e] + dd[r]), (double)ov[r][e],
+                                        (double)up[r][e]);
+                st2(y1 + (size_t)d[r] * dup + c, out[0], out[1], stream);
+            }
+        }
+    }
+}
+
 // Pass 2: the down-spin hops from L2-resident column tiles, added to y1, and
 // the epilogue of the mode.  KMD: bound on the down rows' lengths.
 template <int KMD, bool STEP>
@@ -261,7 +379,9 @@ __global__ void __launch_bounds__(256, 4) down_pass_kernel(const HamDev H, const
         if (mode == kModeFirst || mode == kModeStep) lanczos_finalize(a, ks);
 }
 
-// variant 0: two row pairs per up-pass block when they fit, 1: one pair
+// variant 0: two row pairs per up-pass block when they fit, 1: one pair,
+// 2 and 3: four rows interleaved in one buffer when they fit (else one pair),
+// 512 or 640 threads
 template <int KS, int KMD>
 cudaError_t launch_tiled_t(const HamDev &H, const RowArgs &a, int num_sms, int variant, cudaStream_t st)
 {
@@ -271,21 +391,25 @@ cudaError_t launch_tiled_t(const HamDev &H, const RowArgs &a, int num_sms, int v
     // (one block of 512 threads per SM) or one pair (two blocks per SM)
     {
         const size_t pair = lean_smem_bytes(H.dup);
-        const bool two = variant == 0 && 2 * pair + 8 * 1024 <= 227 * 1024;
+        const bool two = variant != 1 && 2 * pair + 8 * 1024 <= 227 * 1024;
+        const bool quad = two && variant >= 2;
+        const int nt = quad && variant == 3 ? 640 : 512;
         const bool sp = H.up.npal <= 32;
-        auto k = two ? (sp ? up_pass_kernel<KS, 2, 512, 1, true> : up_pass_kernel<KS, 2, 512, 1, false>)
-                     : (sp ? up_pass_kernel<KS, 1, 512, 2, true> : up_pass_kernel<KS, 1, 512, 2, false>);
+        auto k = quad && nt == 640 ? (sp ? up_pass_quad_kernel<KS, 640, true> : up_pass_quad_kernel<KS, 640, false>)
+                 : quad ? (sp ? up_pass_quad_kernel<KS, 512, true> : up_pass_quad_kernel<KS, 512, false>)
+                 : two  ? (sp ? up_pass_kernel<KS, 2, 512, 1, true> : up_pass_kernel<KS, 2, 512, 1, false>)
+                        : (sp ? up_pass_kernel<KS, 1, 512, 2, true> : up_pass_kernel<KS, 1, 512, 2, false>);
         const size_t smem = two ? 2 * pair : pair;
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         int per_sm = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 512, smem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, nt, smem);
         if (e != cudaSuccess) return e;
         if (per_sm < 1) return cudaErrorInvalidConfiguration;
         const int64_t groups = (H.ddn + (two ? 3 : 1)) / (two ? 4 : 2);
         int64_t grid = (int64_t)num_sms * per_sm;
         if (grid > groups) grid = groups;
-        k<<<(int)grid, 512, smem, st>>>(H, static_cast<const float *>(a.x), y1);
+        k<<<(int)grid, nt, smem, st>>>(H, static_cast<const float *>(a.x), y1);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
