@@ -111,8 +111,8 @@ int fast_shapes(const HamDev &H, int elem_bytes, int num_sms, FastShape *out, in
         // L2-resident column tiles
         if (n < cap && 2 * smem + 8 * 1024 <= 227 * 1024) out[n++] = FastShape{2, ks, kd, 0, 5};
         if (n < cap && smem + 8 * 1024 <= 228 * 1024) out[n++] = FastShape{2, ks, kd, 1, 5};
-        if (n < cap && 2 * smem + 8 * 1024 <= 227 * 1024) out[n++] = FastShape{2, ks, kd, 2, 5};
-        if (n < cap && 2 * smem + 8 * 1024 <= 227 * 1024) out[n++] = FastShape{2, ks, kd, 3, 5};
+        for (int v = 2; v <= 5; ++v)
+            if (n < cap && 2 * smem + 8 * 1024 <= 227 * 1024) out[n++] = FastShape{2, ks, kd, v, 5};
     }
     return n;
 }

@@ -28,6 +28,7 @@ namespace edk {
 
 constexpr int kTileW = 512;      // up-spin columns per tile (2 per thread of a 256-thread block)
 constexpr int kTileRows = 16;    // down rows per work unit
+constexpr int kQuadMaxBlocks = 256;   // 64-column blocks of a row the four-row up pass takes
 
 // Pass 1: y1 = (diagonal + density) x + up-spin hops, FP32 out.  NP row
 // pairs per group, each staged interleaved by column in its own buffer, so one
@@ -163,6 +164,7 @@ __global__ void __launch_bounds__(NT, 1) up_pass_quad_kernel(const HamDev H, con
     extern __shared__ __align__(16) float4 xs4[];    // [dup]
     __shared__ __align__(16) float2 pal2[256];
     __shared__ double s_dsum[16];
+    __shared__ uint8_t s_kw[kQuadMaxBlocks];          // hop count per 64-column block
     constexpr int R = 4;
     const int dup = (int)H.dup;
     const int64_t ddn = H.ddn;
@@ -171,6 +173,7 @@ __global__ void __launch_bounds__(NT, 1) up_pass_quad_kernel(const HamDev H, con
         const float h = (float)H.up.pal[i];
         pal2[i] = make_float2(h, h);
     }
+    for (int i = tid; i < (dup + 63) / 64; i += NT) s_kw[i] = H.up.lean_kw[i];
     if (tid < H.ncfg * H.ncfg) {
         double t = 0.0;
         for (int o2 = H.int_off[tid]; o2 < H.int_off[tid + 1]; ++o2) t += H.int_coef[o2];
@@ -178,7 +181,6 @@ __global__ void __launch_bounds__(NT, 1) up_pass_quad_kernel(const HamDev H, con
     }
     const uint64_t keep = l2_keep(), stream = l2_stream();
     const uint32_t *__restrict__ lt = H.up.lean_b;
-    const uint8_t *__restrict__ kwb = H.up.lean_kw;
     const double *__restrict__ upd = H.up.diag;
     const uint8_t *__restrict__ upi = H.up.imp;
     const int ncfg = H.ncfg;
@@ -192,15 +194,12 @@ __global__ void __launch_bounds__(NT, 1) up_pass_quad_kernel(const HamDev H, con
         for (int r = 0; r < R; ++r) d[r] = (int)(R * g + r < ddn ? R * g + r : R * g);
         __syncthreads();
         {
+            // one column per lane: the 16-byte stores of a warp are contiguous
             const float *x0 = x + (int64_t)d[0] * dup, *x1 = x + (int64_t)d[1] * dup;
             const float *x2 = x + (int64_t)d[2] * dup, *x3 = x + (int64_t)d[3] * dup;
 #pragma unroll 2
-            for (int u = 2 * tid; u < dup; u += 2 * NT) {
-                const float2 a0 = ld2(x0 + u, keep), a1 = ld2(x1 + u, keep);
-                const float2 a2 = ld2(x2 + u, keep), a3 = ld2(x3 + u, keep);
-                xs4[u] = make_float4(a0.x, a1.x, a2.x, a3.x);
-                xs4[u + 1] = make_float4(a0.y, a1.y, a2.y, a3.y);
-            }
+            for (int u = tid; u < dup; u += NT)
+                xs4[u] = make_float4(ld1(x0 + u, keep), ld1(x1 + u, keep), ld1(x2 + u, keep), ld1(x3 + u, keep));
         }
         __syncthreads();
         int cd[R];
@@ -215,13 +214,15 @@ __global__ void __launch_bounds__(NT, 1) up_pass_quad_kernel(const HamDev H, con
             const int cl = cw + 2 * lane;
             const bool valid = cl < dup;
             const int c = valid ? cl : cw;
+            // the block's hop count is uniform over the warp: entries past it
+            // are padding and not loaded
+            const int kw = s_kw[cw >> 6];
             uint2 ent[KS];
             const uint2 *tp = reinterpret_cast<const uint2 *>(lt + (size_t)(c >> 6) * 64 * KS + (c & 63));
 #pragma unroll
-            for (int k = 0; k < KS; ++k) ent[k] = __ldg(tp + k * 32);
+            for (int k = 0; k < KS; ++k) ent[k] = k < kw ? __ldg(tp + k * 32) : make_uint2(0u, 0u);
             const double2 du = __ldg(reinterpret_cast<const double2 *>(upd + c));
             const uchar2 cu = *reinterpret_cast<const uchar2 *>(upi + c);
-            const int kw = kwb[cw >> 6];
             // U[p][e]: rows 2p, 2p+1 of column c+e
             float2 U[2][2];
             U[0][0] = U[0][1] = U[1][0] = U[1][1] = make_float2(0.f, 0.f);
@@ -380,8 +381,8 @@ __global__ void __launch_bounds__(256, 4) down_pass_kernel(const HamDev H, const
 }
 
 // variant 0: two row pairs per up-pass block when they fit, 1: one pair,
-// 2 and 3: four rows interleaved in one buffer when they fit (else one pair),
-// 512 or 640 threads
+// 2 to 5: four rows interleaved in one buffer when they fit (else one pair),
+// 512, 640, 768 or 1024 threads
 template <int KS, int KMD>
 cudaError_t launch_tiled_t(const HamDev &H, const RowArgs &a, int num_sms, int variant, cudaStream_t st)
 {
@@ -392,10 +393,12 @@ cudaError_t launch_tiled_t(const HamDev &H, const RowArgs &a, int num_sms, int v
     {
         const size_t pair = lean_smem_bytes(H.dup);
         const bool two = variant != 1 && 2 * pair + 8 * 1024 <= 227 * 1024;
-        const bool quad = two && variant >= 2;
-        const int nt = quad && variant == 3 ? 640 : 512;
+        const bool quad = two && variant >= 2 && (H.dup + 63) / 64 <= kQuadMaxBlocks;
+        const int nt = !quad ? 512 : variant == 3 ? 640 : variant == 4 ? 768 : variant == 5 ? 1024 : 512;
         const bool sp = H.up.npal <= 32;
-        auto k = quad && nt == 640 ? (sp ? up_pass_quad_kernel<KS, 640, true> : up_pass_quad_kernel<KS, 640, false>)
+        auto k = quad && nt == 1024 ? (sp ? up_pass_quad_kernel<KS, 1024, true> : up_pass_quad_kernel<KS, 1024, false>)
+                 : quad && nt == 768 ? (sp ? up_pass_quad_kernel<KS, 768, true> : up_pass_quad_kernel<KS, 768, false>)
+                 : quad && nt == 640 ? (sp ? up_pass_quad_kernel<KS, 640, true> : up_pass_quad_kernel<KS, 640, false>)
                  : quad ? (sp ? up_pass_quad_kernel<KS, 512, true> : up_pass_quad_kernel<KS, 512, false>)
                  : two  ? (sp ? up_pass_kernel<KS, 2, 512, 1, true> : up_pass_kernel<KS, 2, 512, 1, false>)
                         : (sp ? up_pass_kernel<KS, 1, 512, 2, true> : up_pass_kernel<KS, 1, 512, 2, false>);
