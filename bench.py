@@ -37,7 +37,7 @@ WORKLOAD = dict(name="ns16_halffilled_E0_G512", nc=1, nb=15, sector=(8, 8), beta
 # measured on B200 with the library's start-vector table; used to convert a
 # per-step CPU time into solves/s for the reference arm.
 FP64_STEPS_PER_SOLVE = 1418
-PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "row_lean_kernel_step_ns16_9_8_f32.md")
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "row_tiled_step_ns16_9_8_f32.md")
 
 
 def _peaks():
@@ -50,7 +50,8 @@ def _peaks():
 
 
 def _traffic_per_launch():
-    """dram__bytes_read.sum + dram__bytes_write.sum of one fused-step launch (ncu summary)."""
+    """dram__bytes_read.sum + dram__bytes_write.sum of one fused step (ncu summary; the
+    two-pass step's two kernels together)."""
     try:
         with open(PROFILE_TRAFFIC) as f:
             for line in f:
@@ -304,8 +305,9 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
                          "traffic": traffic,
-                         "kernel": "fused FP32 Lanczos step (row kernel timed per sector shape: "
-                                   "row_lean_kernel or the two-pass tiled step on the chain sectors)",
+                         "kernel": "fused FP32 Lanczos step (row kernels timed per sector shape: the "
+                                   "two-pass tiled step, up_pass_quad_kernel + down_pass_kernel, or "
+                                   "row_lean_kernel; one launch = one step)",
                          "launches": n6, "avg_launch_ms": (t6 / n6) if n6 else None,
                          "algorithmic_bytes_per_launch": (step_bytes / n6) if n6 else None},
             "cpu_baseline": cpu,
