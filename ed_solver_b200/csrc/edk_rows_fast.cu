@@ -113,6 +113,11 @@ int fast_shapes(const HamDev &H, int elem_bytes, int num_sms, FastShape *out, in
         if (n < cap && smem + 8 * 1024 <= 228 * 1024) out[n++] = FastShape{2, ks, kd, 1, 5};
         for (int v = 2; v <= 5; ++v)
             if (n < cap && 2 * smem + 8 * 1024 <= 227 * 1024) out[n++] = FastShape{2, ks, kd, v, 5};
+        // the same with the down pass on four columns per thread (16-byte accesses)
+        if (H.dup % 4 == 0)
+            for (int v = 1; v <= 5; ++v)
+                if (n < cap && (v == 1 ? smem + 8 * 1024 <= 228 * 1024 : 2 * smem + 8 * 1024 <= 227 * 1024))
+                    out[n++] = FastShape{2, ks, kd, v | 8, 5};
     }
     return n;
 }

@@ -380,14 +380,143 @@ __global__ void __launch_bounds__(256, 4) down_pass_kernel(const HamDev H, const
         if (mode == kModeFirst || mode == kModeStep) lanczos_finalize(a, ks);
 }
 
-// variant 0: two row pairs per up-pass block when they fit, 1: one pair,
-// 2 to 5: four rows interleaved in one buffer when they fit (else one pair),
-// 512, 640, 768 or 1024 threads
+// Pass 2 with four columns per thread: every vector access is one 16-byte
+// load or store.  The block's 256 threads cover the tile's 512 columns twice,
+// and the two halves take alternate rows of the unit.  Needs dim_up a
+// multiple of 4 and 16-byte aligned vectors (checked at the launch).  Per
+// element the arithmetic is that of down_pass_kernel; only the order in which
+// a thread adds its elements into the reduction sums differs.
+template <int KMD, bool STEP>
+__global__ void __launch_bounds__(256, 3) down_pass4_kernel(const HamDev H, const RowArgs a,
+                                                            const float *__restrict__ y1)
+{
+    constexpr int NT = 256;
+    __shared__ int s_nofs[kTileRows][KMD];
+    __shared__ __align__(16) float2 s_hd2[kTileRows][KMD];
+    __shared__ int s_nd[kTileRows];
+    const int dup = (int)H.dup;
+    const int64_t ddn = H.ddn;
+    const float *__restrict__ x = static_cast<const float *>(a.x);
+    const float *__restrict__ vkp = static_cast<const float *>(a.vk);
+    const float *__restrict__ vmp = static_cast<const float *>(a.vkm1);
+    const int tid = threadIdx.x;
+    const int mode = STEP ? (int)kModeStep : a.mode;
+    StepScalars sc;
+    const int ks = step_index(a);
+    if (!step_scalars(a, ks, sc)) return;
+    const uint64_t keep = l2_keep(), stream = l2_stream();
+    const int ntiles = (dup + kTileW - 1) / kTileW;
+    const int nchunks = (int)((ddn + kTileRows - 1) / kTileRows);
+    const int64_t nunits = (int64_t)ntiles * nchunks;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int64_t q = blockIdx.x; q < nunits; q += gridDim.x) {
+        const int tile = (int)(q / nchunks), chunk = (int)(q - (int64_t)tile * nchunks);
+        const int r0 = chunk * kTileRows;
+        const int nr = (int)(ddn - r0 < kTileRows ? ddn - r0 : kTileRows);
+        __syncthreads();   // the previous unit is done with the row tables
+        for (int t = tid; t < kTileRows * KMD; t += NT) {
+            const int r = t / KMD, f = t - r * KMD;
+            const int d = r0 + (r < nr ? r : 0);
+            const int f0 = H.dn.ptr[d], nd = H.dn.ptr[d + 1] - f0;
+            const bool ok = r < nr && f < nd;
+            const float h = ok ? (float)H.dn.val[f0 + f] : 0.f;
+            s_nofs[r][f] = (ok ? H.dn.tgt[f0 + f] : d) * dup;
+            s_hd2[r][f] = make_float2(h, h);
+            if (f == 0) s_nd[r] = r < nr ? nd : 0;
+        }
+        __syncthreads();
+        const int c = tile * kTileW + 4 * (tid & 127);
+        if (c >= dup) continue;
+        for (int r = tid >> 7; r < nr; r += 2) {
+            const int d = r0 + r;
+            const size_t i = (size_t)d * dup + c;
+            // every global load of the four elements first
+            float4 xd[KMD];
+#pragma unroll
+            for (int f = 0; f < KMD; ++f) xd[f] = ld4(x + s_nofs[r][f] + c, keep);
+            const float4 own = ld4(x + i, keep);
+            const float4 yv = ld4(y1 + i, stream);
+            float4 vk4 = make_float4(0.f, 0.f, 0.f, 0.f), vm4 = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (mode == kModeStep) {
+                vk4 = ld4(vkp + i, stream);
+                if (vmp) vm4 = ld4(vmp + i, stream);
+            }
+            const int nd = s_nd[r];
+            float2 Dl = make_float2(0.f, 0.f), Dh = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int f = 0; f < KMD; ++f)
+                if (f < nd) {
+                    Dl = ffma2(s_hd2[r][f], make_float2(xd[f].x, xd[f].y), Dl);
+                    Dh = ffma2(s_hd2[r][f], make_float2(xd[f].z, xd[f].w), Dh);
+                }
+            const double acc[4] = {(double)yv.x + (double)Dl.x, (double)yv.y + (double)Dl.y,
+                                   (double)yv.z + (double)Dh.x, (double)yv.w + (double)Dh.y};
+            const double sv[4] = {(double)own.x, (double)own.y, (double)own.z, (double)own.w};
+            if (mode == kModeHv) {
+                st4(static_cast<float *>(a.y) + i, (float)acc[0], (float)acc[1], (float)acc[2], (float)acc[3], stream);
+            } else if (mode == kModeFirst) {
+                float st[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    st[e] = (float)(acc[e] - sc.gam1 * sv[e]);
+                    const double sd = (double)st[e];
+                    s0 += sd * sd; s1 += sd * sv[e]; s2 += sv[e] * sv[e];
+                }
+                st4(static_cast<float *>(a.y) + i, st[0], st[1], st[2], st[3], stream);
+            } else if (mode == kModeStep) {
+                const double vk[4] = {(double)vk4.x, (double)vk4.y, (double)vk4.z, (double)vk4.w};
+                const double vm[4] = {(double)vm4.x, (double)vm4.y, (double)vm4.z, (double)vm4.w};
+                float wt[4], vt[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    vt[e] = (float)((sv[e] - sc.delta * vk[e]) * sc.inv_b);
+                    const double hv1 = (acc[e] - sc.delta * (sv[e] + sc.gam * vk[e] + sc.beta_k * vm[e])) * sc.inv_b;
+                    const double w = hv1 - sc.beta_k1 * vk[e];
+                    const double vd = (double)vt[e];
+                    wt[e] = (float)(w - sc.gam1 * vd);
+                    const double wd = (double)wt[e];
+                    s0 += wd * wd; s1 += wd * vd; s2 += vd * vd;
+                }
+                st4(static_cast<float *>(a.y) + i, wt[0], wt[1], wt[2], wt[3], stream);
+                st4(static_cast<float *>(a.vout) + i, vt[0], vt[1], vt[2], vt[3], stream);
+                if (a.psi) {
+                    float *p = static_cast<float *>(a.psi) + i;
+                    const float4 pv = ld4(p, stream);
+                    st4(p, (float)((double)pv.x + sc.cpsi * (double)vt[0]), (float)((double)pv.y + sc.cpsi * (double)vt[1]),
+                        (float)((double)pv.z + sc.cpsi * (double)vt[2]), (float)((double)pv.w + sc.cpsi * (double)vt[3]),
+                        stream);
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const double rr = acc[e] - a.eshift * sv[e];
+                    s0 += rr * rr; s2 += sv[e] * sv[e];
+                }
+            }
+        }
+    }
+    if (mode == kModeHv) return;
+    double v[4] = {s0, s1, s2, 0.0};
+    if (grid_sum<4>(v, a.partials, a.counter, a.sums_out))
+        if (mode == kModeFirst || mode == kModeStep) lanczos_finalize(a, ks);
+}
+
+// variant & 7 -- 0: two row pairs per up-pass block when they fit, 1: one
+// pair, 2 to 5: four rows interleaved in one buffer when they fit (else one
+// pair), 512, 640, 768 or 1024 threads; variant & 8: the down pass with four
+// columns per thread where dim_up is a multiple of 4 and every vector is
+// 16-byte aligned (else two)
 template <int KS, int KMD>
-cudaError_t launch_tiled_t(const HamDev &H, const RowArgs &a, int num_sms, int variant, cudaStream_t st)
+cudaError_t launch_tiled_t(const HamDev &H, const RowArgs &a, int num_sms, int variant_in, cudaStream_t st)
 {
     if (!a.scratch) return cudaErrorInvalidValue;
     float *y1 = static_cast<float *>(a.scratch);
+    const int variant = variant_in & 7;
+    const uintptr_t align = reinterpret_cast<uintptr_t>(a.x) | reinterpret_cast<uintptr_t>(a.vk) |
+                            reinterpret_cast<uintptr_t>(a.vkm1) | reinterpret_cast<uintptr_t>(a.y) |
+                            reinterpret_cast<uintptr_t>(a.vout) | reinterpret_cast<uintptr_t>(a.psi) |
+                            reinterpret_cast<uintptr_t>(y1);
+    const bool four = (variant_in & 8) && H.dup % 4 == 0 && (align & 15u) == 0;
     // pass 1: rows staged in pairs interleaved by column -- two pairs per block
     // (one block of 512 threads per SM) or one pair (two blocks per SM)
     {
@@ -416,7 +545,8 @@ cudaError_t launch_tiled_t(const HamDev &H, const RowArgs &a, int num_sms, int v
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
-    auto k2 = a.mode == kModeStep ? down_pass_kernel<KMD, true> : down_pass_kernel<KMD, false>;
+    auto k2 = four ? (a.mode == kModeStep ? down_pass4_kernel<KMD, true> : down_pass4_kernel<KMD, false>)
+                   : (a.mode == kModeStep ? down_pass_kernel<KMD, true> : down_pass_kernel<KMD, false>);
     int per_sm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2, 256, 0);
     if (e != cudaSuccess) return e;

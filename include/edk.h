@@ -150,7 +150,8 @@ int edk_h_dims(const edk_h *h, int64_t *dim, int64_t *dim_up, int64_t *dim_dn);
  * FP32x2 hop sums, FP32 hop sums only, variant 0: 256 x 2, 1: 512 x 1; 5: the
  * same arithmetic in two passes, the down-spin hops from L2-resident column
  * tiles, variant 0: two row pairs per up-pass block, 1: one, 2 to 5: four
- * rows interleaved in one buffer, 512, 640, 768 or 1024 threads).  FP32 shapes of
+ * rows interleaved in one buffer, 512, 640, 768 or 1024 threads; + 8: the
+ * down pass on four columns per thread, 16-byte accesses).  FP32 shapes of
  * kinds 3 and 5 are listed while the context sums FP32 hops for this sector
  * (edk_ctx_set_fp32_sums). */
 int edk_h_launch_shapes(const edk_h *h, int dtype, int32_t *desc, int32_t cap);
