@@ -351,6 +351,36 @@ def run_kernel_case(args):
     ctx.close()
 
 
+def run_shape_sweep(args):
+    """CUDA-event time of the fused FP32 Lanczos step (FP32 hop sums) at every
+    feasible launch shape of the ns=16 sectors given (--shape-sweep, e.g.
+    9,8;8,9): each shape pinned in turn, 8 untimed steps, then 40 timed ones;
+    one JSON line per shape."""
+    import torch
+    from ed_solver_b200 import edk
+    ctx = edk.Context(0)
+    ctx.set_fp32_sums(True)
+    ctx.set_graphs(False)
+    model = _model()
+    for spec in args.shape_sweep.split(";"):
+        sector = tuple(int(v) for v in spec.split(","))
+        h = edk.Hamiltonian(ctx, model, *sector)
+        for i, sh in enumerate(h.launch_shapes("f32")):
+            ctx.set_kernel_path(16 + i)
+            h.lanczos_e0(dtype="f32", nitermax=8, tolerance=0.0, check_every=8)
+            ctx.timing(True)
+            h.lanczos_e0(dtype="f32", nitermax=40, tolerance=0.0, check_every=40)
+            torch.cuda.synchronize()
+            n, ms, _ = ctx.timing_report(6)
+            ctx.timing(False)
+            step = ms / max(n, 1)
+            print(json.dumps({"sector": list(sector), "shape_index": i, "shape": sh, "steps": n,
+                              "ms_per_step": step, "algorithmic_gbs": 12.0 * h.dim / step / 1e6}), flush=True)
+        h.close()
+    ctx.set_kernel_path(0)
+    ctx.close()
+
+
 def run_grad(args):
     """Gradients of E0 + G(i w_n) of the (8,8) ground state with respect to
     the 32 star-model parameters (15 bath levels, 15 hybridisations, impurity
@@ -737,6 +767,8 @@ def main():
     ap.add_argument("--kernel-sector", default=None, help="sector of the --kernel-case, e.g. 9,8")
     ap.add_argument("--fp32-sums", action="store_true",
                     help="sum the hop terms of H*v in FP32 in the FP32 passes of large sectors")
+    ap.add_argument("--shape-sweep", default=None,
+                    help="time the fused FP32 step at every launch shape of these ns=16 sectors, e.g. '9,8;8,9'")
     ap.add_argument("--grad", action="store_true",
                     help="time the 32 parameter gradients of E0 + G and check them by central differences")
     ap.add_argument("--grad-fd", type=int, default=4, help="parameters checked by central differences (--grad)")
@@ -772,6 +804,9 @@ def main():
         return
     if args.kernel_case:
         run_kernel_case(args)
+        return
+    if args.shape_sweep:
+        run_shape_sweep(args)
         return
     if args.warmup < 3:
         args.warmup = 3
