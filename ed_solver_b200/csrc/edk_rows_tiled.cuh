@@ -240,8 +240,9 @@ __global__ void __launch_bounds__(NT, 1) up_pass_quad_kernel(const HamDev H, con
                         h0 = *reinterpret_cast<const float2 *>(palb + (e0 & 0x7F8u));
                         h1 = *reinterpret_cast<const float2 *>(palb + (e1 & 0x7F8u));
                     }
-                    // byte offset target * 16; bit 14 of an entry is the target's
-                    // lowest bit, and the palette index above bit 6 is masked off
+                    // byte offset target * 16: entry >> 10 puts the target (from
+                    // bit 14) at bit 4, and the mask drops the palette index's top
+                    // bit, which lands in bit 0
                     const float4 g0 = *reinterpret_cast<const float4 *>(xb + ((e0 >> 10) & ~15u));
                     const float4 g1 = *reinterpret_cast<const float4 *>(xb + ((e1 >> 10) & ~15u));
                     U[0][0] = ffma2(h0, make_float2(g0.x, g0.y), U[0][0]);
